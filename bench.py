@@ -1,0 +1,376 @@
+"""Benchmark: all-pairs trajectory similarity, 2000 x 2000 trajectories, all
+six measures (DTW, EDR, LCSS, ERP, discrete Frechet, Hausdorff) per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = the six all-pairs launches over one 2000 x 2000 block (random-walk
+trajectories, lengths U{20..200}, float32; EDR/LCSS eps 3e-4 deg, ERP gap
+point at the box centre).  Under torchrun each rank computes its own
+2000 x 2000 block (rank r: queries = set r, database = set 0; rank 0 is the
+all-pairs matrix of set 0), with no collective on the data path ("weak").
+
+value    = DP cells/s over all ranks (Hausdorff: point-segment evaluations),
+           device time from CUDA events around each step's six launches, inputs
+           resident in HBM, L2 flushed (256 MB write) before every step.
+e2e      = the same cells/s through the public API core.matrix_many with host
+           inputs (padded float64 arrays as the reference takes them): packing,
+           H2D, the six launches, D2H of the six [2000, 2000] results and their
+           float64 normalisation, wall clock per step.
+roofline = the dominant kernel's FP32-issue rate (algorithmic ops per unit x
+           units / its event time) against SMs x 128 lanes x max SM clock.
+cpu_baseline = the reference's C++ measures (oracle/_ref: DTW, ERP, Frechet,
+           Hausdorff) and the FP64 port for EDR/LCSS, on rank 0 only, on a
+           bounded row sample of the same workload, all host threads.
+--impl reference: that CPU reference alone, as the reference arm.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURES = ["dtw", "edr", "lcss", "erp", "dfrechet", "hausdorff"]
+MID = {"dtw": 0, "edr": 1, "lcss": 2, "erp": 3, "dfrechet": 4, "hausdorff": 5}
+# Algorithmic FP32-pipe operations per unit (DP cell or point-segment
+# evaluation): the ideal scalar recurrence, not the kernel's instruction count.
+OPS_PER_UNIT = {"dtw": 7, "edr": 9, "lcss": 7, "erp": 9, "dfrechet": 7, "hausdorff": 12}
+N_TRAJ = 2000
+EPS = 3e-4
+WORKLOAD = "allpairs_2000x2000_six_measures"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU work of the cpu_baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rows", type=int, default=0, help="rows per thread (0 = library default)")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload_sets(rank):
+    from trajsimimeasures_b200 import datagen as D
+    d = D.trajectory_set(N_TRAJ, seed=D.SEED_DB)
+    q = d if rank == 0 else D.trajectory_set(N_TRAJ, seed=D.SEED_DB + rank)
+    return q, d
+
+
+def units(measure, lq, ld):
+    lq = lq.astype(np.float64)
+    ld = ld.astype(np.float64)
+    if measure == "hausdorff":
+        return float(lq.sum() * (ld - 1).sum() + ld.sum() * (lq - 1).sum())
+    return float(lq.sum() * ld.sum())
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        self.path = os.path.join("/tmp", f"tsm_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (oracle/_ref + FP64 port), bounded sample
+# ---------------------------------------------------------------------------
+
+def cpu_reference_run(q, d, rows, threads):
+    """Runs the CPU reference on rows `rows` of the Q x D block, all six
+    measures.  Returns (units, seconds, per-measure dict, kind string)."""
+    from oracle import oracle as O
+    from trajsimimeasures_b200 import datagen as D
+    qp, qo, ql = q
+    dp, do, dl = d
+    pts = np.concatenate([qp, dp])
+    shift = qp.shape[0]
+    nd = len(do)
+    qi = np.repeat(rows, nd)
+    di = np.tile(np.arange(nd), len(rows))
+    have_ref = O.ref_available()
+    rs = O.RefSet(pts, np.concatenate([qo, do + shift]), np.concatenate([ql, dl])) if have_ref else None
+    O.set_threads(threads)
+    tot_u, tot_t, per = 0.0, 0.0, {}
+    for name in MEASURES:
+        m = MID[name]
+        u = units(name, ql[rows], dl)
+        t0 = time.perf_counter()
+        if rs is not None and m in (0, 3, 4, 5):
+            rs.pairs(m, qi, di + len(qo), gpoint=D.BOX_CENTRE, threads=threads)
+            kind = "reference"
+        else:
+            O.pairs_f64(m, pts, qo[qi], ql[qi], do[di] + shift, dl[di], eps=EPS, gpoint=D.BOX_CENTRE)
+            kind = "port"
+        dt = time.perf_counter() - t0
+        per[name] = {"units_per_s": u / dt, "kind": kind}
+        tot_u += u
+        tot_t += dt
+    if rs is not None:
+        rs.close()
+    kinds = sorted({v["kind"] for v in per.values()})
+    return tot_u, tot_t, per, "+".join(kinds)
+
+
+def cpu_sample_rows(q, d, target_s, threads):
+    """Picks a row count whose six-measure CPU time is about target_s."""
+    probe = np.arange(2)
+    u, t, _, _ = cpu_reference_run(q, d, probe, threads)
+    per_row = t / len(probe)
+    nrows = int(max(1, min(N_TRAJ, target_s / max(per_row, 1e-6))))
+    return np.arange(nrows)
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    q, d = workload_sets(0)
+    threads = host_threads()
+    rows = cpu_sample_rows(q, d, 4.0, threads)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        u, t, per, kind = cpu_reference_run(q, d, rows, threads)
+        if i >= args.warmup:
+            vals.append((u, t))
+    U = sum(v[0] for v in vals)
+    T = sum(v[1] for v in vals)
+    value = U / T
+    line = {
+        "metric": "DP cells/s (6 measures, all-pairs 2000x2000)", "value": value, "unit": "cells/s",
+        "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * T / len(vals), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_rows": int(len(rows)), "n_traj": N_TRAJ},
+        "cpu_baseline": {"value": value, "unit": "cells/s", "cores": threads, "kind": kind,
+                         "sample": f"rows 0..{len(rows) - 1} of the 2000x2000 block x 6 measures per step "
+                                   "(reference C++ Traj::DTW/ERP/Frechet/HausdorffDistance; FP64 port for EDR/LCSS)"},
+        "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "per_measure": {k: v["units_per_s"] for k, v in per.items()},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args, ws, rank, local):
+    import torch
+    import torch.distributed as dist
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.engine import TrajSet, matrix_raw
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    q, d = workload_sets(rank)
+    qs = TrajSet.from_packed(*q, device=dev)
+    ds = TrajSet.from_packed(*d, device=dev)
+    order = ds.order_by_length()
+    nq, nd = qs.n, ds.n
+    outs = {m: torch.empty((nq, nd), dtype=torch.float32, device=dev) for m in MEASURES}
+    cnts = {m: torch.empty((nq, nd), dtype=torch.int32, device=dev) for m in ("edr", "lcss")}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    U = {m: units(m, q[2], d[2]) for m in MEASURES}
+
+    def step(evs=None):
+        for i, m in enumerate(MEASURES):
+            if evs is not None:
+                evs[i].record(stream)
+            matrix_raw(MID[m], qs, ds, out=outs[m], counts=cnts.get(m), d_order=order, eps=EPS,
+                       gpoint=D.BOX_CENTRE, rows=args.rows, stream=stream)
+        if evs is not None:
+            evs[len(MEASURES)].record(stream)
+
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        step()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if clk:
+        clk.start()
+        time.sleep(0.3)
+    per_ms = {m: 0.0 for m in MEASURES}
+    step_ms = []
+    launches = 0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(MEASURES) + 1)]
+        step(evs)
+        launches += len(MEASURES)
+        torch.cuda.synchronize()
+        for i, m in enumerate(MEASURES):
+            per_ms[m] += evs[i].elapsed_time(evs[i + 1])
+        step_ms.append(evs[0].elapsed_time(evs[-1]))
+    torch.cuda.synchronize()
+    clocks = clk.stop() if clk else None
+    if ws > 1:
+        dist.barrier()
+    tot_ms = float(sum(step_ms))
+    t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    units_step = sum(U.values())
+    value = ws * units_step * args.steps / (max_ms / 1e3)
+
+    # e2e through the public API, host inputs
+    e2e = None
+    if args.e2e_steps > 0:
+        from trajsimimeasures_b200 import core
+        Qpad = D.pad(D.unpack(*q))
+        lq = q[2].copy()
+        Dpad, ld = (Qpad, lq) if rank == 0 else (D.pad(D.unpack(*d)), d[2].copy())
+        core.matrix_many(MEASURES, Qpad, lq, Dpad, ld, eps=EPS, gpoint=D.BOX_CENTRE)  # warm
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(args.e2e_steps):
+            t0 = time.perf_counter()
+            core.matrix_many(MEASURES, Qpad, lq, Dpad, ld, eps=EPS, gpoint=D.BOX_CENTRE)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        tt = torch.tensor([sum(ts)], dtype=torch.float64, device=dev)
+        if ws > 1:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        h2d = sum(a.shape[0] * a.shape[1] * 8 + a.shape[0] * 12 for a in ((Qpad,) if Dpad is Qpad else (Qpad, Dpad)))
+        d2h = nq * nd * 4 * len(MEASURES)
+        e2e = {"value": ws * units_step * args.e2e_steps / float(tt.item()), "unit": "cells/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": 1e3 * float(tt.item()) / args.e2e_steps,
+               "path": "core.matrix_many(padded float64 host arrays) -> float64 host arrays"}
+
+    if rank != 0:
+        return
+    props = torch.cuda.get_device_properties(dev)
+    sms = props.multi_processor_count
+    max_mhz = (clocks or {}).get("sm_max_mhz") or 1965.0
+    peak_ops = sms * 128 * max_mhz * 1e6
+    per = {}
+    for m in MEASURES:
+        sec = per_ms[m] / 1e3
+        per[m] = {"units_per_s": U[m] * args.steps / sec, "pairs_per_s": nq * nd * args.steps / sec,
+                  "ms": per_ms[m] / args.steps,
+                  "fp32_issue_frac": U[m] * args.steps / sec * OPS_PER_UNIT[m] / peak_ops}
+    dom = max(MEASURES, key=lambda m: per_ms[m])
+    ach = per[dom]["units_per_s"] * OPS_PER_UNIT[dom]
+    roof = {"bound": "fp32-issue", "kernel": f"tsm::dp_matrix_kernel<{dom}>" if dom != "hausdorff"
+            else "tsm::hausdorff_matrix_kernel", "achieved": ach / 1e9, "peak": peak_ops / 1e9, "unit": "Gop/s",
+            "frac": ach / peak_ops, "traffic": None,
+            "peak_source": f"{sms} SMs x 128 FP32 lanes x {max_mhz:.0f} MHz max SM clock (not in MEASURED_PEAKS, "
+                           "which has HBM copy and bf16 GEMM only)",
+            "ops_per_unit": OPS_PER_UNIT[dom], "units_per_launch": U[dom]}
+    line = {
+        "metric": "DP cells/s (6 measures, all-pairs 2000x2000)", "value": value, "unit": "cells/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded random walks, Porto-like box)",
+        "config": {"workload": WORKLOAD, "n_traj": N_TRAJ, "lengths": "U{20..200}", "eps_deg": EPS,
+                   "erp_gpoint": list(D.BOX_CENTRE), "l2": "flushed before each step (256 MB write)",
+                   "parallelism": f"weak: one 2000x2000 block per rank x {ws}", "rows_per_thread": args.rows or 8},
+        "e2e": e2e, "gpu_launches": launches, "roofline": roof, "clocks": clocks, "per_measure": per,
+    }
+    if not args.no_cpu_baseline:
+        threads = host_threads()
+        rows = cpu_sample_rows(q, d, args.cpu_seconds, threads)
+        u, tcpu, cper, kind = cpu_reference_run(q, d, rows, threads)
+        line["cpu_baseline"] = {"value": u / tcpu, "unit": "cells/s", "cores": threads, "kind": kind,
+                                "seconds": tcpu,
+                                "sample": f"rows 0..{len(rows) - 1} of the 2000x2000 block x 6 measures "
+                                          "(reference C++ for DTW/ERP/Frechet/Hausdorff, FP64 port for EDR/LCSS)"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference_arm(args, ws, rank)
+        return
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,120 @@
+/*
+ * tsm.h -- C ABI of the B200 trajectory-similarity library (libtsm_b200.so).
+ *
+ * Replaces the reference's batched GPU measures, which are Python functions
+ * exported by core/__init__.py:1-10 and registered by name in
+ * utilities/method_helper.py:32-73 (heuristic_fn_wrapper):
+ *
+ *   core.dtw(t1, len1, t2, len2, threads_per_traj=64)         core/dtw.py:56-77
+ *   core.edr(t1, len1, t2, len2, eps, threads_per_traj=64)    core/edr.py:55-76
+ *   core.lcss(t1, len1, t2, len2, eps, threads_per_traj=64)   core/lcss.py:56-77
+ *   core.erp(t1, len1, t2, len2, gpoint=None, threads_per_traj=64)  core/erp.py:94-120
+ *   core.dfrechet(t1, len1, t2, len2, threads_per_traj=64)    core/discret_frechet.py:53-74
+ *   core.hausdorff(t1, len1, t2, len2, threads_per_traj=64)   core/hausdorff.py:97-123
+ *
+ * The Python package trajsimimeasures_b200 keeps those signatures and calls
+ * this ABI through ctypes.
+ *
+ * Conventions
+ *  - Trajectories are packed: one float32 array of (x, y) points, plus per
+ *    trajectory an int64 offset (in points) and an int32 length.
+ *  - Every pointer argument is DEVICE memory owned by the caller (for example
+ *    torch tensors).  `params` is a host pointer.  `stream` is a cudaStream_t
+ *    (NULL = legacy default stream).
+ *  - Calls only enqueue work on `stream` and return; results are valid after
+ *    the stream is synchronised.  The library allocates no device memory in
+ *    these calls.  Calls on different streams may run concurrently.
+ *  - Return value: 0 on success, a negative TSM_E* code otherwise; nothing is
+ *    thrown across the ABI.  tsm_last_error() gives the calling thread's last
+ *    message.  Pairs whose lengths are negative or exceed the declared
+ *    `max_len` are written as NaN (counts -1) instead of being computed.
+ *  - Degenerate lengths follow the reference kernels: DTW/Frechet of two empty
+ *    trajectories is 0 and of one empty trajectory +inf; ERP with an empty
+ *    trajectory is 0; EDR/LCSS with a zero denominator are NaN; Hausdorff
+ *    gives 0 for a direction whose target has fewer than two points.
+ */
+#ifndef TSM_B200_H
+#define TSM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Measures (same numbering as the oracle). */
+#define TSM_DTW 0
+#define TSM_EDR 1
+#define TSM_LCSS 2
+#define TSM_ERP 3
+#define TSM_DFRECHET 4
+#define TSM_HAUSDORFF 5
+
+/* flags */
+#define TSM_FLAG_EXACT 1u /* IEEE sqrt/reciprocal per cell: results are bit-identical to the
+                             FP32 twin in the oracle (default: hardware approximations,
+                             within 1e-6 relative) */
+
+/* error codes */
+#define TSM_OK 0
+#define TSM_EINVAL -1   /* bad argument */
+#define TSM_ECUDA -2    /* a CUDA runtime call failed (message has the CUDA error) */
+#define TSM_ETOOLONG -3 /* max_len beyond what the library supports */
+
+typedef struct tsm_params {
+    double eps;       /* EDR/LCSS match threshold (same units as the points); the
+                         kernels compare dx*dx+dy*dy < (float)(eps*eps) in FP32 */
+    double gx, gy;    /* ERP gap point (reference default (0, 0), core/erp.py:103) */
+    uint32_t flags;   /* TSM_FLAG_* */
+    int32_t rows_per_thread; /* 0 = default; else 4, 8 or 16 (register tile height) */
+} tsm_params;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int tsm_version(void);
+
+/* Last error message of the calling thread ("" if none). */
+const char* tsm_last_error(void);
+
+/* Largest trajectory length the kernels accept (points). */
+int32_t tsm_max_supported_len(void);
+
+/*
+ * Paired batch: out[k] = measure(traj a_k, traj b_k) for k < n_pairs.
+ * Replaces core.<measure>(t1, len1, t2, len2, ...) (per-pair batch form, the
+ * call made by test_trajsimi_time.py:253).
+ *   pts     float32 [n_points][2]
+ *   off_a, off_b  int64 [n_pairs]   first point of each trajectory
+ *   len_a, len_b  int32 [n_pairs]   lengths; every length <= max_len
+ *   order   int32 [n_pairs] or NULL: processing order (a permutation of
+ *           0..n_pairs-1 grouping pairs of similar shape), results are still
+ *           written at the pair's own index
+ *   out     float32 [n_pairs]
+ *   out_counts int32 [n_pairs] or NULL: EDR/LCSS edit/match counts before
+ *           normalisation (ignored for other measures)
+ */
+int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t* len_a,
+              const int64_t* off_b, const int32_t* len_b, const int32_t* order, int64_t n_pairs,
+              int32_t max_len, const tsm_params* params, float* out, int32_t* out_counts,
+              void* stream);
+
+/*
+ * All pairs of a query set Q and a database set D:
+ *   out[i*ld_out + j] = measure(Q_i, D_j),  i < nq, j < nd.
+ * Replaces the host-side Q x D pair expansion + batched core.<measure> calls of
+ * test_trajsimi_time_DQ.py:147-173 (and, with Q == D, the all-pairs matrix of
+ * test_clustering_time.py:219-269).
+ *   q_pts/d_pts float32 [.][2]; q_off/d_off int64; q_len/d_len int32
+ *   d_order int32 [nd] or NULL: processing order of D (e.g. D sorted by length)
+ *   q_max_len, d_max_len: upper bounds of the lengths in Q and D
+ *   out float32 [nq][ld_out]; out_counts int32 [nq][ld_out] or NULL (EDR/LCSS)
+ */
+int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len, int64_t nq,
+               int32_t q_max_len, const float* d_pts, const int64_t* d_off, const int32_t* d_len,
+               const int32_t* d_order, int64_t nd, int32_t d_max_len, const tsm_params* params,
+               float* out, int64_t ld_out, int32_t* out_counts, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TSM_B200_H */

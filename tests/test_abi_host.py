@@ -1,0 +1,139 @@
+"""CPU tests: the C-ABI library loads and exports what include/tsm.h declares,
+argument checks that return before any CUDA call, and the host-side logic
+(packing, ordering, generators, reference-signature validation)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "tsm.h")
+
+
+def _declared():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(tsm_[a-z0-9_]+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from trajsimimeasures_b200 import _lib
+    from trajsimimeasures_b200.build import build
+    build()
+    return _lib.load()
+
+
+def test_header_declares_python_exports():
+    from trajsimimeasures_b200 import _lib
+    assert set(_declared()) == set(_lib.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol(lib):
+    for name in _declared():
+        assert hasattr(lib, name), name
+
+
+def test_library_is_sm100a_only():
+    from trajsimimeasures_b200.build import ARCH
+    assert ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_version_and_limits(lib):
+    assert lib.tsm_version() >= 100
+    assert lib.tsm_max_supported_len() >= 200
+    assert lib.tsm_last_error() == b""
+
+
+def test_invalid_arguments_fail_before_cuda(lib):
+    from trajsimimeasures_b200 import _lib
+    p = _lib.params()
+    nul = ctypes.c_void_p(0)
+    rc = lib.tsm_pairs(9, nul, nul, nul, nul, nul, nul, 1, 10, ctypes.byref(p), nul, nul, nul)
+    assert rc == -1 and b"unknown measure" in lib.tsm_last_error()
+    rc = lib.tsm_pairs(0, nul, nul, nul, nul, nul, nul, 4, 10, ctypes.byref(p), nul, nul, nul)
+    assert rc == -1 and b"null pointer" in lib.tsm_last_error()
+    assert lib.tsm_pairs(0, nul, nul, nul, nul, nul, nul, 0, 10, ctypes.byref(p), nul, nul, nul) == 0
+    rc = lib.tsm_pairs(0, nul, nul, nul, nul, nul, nul, -1, 10, ctypes.byref(p), nul, nul, nul)
+    assert rc == -1
+    rc = lib.tsm_matrix(0, nul, nul, nul, 3, 10, nul, nul, nul, nul, 3, 10, ctypes.byref(p), nul, 3, nul, nul)
+    assert rc == -1
+    dummy = ctypes.c_void_p(16)
+    rc = lib.tsm_matrix(0, dummy, dummy, dummy, 3, 10, dummy, dummy, dummy, nul, 3, 10, ctypes.byref(p), dummy, 2,
+                        nul, nul)
+    assert rc == -1 and b"ld_out" in lib.tsm_last_error()
+    with pytest.raises(_lib.TsmError):
+        _lib.check(-1, "x")
+
+
+def test_pack_lists_and_padded():
+    from trajsimimeasures_b200.engine import pack_lists, pack_padded
+    trajs = [np.arange(6, dtype=np.float64).reshape(3, 2), np.zeros((0, 2)), np.ones((2, 2))]
+    pts, off, lens = pack_lists(trajs)
+    assert pts.dtype == np.float32 and pts.shape == (5, 2)
+    assert off.tolist() == [0, 3, 3] and lens.tolist() == [3, 0, 2]
+    arr = np.zeros((2, 4, 2))
+    p2, o2, l2 = pack_padded(arr, [4, 1])
+    assert p2.shape == (8, 2) and o2.tolist() == [0, 4] and l2.tolist() == [4, 1]
+    with pytest.raises(ValueError):
+        pack_padded(arr, [5, 1])
+
+
+def test_pair_order_groups_shapes():
+    from trajsimimeasures_b200.engine import pair_order
+    rng = np.random.default_rng(0)
+    la, lb = rng.integers(1, 300, 1000), rng.integers(1, 300, 1000)
+    o = pair_order(la, lb, rows=8)
+    assert sorted(o.tolist()) == list(range(1000))
+    nr = np.maximum(la, lb)[o]
+    blocks = (nr + 7) // 8
+    assert np.all(np.diff(blocks) >= 0)
+
+
+def test_generators_are_seeded_and_shaped():
+    from trajsimimeasures_b200 import datagen as G
+    a = G.trajectory_set(50)
+    b = G.trajectory_set(50)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    pts, off, lens = a
+    assert pts.dtype == np.float32 and lens.min() >= 20 and lens.max() <= 200
+    assert pts[:, 0].min() > -8.9 and pts[:, 0].max() < -8.3
+    _, _, ll, _, _ = G.pairs_lognormal(5000)
+    assert ll.min() >= 10 and ll.max() <= 2000 and 40 <= np.median(ll) <= 80
+
+
+def test_reference_signature_validation():
+    from trajsimimeasures_b200 import core
+    t = np.zeros((2, 5, 2))
+    with pytest.raises(AssertionError):
+        core.dtw(t, [5, 5], np.zeros((2, 6, 2)), [5, 5])  # dtw.py:60 asserts equal shapes
+    with pytest.raises(ValueError):
+        core.dtw(t, [5, 5], t, [5, 5], threads_per_traj=0)
+    with pytest.raises(AssertionError):
+        core.edr(t, [5, 5], np.zeros((3, 5, 2)), [5, 5, 5], 0.1)
+
+
+def test_heuristic_dispatch_names():
+    from trajsimimeasures_b200 import method_helper as mh
+    assert mh.is_heuristic("dtw") and mh.is_heuristic("hausdorff_cpu") and not mh.is_heuristic("T3S")
+    fn = mh.heuristic_fn_wrapper("edr")
+    assert fn.keywords["eps"] == mh.Config.trajsimi_edr_lcss_eps
+    assert fn.keywords["threads_per_traj"] == mh.Config.effi_gpu_threads_per_traj
+    with pytest.raises(NotImplementedError):
+        mh.heuristic_fn_wrapper("dtw_cpu")
+    with pytest.raises(AssertionError):
+        mh.heuristic_fn_wrapper("nope")
+
+
+def test_collate_pads_jointly():
+    from trajsimimeasures_b200 import method_helper as mh
+    batch = [([[0, 0], [1, 1], [2, 2]], [[5, 5]]), ([[1, 0]], [[3, 3], [4, 4]])]
+    t1, l1, t2, l2 = mh.heuristic_colllate_fn(batch, True)
+    assert t1.shape == t2.shape == (2, 3, 2) and t1.dtype == np.float64
+    assert l1 == [3, 1] and l2 == [1, 2]
+    u1, ul1, u2, ul2 = mh.heuristic_colllate_fn(batch, False)
+    assert ul1 == [3, 1] and len(u1) == 2

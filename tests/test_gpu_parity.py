@@ -1,0 +1,213 @@
+"""GPU parity tests: the CUDA library (through its C ABI) against the oracle.
+
+  * exact mode (IEEE sqrt/reciprocal): every measure bit-identical to the
+    FP32 same-arithmetic twin;
+  * default mode: DTW/ERP/Frechet/Hausdorff within REL_TOL (1e-5) of the FP64
+    restatement of the reference, EDR/LCSS counts bit-identical to the twin
+    (the threshold test runs in the same FP32 arithmetic) in every mode;
+  * the golden fixtures (outputs of the reference's own kernels) through the
+    reference-signature API;
+  * size-independent properties at the full 2000 x 2000 all-pairs size.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import REL_TOL, golden_cases, rel_err
+
+pytestmark = pytest.mark.gpu
+
+MEAS = [0, 1, 2, 3, 4, 5]
+NAMES = {0: "dtw", 1: "edr", 2: "lcss", 3: "erp", 4: "dfrechet", 5: "hausdorff"}
+EPS = 3e-4
+G = (-8.625, 41.15)
+
+
+def _dev(x, dt):
+    return torch.from_numpy(np.ascontiguousarray(x, dtype=dt)).cuda()
+
+
+def run_pairs(m, pts, off, lens, ia, ib, exact=False, rows=0, order=True, eps=EPS, gpoint=G):
+    from trajsimimeasures_b200.engine import pairs_raw, pair_order
+    ia, ib = np.asarray(ia), np.asarray(ib)
+    la, lb = lens[ia], lens[ib]
+    n = len(ia)
+    out = torch.full((n,), -7.0, device="cuda")
+    cnt = torch.full((n,), -7, dtype=torch.int32, device="cuda")
+    o = _dev(pair_order(la, lb), np.int32) if order else None
+    pairs_raw(m, _dev(pts, np.float32), _dev(off[ia], np.int64), _dev(la, np.int32), _dev(off[ib], np.int64),
+              _dev(lb, np.int32), int(max(la.max(initial=0), lb.max(initial=0))), out=out, counts=cnt, order=o,
+              eps=eps, gpoint=gpoint, exact=exact, rows=rows)
+    torch.cuda.synchronize()
+    return out.cpu().numpy(), cnt.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def cfg_pairs():
+    from trajsimimeasures_b200 import datagen as D
+    return D.pairs_uniform(1000)
+
+
+@pytest.fixture(scope="module")
+def near():
+    from trajsimimeasures_b200 import datagen as D
+    return D.near_pairs(300)
+
+
+@pytest.mark.parametrize("m", MEAS)
+@pytest.mark.parametrize("rows", [4, 8, 16])
+def test_exact_mode_bit_identical_to_twin(oracle_mod, cfg_pairs, m, rows):
+    O = oracle_mod
+    pts, off, lens, ia, ib = cfg_pairs
+    got, cnt = run_pairs(m, pts, off, lens, ia, ib, exact=True, rows=rows)
+    want, wcnt = O.pairs_idx(O.pairs_f32, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+    np.testing.assert_array_equal(got, want)
+    if m in (1, 2):
+        np.testing.assert_array_equal(cnt, wcnt)
+
+
+@pytest.mark.parametrize("m", MEAS)
+def test_default_mode_within_tolerance_of_fp64(oracle_mod, cfg_pairs, m):
+    O = oracle_mod
+    pts, off, lens, ia, ib = cfg_pairs
+    got, cnt = run_pairs(m, pts, off, lens, ia, ib)
+    d64, c64 = O.pairs_idx(O.pairs_f64, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+    if m in (1, 2):
+        _, wcnt = O.pairs_idx(O.pairs_f32, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+        np.testing.assert_array_equal(cnt, wcnt)
+        np.testing.assert_array_equal(cnt, c64)
+    else:
+        assert rel_err(got, d64).max() <= REL_TOL
+
+
+@pytest.mark.parametrize("m", [1, 2, 0, 5])
+def test_near_pairs_threshold_counts(oracle_mod, near, m):
+    O = oracle_mod
+    pts, off, lens, ia, ib = near
+    for exact in (False, True):
+        got, cnt = run_pairs(m, pts, off, lens, ia, ib, exact=exact)
+        want, wcnt = O.pairs_idx(O.pairs_f32, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+        if m in (1, 2):
+            np.testing.assert_array_equal(cnt, wcnt)
+            assert np.mean(wcnt > 0) > 0.5  # the threshold actually fires
+        elif exact:
+            np.testing.assert_array_equal(got, want)
+
+
+def test_edge_lengths_follow_reference_rules(oracle_mod):
+    """Lengths 0, 1, 2 and 31..33 (tile boundaries), in one batch."""
+    O = oracle_mod
+    from trajsimimeasures_b200 import datagen as D
+    ls = [0, 1, 2, 3, 7, 8, 9, 15, 16, 17, 31, 32, 33, 64, 65, 200]
+    la = np.repeat(ls, len(ls))
+    lb = np.tile(ls, len(ls))
+    pts, off, lens = D._walks(np.random.default_rng(5), np.concatenate([la, lb]), D.STEP_SIGMA)
+    n = len(la)
+    ia, ib = np.arange(n), np.arange(n) + n
+    for m in MEAS:
+        got, cnt = run_pairs(m, pts, off, lens, ia, ib, exact=True)
+        want, wcnt = O.pairs_idx(O.pairs_f32, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+        np.testing.assert_array_equal(got, want, err_msg=NAMES[m])
+        if m in (1, 2):
+            np.testing.assert_array_equal(cnt, wcnt)
+
+
+def test_overlong_pairs_are_flagged_not_computed():
+    from trajsimimeasures_b200.engine import pairs_raw
+    pts = torch.zeros((10, 2), device="cuda")
+    off = torch.zeros(2, dtype=torch.int64, device="cuda")
+    la = torch.tensor([5, 9], dtype=torch.int32, device="cuda")
+    lb = torch.tensor([5, 5], dtype=torch.int32, device="cuda")
+    out = torch.zeros(2, device="cuda")
+    cnt = torch.zeros(2, dtype=torch.int32, device="cuda")
+    pairs_raw(1, pts, off, la, off, lb, 6, out=out, counts=cnt, eps=0.1)
+    torch.cuda.synchronize()
+    assert out[0].item() == 0.0 and cnt[0].item() == 0
+    assert np.isnan(out[1].item()) and cnt[1].item() == -1
+
+
+@pytest.mark.parametrize("path", golden_cases(), ids=lambda p: p.rsplit("/", 1)[-1][:-4])
+def test_golden_through_reference_signature(path):
+    """The reference's own outputs, reproduced through core.<measure>(t1, len1, t2, len2, ...)."""
+    from trajsimimeasures_b200 import core, datagen as D
+    z = np.load(path)
+    pts, off, lens, ia, ib = z["pts"], z["off"], z["lens"], z["ia"], z["ib"]
+    ta = D.unpack(pts, off, lens, ia)
+    tb = D.unpack(pts, off, lens, ib)
+    w = int(lens.max())
+    t1, t2 = D.pad(ta, w), D.pad(tb, w)
+    l1, l2 = lens[ia], lens[ib]
+    eps, g = float(z["eps"]), list(z["gpoint"])
+    got = {
+        "dtw": core.dtw(t1, l1, t2, l2), "edr": core.edr(t1, l1, t2, l2, eps),
+        "lcss": core.lcss(t1, l1, t2, l2, eps), "erp": core.erp(t1, l1, t2, l2, g),
+        "dfrechet": core.dfrechet(t1, l1, t2, l2), "hausdorff": core.hausdorff(t1, l1, t2, l2),
+    }
+    for k, v in got.items():
+        assert v.dtype == np.float64 and v.shape == (len(ia),)
+        if k in ("edr", "lcss"):
+            np.testing.assert_array_equal(v, z[k], err_msg=k)
+        else:
+            assert rel_err(v, z[k]).max() <= REL_TOL, k
+
+
+def test_list_inputs_and_device_tensors_agree():
+    from trajsimimeasures_b200 import core, datagen as D
+    pts, off, lens, ia, ib = D.pairs_uniform(64, seed=11)
+    ta, tb = D.unpack(pts, off, lens, ia), D.unpack(pts, off, lens, ib)
+    w = int(lens.max())
+    t1, t2 = D.pad(ta, w), D.pad(tb, w)
+    a = core.dtw(t1, lens[ia], t2, lens[ib])
+    b = core.pairs(0, ta, None, tb, None)
+    c = core.dtw(torch.from_numpy(t1).cuda(), lens[ia], torch.from_numpy(t2).cuda(), lens[ib])
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(a, c.cpu().numpy())
+
+
+@pytest.mark.parametrize("m", MEAS)
+def test_matrix_equals_pairs_and_oracle(oracle_mod, m):
+    O = oracle_mod
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.engine import TrajSet, matrix
+    qp, qo, ql = D.trajectory_set(37, seed=D.SEED_QUERY)
+    dp, do, dl = D.trajectory_set(301)
+    qs, ds = TrajSet.from_packed(qp, qo, ql), TrajSet.from_packed(dp, do, dl)
+    for exact in (True, False):
+        out, cnt = matrix(m, qs, ds, eps=EPS, gpoint=G, exact=exact)
+        out = out.cpu().numpy()
+        if exact:
+            want, wcnt = O.matrix_idx(O.pairs_f32, m, qp, qo, ql, dp, do, dl, eps=EPS, gpoint=G)
+            np.testing.assert_array_equal(out, want)
+        else:
+            d64, c64 = O.matrix_idx(O.pairs_f64, m, qp, qo, ql, dp, do, dl, eps=EPS, gpoint=G)
+            if m in (1, 2):
+                np.testing.assert_array_equal(cnt.cpu().numpy(), c64)
+            else:
+                assert rel_err(out, d64).max() <= REL_TOL
+
+
+@pytest.fixture(scope="module")
+def full_set():
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.engine import TrajSet
+    p, o, l = D.trajectory_set(2000)
+    return (p, o, l), TrajSet.from_packed(p, o, l)
+
+
+@pytest.mark.parametrize("m", MEAS)
+def test_full_size_all_pairs_properties(oracle_mod, full_set, m):
+    """2000 x 2000 (the all-pairs benchmark size): exact symmetry, zero
+    self-distance, and 16 sampled rows against the oracle."""
+    O = oracle_mod
+    (p, o, l), s = full_set
+    from trajsimimeasures_b200.engine import matrix
+    out, cnt = matrix(m, s, s, eps=EPS, gpoint=G)
+    M = out.cpu().numpy()
+    assert np.array_equal(M, M.T)
+    np.testing.assert_array_equal(np.diag(M), np.zeros(2000, np.float32))
+    rows = np.random.default_rng(m).choice(2000, 16, replace=False)
+    d64, c64 = O.matrix_idx(O.pairs_f64, m, p, o[rows], l[rows], p, o, l, eps=EPS, gpoint=G)
+    if m in (1, 2):
+        np.testing.assert_array_equal(cnt.cpu().numpy()[rows], c64)
+    else:
+        assert rel_err(M[rows], d64).max() <= REL_TOL

@@ -1,0 +1,76 @@
+"""Pins the oracle against the reference's own outputs (CPU only).
+
+The golden fixtures hold outputs of the reference GPU kernels (core/*.py run
+by Numba's CUDA simulator) and of the reference C++ measures
+(query/cpp/spatial/traj.cpp), made by tests/golden/make_golden.py.
+"""
+import numpy as np
+import pytest
+
+from conftest import REL_TOL, golden_cases, rel_err
+
+MEASURES = [("dtw", 0), ("edr", 1), ("lcss", 2), ("erp", 3), ("dfrechet", 4), ("hausdorff", 5)]
+
+
+def _load(path):
+    z = np.load(path)
+    return {k: z[k] for k in z.files}
+
+
+@pytest.fixture(params=golden_cases(), ids=lambda p: p.rsplit("/", 1)[-1][:-4])
+def case(request):
+    return _load(request.param)
+
+
+def test_golden_present():
+    assert len(golden_cases()) >= 4
+
+
+@pytest.mark.parametrize("name,m", MEASURES)
+def test_f64_oracle_matches_reference_kernels(case, oracle_mod, name, m):
+    """FP64 restatement == the reference Numba kernels (same FP64 arithmetic)."""
+    O = oracle_mod
+    d64, _ = O.pairs_idx(O.pairs_f64, m, case["pts"], case["off"], case["lens"], case["ia"], case["ib"],
+                         eps=float(case["eps"]), gpoint=tuple(case["gpoint"]))
+    ref = case[name]
+    if m in (1, 2):
+        np.testing.assert_array_equal(d64, ref)  # identical counts, identical float64 division
+    else:
+        assert rel_err(d64, ref).max() <= 1e-12
+
+
+@pytest.mark.parametrize("name,m", [("dtw", 0), ("erp", 3), ("dfrechet", 4), ("hausdorff", 5)])
+def test_f64_oracle_matches_reference_cpp(case, oracle_mod, name, m):
+    """FP64 restatement vs the reference's C++ Traj measures (FP32 arithmetic,
+    FP32 gap point for ERP; its Hausdorff rebuilds the foot point in absolute
+    FP32 coordinates, so it only agrees to ~1e-3 there)."""
+    O = oracle_mod
+    ok = np.minimum(case["lens"][case["ia"]], case["lens"][case["ib"]]) >= 2  # C++ needs edges
+    d64, _ = O.pairs_idx(O.pairs_f64, m, case["pts"], case["off"], case["lens"], case["ia"], case["ib"],
+                         eps=float(case["eps"]), gpoint=tuple(case["gpoint"]))
+    tol = {0: 1e-5, 4: 1e-6, 3: 2e-4, 5: 5e-3}[m]
+    r = rel_err(case["cpp_" + name][ok], d64[ok])
+    assert r.max() <= tol, (name, r.max())
+
+
+@pytest.mark.parametrize("name,m", MEASURES)
+def test_f32_twin_within_tolerance_of_reference(case, oracle_mod, name, m):
+    O = oracle_mod
+    d32, c32 = O.pairs_idx(O.pairs_f32, m, case["pts"], case["off"], case["lens"], case["ia"], case["ib"],
+                           eps=float(case["eps"]), gpoint=tuple(case["gpoint"]))
+    ref = case[name]
+    if m in (1, 2):
+        la = case["lens"][case["ia"]].astype(np.int64)
+        lb = case["lens"][case["ib"]].astype(np.int64)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            norm = c32 / np.maximum(la, lb) if m == 1 else 1.0 - c32 / np.minimum(la, lb)
+        np.testing.assert_array_equal(norm, ref)
+    else:
+        assert rel_err(d32, ref).max() <= REL_TOL
+
+
+def test_near_case_exercises_thresholds(oracle_mod):
+    """The near-pairs fixture has both matching and non-matching point pairs."""
+    z = _load([p for p in golden_cases() if p.endswith("walks_near.npz")][0])
+    assert 0.0 < np.mean(z["lcss"]) < 1.0
+    assert np.any(z["edr"] < 1.0)

@@ -1,0 +1,73 @@
+"""ctypes binding of libtsm_b200.so (C ABI declared in include/tsm.h).
+
+The library is the only compute path: if it is missing or a call fails, the
+functions here raise.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libtsm_b200.so")
+
+DTW, EDR, LCSS, ERP, DFRECHET, HAUSDORFF = 0, 1, 2, 3, 4, 5
+MEASURES = {"dtw": DTW, "edr": EDR, "lcss": LCSS, "erp": ERP, "dfrechet": DFRECHET,
+            "frechet": DFRECHET, "hausdorff": HAUSDORFF}
+MEASURE_NAMES = {DTW: "dtw", EDR: "edr", LCSS: "lcss", ERP: "erp", DFRECHET: "dfrechet",
+                 HAUSDORFF: "hausdorff"}
+FLAG_EXACT = 1
+
+# Every symbol include/tsm.h declares (checked by the test suite).
+EXPORTS = ("tsm_version", "tsm_last_error", "tsm_max_supported_len", "tsm_pairs", "tsm_matrix")
+
+
+class TsmParams(ctypes.Structure):
+    _fields_ = [("eps", ctypes.c_double), ("gx", ctypes.c_double), ("gy", ctypes.c_double),
+                ("flags", ctypes.c_uint32), ("rows_per_thread", ctypes.c_int32)]
+
+
+class TsmError(RuntimeError):
+    pass
+
+
+_lock = threading.Lock()
+_lib = None
+
+_vp, _i32, _i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+
+
+def load():
+    """Loads the CUDA library once; raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise TsmError(f"{LIB_PATH} is missing: build it with `python -m trajsimimeasures_b200.build` "
+                           "(the CUDA library is the only compute path)")
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.tsm_version.restype = ctypes.c_int
+        lib.tsm_last_error.restype = ctypes.c_char_p
+        lib.tsm_max_supported_len.restype = _i32
+        lib.tsm_pairs.restype = ctypes.c_int
+        lib.tsm_pairs.argtypes = [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i32,
+                                  ctypes.POINTER(TsmParams), _vp, _vp, _vp]
+        lib.tsm_matrix.restype = ctypes.c_int
+        lib.tsm_matrix.argtypes = [ctypes.c_int, _vp, _vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _i64, _i32,
+                                   ctypes.POINTER(TsmParams), _vp, _i64, _vp, _vp]
+        _lib = lib
+    return _lib
+
+
+def check(rc: int, what: str):
+    if rc != 0:
+        msg = load().tsm_last_error().decode(errors="replace")
+        raise TsmError(f"{what} failed ({rc}): {msg}")
+
+
+def params(eps=0.0, gpoint=(0.0, 0.0), exact=False, rows_per_thread=0) -> TsmParams:
+    gx, gy = float(gpoint[0]), float(gpoint[1])
+    return TsmParams(float(eps), gx, gy, FLAG_EXACT if exact else 0, int(rows_per_thread))

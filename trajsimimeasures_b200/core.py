@@ -1,0 +1,299 @@
+"""Drop-in replacements for the reference's batched GPU measures (core/*.py).
+
+Same call surface as the reference:
+
+    dtw(t1, len1, t2, len2, threads_per_traj=64)            core/dtw.py:56-77
+    edr(t1, len1, t2, len2, eps, threads_per_traj=64)       core/edr.py:55-76
+    lcss(t1, len1, t2, len2, eps, threads_per_traj=64)      core/lcss.py:56-77
+    erp(t1, len1, t2, len2, gpoint=None, threads_per_traj=64)  core/erp.py:94-120
+    dfrechet(t1, len1, t2, len2, threads_per_traj=64)       core/discret_frechet.py:53-74
+    hausdorff(t1, len1, t2, len2, threads_per_traj=64)      core/hausdorff.py:97-123
+
+t1, t2: padded [batch, seq, 2] arrays (float64 in the reference; any float
+dtype is accepted and rounded to float32, the arithmetic type of the B200
+kernels) or lists of [n_i, 2] trajectories; len1, len2: lengths.  The result
+is a float64 NumPy array [batch] computed synchronously, like the reference.
+CUDA torch tensors in give a CUDA float64 tensor out without host copies.
+
+Differences from the reference, all deliberate:
+  * threads_per_traj is accepted and validated but does not set the launch
+    shape (the reference runs one 64-thread block per pair; the B200 kernels
+    pick their own tiling).
+  * erp accepts the gap point as a list, tuple or ndarray (the reference's
+    `gpoint == None` test raises for an ndarray, core/erp.py:103).
+  * hausdorff takes the max over valid points only (the reference's host
+    reduction also reads uninitialised padded slots, core/hausdorff.py:114,121).
+  * EDR/LCSS normalise the exact integer counts in float64 exactly as the
+    reference does (count / max(n1, n2), 1 - count / min(n1, n2)).
+
+Extra entry points for the Q x D and all-pairs shapes (the reference expands
+them into pair batches on the host, test_trajsimi_time_DQ.py:147-173 and
+test_clustering_time.py:219-269): ``matrix(measure, Q, lenQ, D, lenD, ...)``
+and ``<measure>_matrix(...)``.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from .engine import TrajSet, pack_lists, pair_order, pairs_raw, matrix_raw, measure_id
+
+__all__ = ["dtw", "edr", "lcss", "erp", "dfrechet", "hausdorff", "matrix", "dtw_matrix", "edr_matrix",
+           "lcss_matrix", "erp_matrix", "dfrechet_matrix", "hausdorff_matrix", "pairs"]
+
+
+def _check_tpt(threads_per_traj):
+    if not isinstance(threads_per_traj, (int, np.integer)) or threads_per_traj <= 0:
+        raise ValueError(f"threads_per_traj must be a positive int, got {threads_per_traj!r}")
+
+
+def _lens_np(lens, n):
+    if isinstance(lens, torch.Tensor):
+        lens = lens.detach().cpu().numpy()
+    a = np.asarray(lens, dtype=np.int64).reshape(-1)
+    if a.shape[0] != n:
+        raise ValueError(f"{a.shape[0]} lengths for {n} trajectories")
+    return a
+
+
+def _as_points(t):
+    """padded array/tensor -> (float32 [N, L, 2] host array or CUDA tensor, N, L); list -> None."""
+    if isinstance(t, torch.Tensor):
+        if t.dim() != 3 or t.shape[-1] < 2:
+            raise ValueError("expected a padded [batch, seq, 2] tensor")
+        return t[..., :2].to(torch.float32).contiguous(), t.shape[0], t.shape[1]
+    if isinstance(t, np.ndarray):
+        if t.ndim != 3 or t.shape[-1] < 2:
+            raise ValueError("expected a padded [batch, seq, 2] array")
+        return np.ascontiguousarray(t[..., :2], dtype=np.float32), t.shape[0], t.shape[1]
+    return None
+
+
+def _normalise_counts(m, counts, la, lb):
+    """Reference normalisation in float64 (edr.py:51, lcss.py:52)."""
+    c = counts.astype(np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        if m == _lib.EDR:
+            return c / np.maximum(la, lb)
+        return 1.0 - c / np.minimum(la, lb)
+
+
+def pairs(measure, t1, len1, t2, len2, *, eps=0.0, gpoint=(0.0, 0.0), exact=False, rows=0, counts=False):
+    """Paired batch: result[k] = measure(t1[k][:len1[k]], t2[k][:len2[k]]).
+
+    Returns float64 (NumPy for host inputs, CUDA tensor for CUDA inputs); with
+    counts=True also the int32 EDR/LCSS counts."""
+    m = measure_id(measure)
+    p1, p2 = _as_points(t1), _as_points(t2)
+    if p1 is None or p2 is None:  # lists of trajectories
+        n = len(t1)
+        if len(t2) != n:
+            raise ValueError("t1 and t2 hold different numbers of trajectories")
+        la = _lens_np(len1, n) if len1 is not None else np.array([len(x) for x in t1])
+        lb = _lens_np(len2, n) if len2 is not None else np.array([len(x) for x in t2])
+        pts, off, lens = pack_lists([np.asarray(x)[:l] for x, l in zip(list(t1) + list(t2), np.concatenate([la, lb]))])
+        off_a, off_b = off[:n], off[n:]
+        on_device = False
+        dev = torch.device("cuda")
+    else:
+        (a1, n, L1), (a2, n2, L2) = p1, p2
+        if n2 != n:
+            raise ValueError("t1 and t2 hold different numbers of trajectories")
+        la, lb = _lens_np(len1, n), _lens_np(len2, n)
+        if n and (la.min() < 0 or lb.min() < 0 or la.max() > L1 or lb.max() > L2):
+            raise ValueError("a length is negative or exceeds the padded width")
+        on_device = isinstance(a1, torch.Tensor) and a1.is_cuda
+        dev = a1.device if on_device else torch.device("cuda")
+        off_a = np.arange(n, dtype=np.int64) * L1
+        off_b = n * L1 + np.arange(n, dtype=np.int64) * L2
+        if on_device:
+            pts = torch.cat([a1.reshape(-1, 2), a2.to(dev).reshape(-1, 2)])
+        else:
+            a1 = a1.numpy() if isinstance(a1, torch.Tensor) else a1
+            a2 = a2.numpy() if isinstance(a2, torch.Tensor) else a2
+            pts = np.concatenate([a1.reshape(-1, 2), a2.reshape(-1, 2)])
+    max_len = int(max(la.max(initial=0), lb.max(initial=0)))
+    order = pair_order(la, lb)
+
+    def up(x, dt):
+        if isinstance(x, torch.Tensor):
+            return x.to(dev)
+        return torch.from_numpy(np.ascontiguousarray(x, dtype=dt)).to(dev)
+
+    pts_t = up(pts, np.float32)
+    la_t, lb_t = up(la, np.int32), up(lb, np.int32)
+    out = torch.empty(n, dtype=torch.float32, device=dev)
+    cnt = torch.empty(n, dtype=torch.int32, device=dev) if m in (_lib.EDR, _lib.LCSS) else None
+    pairs_raw(m, pts_t, up(off_a, np.int64), la_t, up(off_b, np.int64), lb_t, max_len, out=out, counts=cnt,
+              order=up(order, np.int32), eps=eps, gpoint=gpoint, exact=exact, rows=rows)
+    if on_device:
+        if cnt is not None:
+            c = cnt.double()
+            lat, lbt = la_t.double(), lb_t.double()
+            res = c / torch.maximum(lat, lbt) if m == _lib.EDR else 1.0 - c / torch.minimum(lat, lbt)
+        else:
+            res = out.double()
+        return (res, cnt) if counts else res
+    if cnt is not None:
+        c_h = cnt.cpu().numpy()
+        res = _normalise_counts(m, c_h, la, lb)
+        return (res, c_h) if counts else res
+    res = out.cpu().numpy().astype(np.float64)
+    return (res, None) if counts else res
+
+
+def dtw(t1, len1, t2, len2, threads_per_traj=64):
+    """core/dtw.py:56-77 (asserts t1.shape == t2.shape as the reference does, :60)."""
+    _check_tpt(threads_per_traj)
+    assert np.shape(t1) == np.shape(t2) if not isinstance(t1, list) else len(t1) == len(t2)
+    return pairs(_lib.DTW, t1, len1, t2, len2)
+
+
+def edr(t1, len1, t2, len2, eps, threads_per_traj=64):
+    """core/edr.py:55-76: count / max(n1, n2), match iff dx^2 + dy^2 < eps^2."""
+    _check_tpt(threads_per_traj)
+    assert len(t1) == len(t2)
+    return pairs(_lib.EDR, t1, len1, t2, len2, eps=eps)
+
+
+def lcss(t1, len1, t2, len2, eps, threads_per_traj=64):
+    """core/lcss.py:56-77: 1 - count / min(n1, n2)."""
+    _check_tpt(threads_per_traj)
+    assert len(t1) == len(t2)
+    return pairs(_lib.LCSS, t1, len1, t2, len2, eps=eps)
+
+
+def _gpoint(gpoint):
+    if gpoint is None:
+        return (0.0, 0.0)  # core/erp.py:103
+    g = np.asarray(gpoint, dtype=np.float64).reshape(-1)
+    if g.shape[0] < 2:
+        raise ValueError("gpoint must have two coordinates")
+    return (float(g[0]), float(g[1]))
+
+
+def erp(t1, len1, t2, len2, gpoint=None, threads_per_traj=64):
+    """core/erp.py:94-120 (gap point default (0, 0))."""
+    _check_tpt(threads_per_traj)
+    assert len(t1) == len(t2)
+    return pairs(_lib.ERP, t1, len1, t2, len2, gpoint=_gpoint(gpoint))
+
+
+def dfrechet(t1, len1, t2, len2, threads_per_traj=64):
+    """core/discret_frechet.py:53-74."""
+    _check_tpt(threads_per_traj)
+    assert len(t1) == len(t2)
+    return pairs(_lib.DFRECHET, t1, len1, t2, len2)
+
+
+def hausdorff(t1, len1, t2, len2, threads_per_traj=64):
+    """core/hausdorff.py:97-123 (max over valid points only)."""
+    _check_tpt(threads_per_traj)
+    assert len(t1) == len(t2)
+    return pairs(_lib.HAUSDORFF, t1, len1, t2, len2)
+
+
+# ---------------------------------------------------------------------------
+# Q x D / all-pairs
+# ---------------------------------------------------------------------------
+
+def _set_of(t, lens, device):
+    if isinstance(t, TrajSet):
+        return t
+    p = _as_points(t)
+    if p is None:
+        trajs = list(t) if lens is None else [np.asarray(x)[:l] for x, l in zip(t, _lens_np(lens, len(t)))]
+        return TrajSet.from_lists(trajs, device=device)
+    a, n, L = p
+    la = _lens_np(lens, n)
+    if isinstance(a, torch.Tensor) and a.is_cuda:
+        off = torch.arange(n, dtype=torch.int64, device=a.device) * L
+        lens_t = torch.as_tensor(la, dtype=torch.int32).to(a.device)
+        return TrajSet(a.reshape(-1, 2), off, lens_t, int(la.max(initial=0)), la.astype(np.int32))
+    a = a.numpy() if isinstance(a, torch.Tensor) else a
+    return TrajSet.from_packed(a.reshape(-1, 2), np.arange(n, dtype=np.int64) * L, la, device=device)
+
+
+def matrix(measure, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False, rows=0, counts=False):
+    """result[i, j] = measure(Q_i, D_j) for all pairs, one launch.
+
+    Q, D: padded arrays/tensors with lengths, lists of trajectories (lengths
+    optional), or TrajSet objects already on the device.  Returns float64
+    [nq, nd] (NumPy for host inputs, CUDA tensor for device inputs)."""
+    m = measure_id(measure)
+    dev = torch.device("cuda")
+    on_device = isinstance(Q, TrajSet) or (isinstance(Q, torch.Tensor) and Q.is_cuda)
+    qs = _set_of(Q, lenQ, dev)
+    ds = _set_of(D, lenD, qs.device)
+    out = torch.empty((qs.n, ds.n), dtype=torch.float32, device=qs.device)
+    cnt = torch.empty((qs.n, ds.n), dtype=torch.int32, device=qs.device) if m in (_lib.EDR, _lib.LCSS) else None
+    matrix_raw(m, qs, ds, out=out, counts=cnt, eps=eps, gpoint=_gpoint(gpoint), exact=exact, rows=rows)
+    lq = qs.lens_host if qs.lens_host is not None else qs.lens.cpu().numpy()
+    ld = ds.lens_host if ds.lens_host is not None else ds.lens.cpu().numpy()
+    if on_device:
+        if cnt is not None:
+            c = cnt.double()
+            a = qs.lens.double()[:, None]
+            b = ds.lens.double()[None, :]
+            res = c / torch.maximum(a, b) if m == _lib.EDR else 1.0 - c / torch.minimum(a, b)
+        else:
+            res = out.double()
+        return (res, cnt) if counts else res
+    if cnt is not None:
+        c_h = cnt.cpu().numpy()
+        res = _normalise_counts(m, c_h, lq.astype(np.int64)[:, None], ld.astype(np.int64)[None, :])
+        return (res, c_h) if counts else res
+    res = out.cpu().numpy().astype(np.float64)
+    return (res, None) if counts else res
+
+
+def matrix_many(measures, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False, rows=0, stream=None):
+    """Several measures over the same Q x D, one upload of each set:
+    {name: float64 [nq, nd] NumPy array}.  Host inputs only (padded arrays
+    with lengths, or lists).  Points go up as float32 from pinned memory; each
+    result comes back once, EDR/LCSS as counts normalised on the host."""
+    dev = torch.device("cuda")
+    qs = _set_of(Q, lenQ, dev)
+    ds = qs if (D is Q and lenD is lenQ) else _set_of(D, lenD, dev)
+    g = _gpoint(gpoint)
+    outs = {}
+    for meas in measures:
+        m = measure_id(meas)
+        out = torch.empty((qs.n, ds.n), dtype=torch.float32, device=dev)
+        cnt = torch.empty((qs.n, ds.n), dtype=torch.int32, device=dev) if m in (_lib.EDR, _lib.LCSS) else None
+        matrix_raw(m, qs, ds, out=out, counts=cnt, eps=eps, gpoint=g, exact=exact, rows=rows, stream=stream)
+        outs[_lib.MEASURE_NAMES[m]] = (out, cnt)
+    lq = qs.lens_host.astype(np.int64)[:, None]
+    ld = ds.lens_host.astype(np.int64)[None, :]
+    res = {}
+    for name, (out, cnt) in outs.items():
+        if cnt is not None:
+            res[name] = _normalise_counts(_lib.MEASURES[name], cnt.cpu().numpy(), lq, ld)
+        else:
+            res[name] = out.cpu().numpy().astype(np.float64)
+    return res
+
+
+def dtw_matrix(Q, lenQ, D, lenD, **kw):
+    return matrix(_lib.DTW, Q, lenQ, D, lenD, **kw)
+
+
+def edr_matrix(Q, lenQ, D, lenD, eps, **kw):
+    return matrix(_lib.EDR, Q, lenQ, D, lenD, eps=eps, **kw)
+
+
+def lcss_matrix(Q, lenQ, D, lenD, eps, **kw):
+    return matrix(_lib.LCSS, Q, lenQ, D, lenD, eps=eps, **kw)
+
+
+def erp_matrix(Q, lenQ, D, lenD, gpoint=None, **kw):
+    return matrix(_lib.ERP, Q, lenQ, D, lenD, gpoint=gpoint, **kw)
+
+
+def dfrechet_matrix(Q, lenQ, D, lenD, **kw):
+    return matrix(_lib.DFRECHET, Q, lenQ, D, lenD, **kw)
+
+
+def hausdorff_matrix(Q, lenQ, D, lenD, **kw):
+    return matrix(_lib.HAUSDORFF, Q, lenQ, D, lenD, **kw)

@@ -1,0 +1,220 @@
+// C ABI of libtsm_b200.so (declarations and contract: include/tsm.h).
+//
+// Host-side launch logic only: argument checks, kernel selection by
+// (measure, rows-per-thread, exact), shared-memory sizing, launch on the
+// caller's stream.  No device allocation happens here.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "tsm.h"
+#include "tsm_tile.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char b[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(b, sizeof(b), fmt, ap);
+    va_end(ap);
+    g_err = b;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(TSM_ECUDA, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+// Longest trajectory the tile kernels keep a boundary row for (points).
+constexpr int kTileCapMax = 1024;
+// Shared memory one CTA may use, leaving room for two CTAs per SM at cap 200.
+constexpr int kSmemPerCta = 113 * 1024;
+constexpr int kSmemMax = 227 * 1024;
+
+tsm::KParams make_kparams(const tsm_params* p) {
+    tsm::KParams k{};
+    const double eps = p ? p->eps : 0.0;
+    const double gx = p ? p->gx : 0.0, gy = p ? p->gy : 0.0;
+    k.eps2 = (float)(eps * eps);
+    k.ghx = (float)gx;
+    k.glx = (float)(gx - (double)k.ghx);
+    k.ghy = (float)gy;
+    k.gly = (float)(gy - (double)k.ghy);
+    return k;
+}
+
+int rows_of(const tsm_params* p) {
+    const int r = p ? p->rows_per_thread : 0;
+    return r == 0 ? 8 : r;
+}
+
+bool exact_of(const tsm_params* p) { return p && (p->flags & TSM_FLAG_EXACT); }
+
+// Warps per CTA for a boundary row of `cap` floats per thread.
+int warps_for(int cap, int extra_bytes) {
+    for (int w = 4; w > 1; --w)
+        if (w * 32 * cap * 4 + extra_bytes <= kSmemPerCta) return w;
+    return 1;
+}
+
+cudaError_t set_smem(const void* fn, int bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+// --- kernel tables -----------------------------------------------------------
+
+template <int M, int R, bool E>
+const void* dp_pairs_fn() {
+    return (const void*)&tsm::dp_pairs_kernel<M, R, E>;
+}
+template <int M, int R, bool E>
+const void* dp_matrix_fn() {
+    return (const void*)&tsm::dp_matrix_kernel<M, R, E>;
+}
+
+template <int M, bool E>
+const void* pick_dp(bool matrix, int R) {
+    switch (R) {
+        case 4: return matrix ? dp_matrix_fn<M, 4, E>() : dp_pairs_fn<M, 4, E>();
+        case 8: return matrix ? dp_matrix_fn<M, 8, E>() : dp_pairs_fn<M, 8, E>();
+        case 16: return matrix ? dp_matrix_fn<M, 16, E>() : dp_pairs_fn<M, 16, E>();
+        default: return nullptr;
+    }
+}
+
+template <bool E>
+const void* pick_dp_m(int measure, bool matrix, int R) {
+    switch (measure) {
+        case TSM_DTW: return pick_dp<tsm::DTW, E>(matrix, R);
+        case TSM_EDR: return pick_dp<tsm::EDR, E>(matrix, R);
+        case TSM_LCSS: return pick_dp<tsm::LCSS, E>(matrix, R);
+        case TSM_ERP: return pick_dp<tsm::ERP, E>(matrix, R);
+        case TSM_DFRECHET: return pick_dp<tsm::DFRECHET, E>(matrix, R);
+        default: return nullptr;
+    }
+}
+
+template <int R, bool E>
+const void* haus_fn(bool matrix) {
+    return matrix ? (const void*)&tsm::hausdorff_matrix_kernel<R, E> : (const void*)&tsm::hausdorff_pairs_kernel<R, E>;
+}
+
+const void* pick_haus(bool matrix, int R, bool exact) {
+    switch (R) {
+        case 4: return exact ? haus_fn<4, true>(matrix) : haus_fn<4, false>(matrix);
+        case 8: return exact ? haus_fn<8, true>(matrix) : haus_fn<8, false>(matrix);
+        case 16: return exact ? haus_fn<16, true>(matrix) : haus_fn<16, false>(matrix);
+        default: return nullptr;
+    }
+}
+
+int launch(const void* fn, dim3 grid, dim3 block, int smem, void** args, cudaStream_t s) {
+    cudaError_t e = set_smem(fn, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    e = cudaLaunchKernel(fn, grid, block, args, (size_t)smem, s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaLaunchKernel");
+    return TSM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tsm_version(void) { return 100; }
+
+const char* tsm_last_error(void) { return g_err.c_str(); }
+
+int32_t tsm_max_supported_len(void) { return kTileCapMax; }
+
+int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t* len_a,
+              const int64_t* off_b, const int32_t* len_b, const int32_t* order, int64_t n_pairs,
+              int32_t max_len, const tsm_params* params, float* out, int32_t* out_counts, void* stream) {
+    g_err.clear();
+    if (measure < TSM_DTW || measure > TSM_HAUSDORFF) return fail(TSM_EINVAL, "tsm_pairs: unknown measure %d", measure);
+    if (n_pairs < 0) return fail(TSM_EINVAL, "tsm_pairs: n_pairs < 0");
+    if (n_pairs == 0) return TSM_OK;
+    if (!pts || !off_a || !len_a || !off_b || !len_b || !out) return fail(TSM_EINVAL, "tsm_pairs: null pointer");
+    if (max_len < 0) return fail(TSM_EINVAL, "tsm_pairs: max_len < 0");
+    const int R = rows_of(params);
+    const bool exact = exact_of(params);
+    cudaStream_t s = (cudaStream_t)stream;
+    const tsm::KParams kp = make_kparams(params);
+    const float2* p2 = reinterpret_cast<const float2*>(pts);
+    int64_t n = n_pairs;
+    int ml = max_len;
+    if (measure == TSM_HAUSDORFF) {
+        const void* fn = pick_haus(false, R, exact);
+        if (!fn) return fail(TSM_EINVAL, "tsm_pairs: rows_per_thread must be 4, 8 or 16");
+        const int threads = 128;
+        dim3 grid((unsigned)((n + threads - 1) / threads));
+        void* args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &ml, &out};
+        return launch(fn, grid, dim3(threads), 0, args, s);
+    }
+    if (max_len > kTileCapMax) return fail(TSM_ETOOLONG, "tsm_pairs: max_len %d > %d", max_len, kTileCapMax);
+    const void* fn = exact ? pick_dp_m<true>(measure, false, R) : pick_dp_m<false>(measure, false, R);
+    if (!fn) return fail(TSM_EINVAL, "tsm_pairs: rows_per_thread must be 4, 8 or 16");
+    int cap = max_len < 1 ? 1 : max_len;
+    const int W = warps_for(cap, 0);
+    const int threads = 32 * W;
+    const int smem = W * 32 * cap * 4;
+    if (smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_pairs: boundary rows need %d bytes", smem);
+    dim3 grid((unsigned)((n + threads - 1) / threads));
+    void* args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &cap, &ml, (void*)&kp, &out, &out_counts};
+    return launch(fn, grid, dim3(threads), smem, args, s);
+}
+
+int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len, int64_t nq,
+               int32_t q_max_len, const float* d_pts, const int64_t* d_off, const int32_t* d_len,
+               const int32_t* d_order, int64_t nd, int32_t d_max_len, const tsm_params* params,
+               float* out, int64_t ld_out, int32_t* out_counts, void* stream) {
+    g_err.clear();
+    if (measure < TSM_DTW || measure > TSM_HAUSDORFF) return fail(TSM_EINVAL, "tsm_matrix: unknown measure %d", measure);
+    if (nq < 0 || nd < 0) return fail(TSM_EINVAL, "tsm_matrix: negative set size");
+    if (nq == 0 || nd == 0) return TSM_OK;
+    if (!q_pts || !q_off || !q_len || !d_pts || !d_off || !d_len || !out)
+        return fail(TSM_EINVAL, "tsm_matrix: null pointer");
+    if (ld_out < nd) return fail(TSM_EINVAL, "tsm_matrix: ld_out < nd");
+    if (q_max_len < 0 || d_max_len < 0) return fail(TSM_EINVAL, "tsm_matrix: max_len < 0");
+    const int R = rows_of(params);
+    const bool exact = exact_of(params);
+    cudaStream_t s = (cudaStream_t)stream;
+    const tsm::KParams kp = make_kparams(params);
+    const float2* q2 = reinterpret_cast<const float2*>(q_pts);
+    const float2* d2 = reinterpret_cast<const float2*>(d_pts);
+    int qcap = q_max_len < 1 ? 1 : q_max_len;
+    int dml = d_max_len;
+    int64_t ndd = nd, ld = ld_out;
+    if (measure == TSM_HAUSDORFF) {
+        const void* fn = pick_haus(true, R, exact);
+        if (!fn) return fail(TSM_EINVAL, "tsm_matrix: rows_per_thread must be 4, 8 or 16");
+        const int smem = qcap * 16;
+        if (smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_matrix: query length %d too long", q_max_len);
+        const int threads = 128;
+        int chunks = (int)((nd + threads - 1) / threads);
+        if ((int64_t)chunks * nq > 0x7fffffffLL) return fail(TSM_EINVAL, "tsm_matrix: grid too large");
+        dim3 grid((unsigned)(chunks * nq));
+        void* args[] = {&q2, &q_off, &q_len, &d2, &d_off, &d_len, &d_order, &ndd, &chunks, &qcap, &dml, &out, &ld};
+        return launch(fn, grid, dim3(threads), smem, args, s);
+    }
+    if (q_max_len > kTileCapMax) return fail(TSM_ETOOLONG, "tsm_matrix: q_max_len %d > %d", q_max_len, kTileCapMax);
+    const void* fn = exact ? pick_dp_m<true>(measure, true, R) : pick_dp_m<false>(measure, true, R);
+    if (!fn) return fail(TSM_EINVAL, "tsm_matrix: rows_per_thread must be 4, 8 or 16");
+    const int W = warps_for(qcap, qcap * 16);
+    const int threads = 32 * W;
+    const int smem = qcap * 16 + W * 32 * qcap * 4;
+    if (smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_matrix: boundary rows need %d bytes", smem);
+    int chunks = (int)((nd + threads - 1) / threads);
+    if ((int64_t)chunks * nq > 0x7fffffffLL) return fail(TSM_EINVAL, "tsm_matrix: grid too large");
+    dim3 grid((unsigned)(chunks * nq));
+    void* args[] = {&q2, &q_off, &q_len, &d2, &d_off, &d_len, &d_order, &ndd, &chunks, &qcap, &dml, (void*)&kp,
+                    &out, &ld, &out_counts};
+    return launch(fn, grid, dim3(threads), smem, args, s);
+}
+
+}  // extern "C"
