@@ -57,7 +57,16 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU work of the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=0, help="rows per thread (0 = library default)")
-    return ap.parse_args()
+    ap.add_argument("--n-traj", type=int, default=N_TRAJ,
+                    help="trajectories per set (smaller cases are for profiling, not bench lines)")
+    ap.add_argument("--measures", default=",".join(MEASURES), help="comma-separated subset of the six measures")
+    ap.add_argument("--flush-mb", type=int, default=256, help="L2 flush buffer written before each step (0: none)")
+    a = ap.parse_args()
+    a.measures = [m for m in a.measures.split(",") if m]
+    for m in a.measures:
+        if m not in MID:
+            ap.error(f"unknown measure {m}")
+    return a
 
 
 def dist_env():
@@ -67,10 +76,10 @@ def dist_env():
     return ws, rank, local
 
 
-def workload_sets(rank):
+def workload_sets(rank, n=N_TRAJ):
     from trajsimimeasures_b200 import datagen as D
-    d = D.trajectory_set(N_TRAJ, seed=D.SEED_DB)
-    q = d if rank == 0 else D.trajectory_set(N_TRAJ, seed=D.SEED_DB + rank)
+    d = D.trajectory_set(n, seed=D.SEED_DB)
+    q = d if rank == 0 else D.trajectory_set(n, seed=D.SEED_DB + rank)
     return q, d
 
 
@@ -231,28 +240,30 @@ def run_ours(args, ws, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    q, d = workload_sets(rank)
+    q, d = workload_sets(rank, args.n_traj)
+    MEAS = args.measures
     qs = TrajSet.from_packed(*q, device=dev)
     ds = TrajSet.from_packed(*d, device=dev)
     order = ds.order_by_length()
     nq, nd = qs.n, ds.n
-    outs = {m: torch.empty((nq, nd), dtype=torch.float32, device=dev) for m in MEASURES}
-    cnts = {m: torch.empty((nq, nd), dtype=torch.int32, device=dev) for m in ("edr", "lcss")}
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    outs = {m: torch.empty((nq, nd), dtype=torch.float32, device=dev) for m in MEAS}
+    cnts = {m: torch.empty((nq, nd), dtype=torch.int32, device=dev) for m in ("edr", "lcss") if m in MEAS}
+    flush = torch.empty(max(args.flush_mb, 1) * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
-    U = {m: units(m, q[2], d[2]) for m in MEASURES}
+    U = {m: units(m, q[2], d[2]) for m in MEAS}
 
     def step(evs=None):
-        for i, m in enumerate(MEASURES):
+        for i, m in enumerate(MEAS):
             if evs is not None:
                 evs[i].record(stream)
             matrix_raw(MID[m], qs, ds, out=outs[m], counts=cnts.get(m), d_order=order, eps=EPS,
                        gpoint=D.BOX_CENTRE, rows=args.rows, stream=stream)
         if evs is not None:
-            evs[len(MEASURES)].record(stream)
+            evs[len(MEAS)].record(stream)
 
     for _ in range(args.warmup):
-        flush.fill_(1.0)
+        if args.flush_mb:
+            flush.fill_(1.0)
         step()
     torch.cuda.synchronize()
     if ws > 1:
@@ -262,16 +273,17 @@ def run_ours(args, ws, rank, local):
     if clk:
         clk.start()
         time.sleep(0.3)
-    per_ms = {m: 0.0 for m in MEASURES}
+    per_ms = {m: 0.0 for m in MEAS}
     step_ms = []
     launches = 0
     for _ in range(args.steps):
-        flush.fill_(1.0)
-        evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(MEASURES) + 1)]
+        if args.flush_mb:
+            flush.fill_(1.0)
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(MEAS) + 1)]
         step(evs)
-        launches += len(MEASURES)
+        launches += len(MEAS)
         torch.cuda.synchronize()
-        for i, m in enumerate(MEASURES):
+        for i, m in enumerate(MEAS):
             per_ms[m] += evs[i].elapsed_time(evs[i + 1])
         step_ms.append(evs[0].elapsed_time(evs[-1]))
     torch.cuda.synchronize()
@@ -293,19 +305,19 @@ def run_ours(args, ws, rank, local):
         Qpad = D.pad(D.unpack(*q))
         lq = q[2].copy()
         Dpad, ld = (Qpad, lq) if rank == 0 else (D.pad(D.unpack(*d)), d[2].copy())
-        core.matrix_many(MEASURES, Qpad, lq, Dpad, ld, eps=EPS, gpoint=D.BOX_CENTRE)  # warm
+        core.matrix_many(MEAS, Qpad, lq, Dpad, ld, eps=EPS, gpoint=D.BOX_CENTRE)  # warm
         torch.cuda.synchronize()
         ts = []
         for _ in range(args.e2e_steps):
             t0 = time.perf_counter()
-            core.matrix_many(MEASURES, Qpad, lq, Dpad, ld, eps=EPS, gpoint=D.BOX_CENTRE)
+            core.matrix_many(MEAS, Qpad, lq, Dpad, ld, eps=EPS, gpoint=D.BOX_CENTRE)
             torch.cuda.synchronize()
             ts.append(time.perf_counter() - t0)
         tt = torch.tensor([sum(ts)], dtype=torch.float64, device=dev)
         if ws > 1:
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         h2d = sum(a.shape[0] * a.shape[1] * 8 + a.shape[0] * 12 for a in ((Qpad,) if Dpad is Qpad else (Qpad, Dpad)))
-        d2h = nq * nd * 4 * len(MEASURES)
+        d2h = nq * nd * 4 * len(MEAS)
         e2e = {"value": ws * units_step * args.e2e_steps / float(tt.item()), "unit": "cells/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": 1e3 * float(tt.item()) / args.e2e_steps,
@@ -318,12 +330,12 @@ def run_ours(args, ws, rank, local):
     max_mhz = (clocks or {}).get("sm_max_mhz") or 1965.0
     peak_ops = sms * 128 * max_mhz * 1e6
     per = {}
-    for m in MEASURES:
+    for m in MEAS:
         sec = per_ms[m] / 1e3
         per[m] = {"units_per_s": U[m] * args.steps / sec, "pairs_per_s": nq * nd * args.steps / sec,
                   "ms": per_ms[m] / args.steps,
                   "fp32_issue_frac": U[m] * args.steps / sec * OPS_PER_UNIT[m] / peak_ops}
-    dom = max(MEASURES, key=lambda m: per_ms[m])
+    dom = max(MEAS, key=lambda m: per_ms[m])
     ach = per[dom]["units_per_s"] * OPS_PER_UNIT[dom]
     roof = {"bound": "fp32-issue", "kernel": f"tsm::dp_matrix_kernel<{dom}>" if dom != "hausdorff"
             else "tsm::hausdorff_matrix_kernel", "achieved": ach / 1e9, "peak": peak_ops / 1e9, "unit": "Gop/s",
@@ -336,8 +348,9 @@ def run_ours(args, ws, rank, local):
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded random walks, Porto-like box)",
-        "config": {"workload": WORKLOAD, "n_traj": N_TRAJ, "lengths": "U{20..200}", "eps_deg": EPS,
-                   "erp_gpoint": list(D.BOX_CENTRE), "l2": "flushed before each step (256 MB write)",
+        "config": {"workload": WORKLOAD if (args.n_traj == N_TRAJ and MEAS == MEASURES)
+                   else f"allpairs_{args.n_traj}x{args.n_traj}_{'+'.join(MEAS)} (profiling case)", "n_traj": args.n_traj, "lengths": "U{20..200}", "eps_deg": EPS,
+                   "erp_gpoint": list(D.BOX_CENTRE), "l2": f"flushed before each step ({args.flush_mb} MB write)" if args.flush_mb else "not flushed",
                    "parallelism": f"weak: one 2000x2000 block per rank x {ws}", "rows_per_thread": args.rows or 8},
         "e2e": e2e, "gpu_launches": launches, "roofline": roof, "clocks": clocks, "per_measure": per,
     }

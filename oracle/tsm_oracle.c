@@ -397,9 +397,13 @@ static float directed_f32(const float* a, int n1, const float* b, int n2) {
     for (int i = 0; i < n1; ++i) {
         float px = a[2 * i], py = a[2 * i + 1];
         float best = INFINITY;
-        for (int k = 0; k + 1 < n2; ++k) {
+        /* the n2-1 segments, then the last vertex as a zero-length segment
+         * (never below the last segment's distance in exact arithmetic; makes
+         * a point equal to that vertex exactly 0 in FP32) */
+        for (int k = 0; k < n2; ++k) {
+            int k2 = (k + 1 < n2) ? k + 1 : k;
             float s1x = b[2 * k], s1y = b[2 * k + 1];
-            float sx = b[2 * k + 2] - s1x, sy = b[2 * k + 3] - s1y;
+            float sx = b[2 * k2] - s1x, sy = b[2 * k2 + 1] - s1y;
             float len2 = fmaf(sy, sy, sx * sx);
             float inv = (sx == 0.0f && sy == 0.0f) ? 0.0f : 1.0f / len2;
             float d = p2s_f32(px, py, s1x, s1y, sx, sy, inv);

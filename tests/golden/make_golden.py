@@ -3,7 +3,7 @@
 Run in a checkout that has the reference at /root/reference (or
 TSM_REFERENCE_ROOT) -- it is not needed afterwards:
 
-    NUMBA_ENABLE_CUDASIM=1 python tests/golden/make_golden.py
+    NUMBA_ENABLE_CUDASIM=1 python tests/golden/make_golden.py [--force]
 
 For each case it runs
   * the reference GPU kernels of core/*.py (dtw, edr, lcss, erp, dfrechet
@@ -58,6 +58,10 @@ def ref_hausdorff(t1, l1, t2, l2):
 
 
 def run_case(name, trajs_a, trajs_b, eps, gpoint):
+    path = os.path.join(HERE, f"{name}.npz")
+    if os.path.exists(path) and "--force" not in sys.argv:
+        print(f"{path}: exists (--force regenerates)")
+        return
     n = len(trajs_a)
     l1 = np.array([len(t) for t in trajs_a], dtype=np.int64)
     l2 = np.array([len(t) for t in trajs_b], dtype=np.int64)
@@ -68,7 +72,12 @@ def run_case(name, trajs_a, trajs_b, eps, gpoint):
     out["dtw"] = refcore.dtw(t1, l1, t2, l2, threads_per_traj=TPT)
     out["edr"] = refcore.edr(t1, l1, t2, l2, eps, threads_per_traj=TPT)
     out["lcss"] = refcore.lcss(t1, l1, t2, l2, eps, threads_per_traj=TPT)
-    out["erp"] = refcore.erp(t1, l1, t2, l2, list(gpoint), threads_per_traj=TPT)
+    # core/erp.py sizes gpdists_g by max(len2) only (:106,:112) but writes
+    # len1 entries into it (:32-34): a trailing dummy pair with len2 = width
+    # keeps the reference in bounds; its output is dropped.
+    t1e = np.concatenate([t1, np.zeros((1, w, 2))])
+    t2e = np.concatenate([t2, np.zeros((1, w, 2))])
+    out["erp"] = refcore.erp(t1e, np.append(l1, 1), t2e, np.append(l2, w), list(gpoint), threads_per_traj=TPT)[:n]
     out["dfrechet"] = refcore.dfrechet(t1, l1, t2, l2, threads_per_traj=TPT)
     out["hausdorff"] = ref_hausdorff(t1, l1, t2, l2)
     pts, off, lens = pack_lists(list(trajs_a) + list(trajs_b))
@@ -79,7 +88,6 @@ def run_case(name, trajs_a, trajs_b, eps, gpoint):
     for m, key in ((O.DTW, "dtw"), (O.ERP, "erp"), (O.DFRECHET, "dfrechet"), (O.HAUSDORFF, "hausdorff")):
         cpp["cpp_" + key] = rs.pairs(m, ia, ib, gpoint=gpoint).astype(np.float64)
     rs.close()
-    path = os.path.join(HERE, f"{name}.npz")
     np.savez_compressed(path, pts=pts, off=off, lens=lens, ia=ia, ib=ib, eps=np.float64(eps),
                         gpoint=np.asarray(gpoint, np.float64), **out, **cpp)
     print(f"{path}: {n} pairs, lengths {lens.min()}..{lens.max()}")
@@ -101,7 +109,7 @@ def main():
     run_case("walks_near", [t[i] for i in ia], [t[i] for i in ib], G.EPS_DEG, G.BOX_CENTRE)
     # 3. identical and reversed trajectories
     base = G.unpack(*G.trajectory_set(8, 3, 25, seed=99))
-    run_case("walks_self", base + base[:4], base + [b[::-1].copy() for b in base[4:]] + base[:4][::-1],
+    run_case("walks_self", base + base[:4], base[:4] + [b[::-1].copy() for b in base[4:]] + base[4:],
              G.EPS_DEG, G.BOX_CENTRE)
     # 4. the reference's own synthetic distribution (DatasetSynthetic: uniform
     #    [0,1]^2 points, utilities/data_loader.py:114-144), float32 values

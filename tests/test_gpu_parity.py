@@ -211,3 +211,40 @@ def test_full_size_all_pairs_properties(oracle_mod, full_set, m):
         np.testing.assert_array_equal(cnt.cpu().numpy()[rows], c64)
     else:
         assert rel_err(M[rows], d64).max() <= REL_TOL
+
+
+@pytest.mark.parametrize("rows", [4, 8, 16])
+def test_long_pairs_wave_kernel_exact(oracle_mod, rows):
+    """Pairs whose shorter side exceeds the tile kernel's boundary row
+    (256 points) run one warp per pair; mixed in one batch with short pairs."""
+    O = oracle_mod
+    from trajsimimeasures_b200 import datagen as D
+    la = np.array([257, 300, 513, 1000, 2000, 2000, 40, 700, 256, 999, 1, 2000])
+    lb = np.array([300, 257, 600, 1000, 2000, 31, 2000, 1500, 257, 1001, 2000, 1999])
+    pts, off, lens = D._walks(np.random.default_rng(rows), np.concatenate([la, lb]), D.STEP_SIGMA)
+    n = len(la)
+    ia, ib = np.arange(n), np.arange(n) + n
+    for m in (0, 1, 2, 3, 4):
+        got, cnt = run_pairs(m, pts, off, lens, ia, ib, exact=True, rows=rows)
+        want, wcnt = O.pairs_idx(O.pairs_f32, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+        np.testing.assert_array_equal(got, want, err_msg=NAMES[m])
+        if m in (1, 2):
+            np.testing.assert_array_equal(cnt, wcnt)
+
+
+def test_lognormal_batch(oracle_mod):
+    """20k pairs of the uneven (lognormal, clipped to [10, 2000]) workload."""
+    O = oracle_mod
+    from trajsimimeasures_b200 import datagen as D
+    pts, off, lens, ia, ib = D.pairs_lognormal(20_000, seed=4)
+    assert np.minimum(lens[ia], lens[ib]).max() > 256  # the wave kernel runs too
+    for m in MEAS:
+        got, cnt = run_pairs(m, pts, off, lens, ia, ib, exact=True)
+        want, wcnt = O.pairs_idx(O.pairs_f32, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+        np.testing.assert_array_equal(got, want, err_msg=NAMES[m])
+        got, cnt = run_pairs(m, pts, off, lens, ia, ib)
+        d64, c64 = O.pairs_idx(O.pairs_f64, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+        if m in (1, 2):
+            np.testing.assert_array_equal(cnt, wcnt)
+        else:
+            assert rel_err(got, d64).max() <= REL_TOL, NAMES[m]

@@ -42,13 +42,15 @@ def test_f64_oracle_matches_reference_kernels(case, oracle_mod, name, m):
 @pytest.mark.parametrize("name,m", [("dtw", 0), ("erp", 3), ("dfrechet", 4), ("hausdorff", 5)])
 def test_f64_oracle_matches_reference_cpp(case, oracle_mod, name, m):
     """FP64 restatement vs the reference's C++ Traj measures (FP32 arithmetic,
-    FP32 gap point for ERP; its Hausdorff rebuilds the foot point in absolute
-    FP32 coordinates, so it only agrees to ~1e-3 there)."""
+    FP32 gap point for ERP).  Its Hausdorff rebuilds the foot point in absolute
+    FP32 coordinates (traj.cpp:116-118): ~1e-6 deg of absolute error, which on
+    near pairs (distances ~1e-4 deg) is ~1e-2 relative.  Hausdorff is pinned by
+    the reference kernels instead (test above)."""
     O = oracle_mod
     ok = np.minimum(case["lens"][case["ia"]], case["lens"][case["ib"]]) >= 2  # C++ needs edges
     d64, _ = O.pairs_idx(O.pairs_f64, m, case["pts"], case["off"], case["lens"], case["ia"], case["ib"],
                          eps=float(case["eps"]), gpoint=tuple(case["gpoint"]))
-    tol = {0: 1e-5, 4: 1e-6, 3: 2e-4, 5: 5e-3}[m]
+    tol = {0: 1e-5, 4: 1e-6, 3: 2e-4, 5: 3e-2}[m]
     r = rel_err(case["cpp_" + name][ok], d64[ok])
     assert r.max() <= tol, (name, r.max())
 

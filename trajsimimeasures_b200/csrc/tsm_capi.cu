@@ -11,6 +11,7 @@
 
 #include "tsm.h"
 #include "tsm_tile.cuh"
+#include "tsm_wave.cuh"
 
 namespace {
 
@@ -30,8 +31,16 @@ int cuda_fail(cudaError_t e, const char* what) {
     return fail(TSM_ECUDA, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
 }
 
-// Longest trajectory the tile kernels keep a boundary row for (points).
-constexpr int kTileCapMax = 1024;
+// Pairs mode: pairs whose shorter trajectory has at most kTileCap points run
+// on the tile kernel (one thread per pair, a kTileCap-float boundary row per
+// thread); longer ones on the wave kernel (one warp per pair).
+constexpr int kTileCap = 256;
+// Matrix mode keeps the query as the tile kernel's columns: its boundary
+// rows (32 per warp) and staged columns must fit one CTA's shared memory.
+constexpr int kMatrixQueryMax = 1400;
+// Longest trajectory accepted (wave kernel: 20 bytes of shared memory per
+// column point and warp).
+constexpr int kMaxLen = 8192;
 // Shared memory one CTA may use, leaving room for two CTAs per SM at cap 200.
 constexpr int kSmemPerCta = 113 * 1024;
 constexpr int kSmemMax = 227 * 1024;
@@ -76,6 +85,33 @@ const void* dp_pairs_fn() {
 template <int M, int R, bool E>
 const void* dp_matrix_fn() {
     return (const void*)&tsm::dp_matrix_kernel<M, R, E>;
+}
+
+template <int M, int R, bool E>
+const void* dp_wave_fn() {
+    return (const void*)&tsm::dp_wave_kernel<M, R, E>;
+}
+
+template <int M, bool E>
+const void* pick_wave(int R) {
+    switch (R) {
+        case 4: return dp_wave_fn<M, 4, E>();
+        case 8: return dp_wave_fn<M, 8, E>();
+        case 16: return dp_wave_fn<M, 16, E>();
+        default: return nullptr;
+    }
+}
+
+template <bool E>
+const void* pick_wave_m(int measure, int R) {
+    switch (measure) {
+        case TSM_DTW: return pick_wave<tsm::DTW, E>(R);
+        case TSM_EDR: return pick_wave<tsm::EDR, E>(R);
+        case TSM_LCSS: return pick_wave<tsm::LCSS, E>(R);
+        case TSM_ERP: return pick_wave<tsm::ERP, E>(R);
+        case TSM_DFRECHET: return pick_wave<tsm::DFRECHET, E>(R);
+        default: return nullptr;
+    }
 }
 
 template <int M, bool E>
@@ -130,7 +166,7 @@ int tsm_version(void) { return 100; }
 
 const char* tsm_last_error(void) { return g_err.c_str(); }
 
-int32_t tsm_max_supported_len(void) { return kTileCapMax; }
+int32_t tsm_max_supported_len(void) { return kMaxLen; }
 
 int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t* len_a,
               const int64_t* off_b, const int32_t* len_b, const int32_t* order, int64_t n_pairs,
@@ -156,17 +192,32 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
         void* args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &ml, &out};
         return launch(fn, grid, dim3(threads), 0, args, s);
     }
-    if (max_len > kTileCapMax) return fail(TSM_ETOOLONG, "tsm_pairs: max_len %d > %d", max_len, kTileCapMax);
+    if (max_len > kMaxLen) return fail(TSM_ETOOLONG, "tsm_pairs: max_len %d > %d", max_len, kMaxLen);
     const void* fn = exact ? pick_dp_m<true>(measure, false, R) : pick_dp_m<false>(measure, false, R);
     if (!fn) return fail(TSM_EINVAL, "tsm_pairs: rows_per_thread must be 4, 8 or 16");
-    int cap = max_len < 1 ? 1 : max_len;
-    const int W = warps_for(cap, 0);
-    const int threads = 32 * W;
-    const int smem = W * 32 * cap * 4;
-    if (smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_pairs: boundary rows need %d bytes", smem);
-    dim3 grid((unsigned)((n + threads - 1) / threads));
-    void* args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &cap, &ml, (void*)&kp, &out, &out_counts};
-    return launch(fn, grid, dim3(threads), smem, args, s);
+    int cap = max_len < 1 ? 1 : (max_len < kTileCap ? max_len : kTileCap);
+    {
+        const int W = warps_for(cap, 0);
+        const int threads = 32 * W;
+        const int smem = W * 32 * cap * 4;
+        dim3 grid((unsigned)((n + threads - 1) / threads));
+        void* args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &cap, &ml, (void*)&kp, &out, &out_counts};
+        int rc = launch(fn, grid, dim3(threads), smem, args, s);
+        if (rc != TSM_OK) return rc;
+    }
+    if (max_len <= cap) return TSM_OK;
+    // pairs whose shorter side exceeds cap: one warp each
+    const void* wfn = exact ? pick_wave_m<true>(measure, R) : pick_wave_m<false>(measure, R);
+    int wcap = (max_len + 3) & ~3;
+    const int per_warp = tsm::wave_warp_floats(wcap) * 4;
+    int W = (kSmemPerCta / per_warp) < 1 ? 1 : (kSmemPerCta / per_warp);
+    if (W > 4) W = 4;
+    const int smem = W * per_warp;
+    if (smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_pairs: wave kernel needs %d bytes", smem);
+    dim3 grid((unsigned)((n + W - 1) / W));
+    int tcap = cap;
+    void* args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &tcap, &wcap, &ml, (void*)&kp, &out, &out_counts};
+    return launch(wfn, grid, dim3(32 * W), smem, args, s);
 }
 
 int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len, int64_t nq,
@@ -202,7 +253,8 @@ int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int3
         void* args[] = {&q2, &q_off, &q_len, &d2, &d_off, &d_len, &d_order, &ndd, &chunks, &qcap, &dml, &out, &ld};
         return launch(fn, grid, dim3(threads), smem, args, s);
     }
-    if (q_max_len > kTileCapMax) return fail(TSM_ETOOLONG, "tsm_matrix: q_max_len %d > %d", q_max_len, kTileCapMax);
+    if (q_max_len > kMatrixQueryMax)
+        return fail(TSM_ETOOLONG, "tsm_matrix: q_max_len %d > %d (use the pairs form)", q_max_len, kMatrixQueryMax);
     const void* fn = exact ? pick_dp_m<true>(measure, true, R) : pick_dp_m<false>(measure, true, R);
     if (!fn) return fail(TSM_EINVAL, "tsm_matrix: rows_per_thread must be 4, 8 or 16");
     const int W = warps_for(qcap, qcap * 16);

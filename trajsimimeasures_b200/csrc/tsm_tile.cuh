@@ -228,6 +228,12 @@ __device__ __forceinline__ float p2s(float px, float py, float s1x, float s1y, f
 
 // max over the points of P of (min over the segments of T): hausdorff.py:48-69
 // per point, then the max of the host reduction at :121 over valid points.
+// The loop also visits T's last vertex as a zero-length segment (k = nt-1).
+// In exact arithmetic that distance is never below the last segment's, so
+// the min is the reference's; in FP32 it makes a point that coincides with
+// the last vertex come out exactly 0 (u = dot * (1/len2) can round to 1-ulp,
+// leaving a ~1e-11 residue), as every other vertex already does as the
+// first endpoint of its outgoing segment.
 template <int R, bool EXACT, class Segs>
 __device__ __forceinline__ float directed_max(const float2* __restrict__ P, int np, const Segs& T, int nt) {
     if (nt < 2 || np <= 0) return 0.f;  // p2t_dist over zero segments is 0.0
@@ -243,7 +249,7 @@ __device__ __forceinline__ float directed_max(const float2* __restrict__ P, int 
         }
         float2 s1 = T.pt(0);
         float2 s2n = T.pt(1);
-        for (int k = 0; k + 1 < nt; ++k) {
+        for (int k = 0; k < nt; ++k) {  // nt-1 segments + the last vertex
             const float2 s2 = s2n;
             s2n = T.pt(min(k + 2, nt - 1));
             const float sx = __fsub_rn(s2.x, s1.x), sy = __fsub_rn(s2.y, s1.y);
