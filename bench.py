@@ -351,7 +351,7 @@ def run_ours(args, ws, rank, local):
         "config": {"workload": WORKLOAD if (args.n_traj == N_TRAJ and MEAS == MEASURES)
                    else f"allpairs_{args.n_traj}x{args.n_traj}_{'+'.join(MEAS)} (profiling case)", "n_traj": args.n_traj, "lengths": "U{20..200}", "eps_deg": EPS,
                    "erp_gpoint": list(D.BOX_CENTRE), "l2": f"flushed before each step ({args.flush_mb} MB write)" if args.flush_mb else "not flushed",
-                   "parallelism": f"weak: one 2000x2000 block per rank x {ws}", "rows_per_thread": args.rows or 8},
+                   "parallelism": f"weak: one 2000x2000 block per rank x {ws}", "rows_per_thread": args.rows or "default (8; hausdorff 16)"},
         "e2e": e2e, "gpu_launches": launches, "roofline": roof, "clocks": clocks, "per_measure": per,
     }
     if not args.no_cpu_baseline:

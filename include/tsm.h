@@ -113,6 +113,47 @@ int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int3
                const int32_t* d_order, int64_t nd, int32_t d_max_len, const tsm_params* params,
                float* out, int64_t ld_out, int32_t* out_counts, void* stream);
 
+/*
+ * Scheduled paired batch: one persistent launch over a task list that the
+ * planner (trajsimimeasures_b200.sched) builds from the pair lengths.  It
+ * replaces the same reference call as tsm_pairs (core.<measure>(t1, len1,
+ * t2, len2), batched 512 pairs at a time by test_trajsimi_time.py:222-276),
+ * for batches of very uneven lengths and several measures at once.
+ *   tasks      device int32 [n_tasks][4] = {kind, measure, first, count}:
+ *              pairs order[first .. first+count) as one warp task; kind 0 =
+ *              one pair per lane, 1 = one pair per 8 lanes, 2 = one pair per
+ *              warp, 3 = Hausdorff one pair per lane, 4 = Hausdorff one pair
+ *              per warp.  Sorted by the caller, largest first.
+ *   warp_smem_floats  shared memory per warp (floats): the tile capacity is
+ *              warp_smem_floats/32 columns, the 8-lane capacity /4, the
+ *              one-warp capacity warp_smem_floats; tasks must respect them
+ *   out        float32 [n_measures_used][out_stride]: out[measure*out_stride + pair]
+ *   out_counts int32, same layout (EDR/LCSS), or NULL
+ *   workspace  device memory of tsm_sched_workspace_bytes() bytes, zeroed
+ *              once by the caller before its first use; the kernel leaves it
+ *              zeroed again at exit (a task queue head and an exit count).
+ *              Launches that share a workspace must not overlap.
+ */
+int tsm_sched_workspace_bytes(void);
+
+int tsm_pairs_sched(const float* pts, const int64_t* off_a, const int32_t* len_a, const int64_t* off_b,
+                    const int32_t* len_b, const int32_t* order, const int32_t* tasks, int32_t n_tasks,
+                    int32_t max_len, int32_t warp_smem_floats, const tsm_params* params, float* out,
+                    int32_t* out_counts, int64_t out_stride, void* workspace, void* stream);
+
+/*
+ * Row-wise k smallest (kNN result lists): for each row r < n_rows of the
+ * float32 matrix d (row stride ld), the k smallest values in ascending order,
+ * ties to the smaller column index (= the first k entries of a stable argsort;
+ * NaN after +inf).  out_d float32 [n_rows][k], out_idx int32 [n_rows][k];
+ * rows shorter than k are padded with +inf / -1.  k <= 256.
+ * The reference's kNN answers queries with CPU index pruning
+ * (query/cpp/DITA.cpp:276-431, DFT.cpp:89-230: std::nth_element over refined
+ * candidates); this is the selection step of the exhaustive GPU replacement.
+ */
+int tsm_topk_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, int32_t k, float* out_d,
+                  int32_t* out_idx, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -137,3 +137,43 @@ def test_collate_pads_jointly():
     assert l1 == [3, 1] and l2 == [1, 2]
     u1, ul1, u2, ul2 = mh.heuristic_colllate_fn(batch, False)
     assert ul1 == [3, 1] and len(u1) == 2
+
+
+def test_sched_plan_covers_every_item_once():
+    from trajsimimeasures_b200 import datagen as D, sched
+    _, _, lens, ia, ib = D.pairs_lognormal(20_000, seed=2)
+    la, lb = lens[ia], lens[ib]
+    for rows, wf in [(8, 4096), (4, 2048), (8, 8192)]:
+        pl = sched.plan_pairs(la, lb, ["dtw", "dfrechet", "edr", "hausdorff"], rows=rows, warp_floats=wf)
+        t = pl.tasks
+        assert t.dtype == np.int32 and t.shape[1] == 4
+        assert np.all(np.diff(pl.cost) <= 0)  # largest first
+        nc = np.minimum(la, lb)
+        seen = {m: np.zeros(len(la), np.int64) for m in (0, 4, 1, 5)}
+        for kind, m, first, cnt in t:
+            idx = pl.order[first:first + cnt]
+            seen[m][idx] += 1
+            cap = {0: wf // 32, 1: wf // 4, 2: wf, 3: 1 << 30, 4: 1 << 30}[kind]
+            assert cnt <= {0: 32, 1: 4, 2: 1, 3: 32, 4: 1}[kind]
+            assert nc[idx].max() <= cap
+            assert (kind in (3, 4)) == (m == 5)
+        for m, v in seen.items():
+            assert np.all(v == 1), m
+
+
+def test_sched_plan_rejects_pairs_beyond_capacity():
+    from trajsimimeasures_b200 import sched
+    with pytest.raises(ValueError):
+        sched.plan_pairs([5000], [5000], ["dtw"], warp_floats=4096)
+    pl = sched.plan_pairs([5000], [5000], ["hausdorff"], warp_floats=4096)  # no shared memory needed
+    assert pl.n_tasks == 1
+
+
+def test_autotune_signature_and_cache(tmp_path, monkeypatch):
+    from trajsimimeasures_b200 import sched
+    monkeypatch.setenv("TSM_CACHE_DIR", str(tmp_path))
+    a = sched.signature([10, 20, 300], [40, 50, 60], ["dtw", "edr"])
+    b = sched.signature([10, 20, 300], [40, 50, 60], ["edr", "dtw"])
+    assert a == b
+    sched.save_cache({"k": {"best": [8, 4096]}})
+    assert sched.load_cache()["k"]["best"] == [8, 4096]

@@ -1,0 +1,60 @@
+"""GPU tests of the kNN selection (tsm_topk_rows) and the kNN drivers."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _stable_topk(a, k):
+    o = np.argsort(a, axis=1, kind="stable")[:, :k]
+    return np.take_along_axis(a, o, axis=1), o
+
+
+@pytest.mark.parametrize("k", [1, 10, 64, 256])
+def test_topk_rows_matches_stable_argsort(k):
+    from trajsimimeasures_b200.knn import topk_rows
+    rng = np.random.default_rng(k)
+    a = rng.random((37, 5000)).astype(np.float32)
+    a[:, ::7] = np.round(a[:, ::7], 2)  # many ties
+    a[0, :] = 0.5                     # a row of equal values
+    a[1, 100:200] = np.inf
+    a[2, 5] = np.nan
+    a[3, :50] = -1.0 - a[3, :50]        # negative values
+    v, i = topk_rows(torch.from_numpy(a).cuda(), k)
+    wv, wi = _stable_topk(a, k)
+    np.testing.assert_array_equal(i.cpu().numpy(), wi)
+    np.testing.assert_array_equal(v.cpu().numpy(), wv)
+
+
+def test_topk_rows_short_rows_are_padded():
+    from trajsimimeasures_b200.knn import topk_rows
+    a = torch.tensor([[3.0, 1.0, 2.0]], device="cuda")
+    v, i = topk_rows(a, 5)
+    assert i.cpu().tolist() == [[1, 2, 0, -1, -1]]
+    assert v.cpu().numpy()[0, 3] == np.inf
+
+
+def test_knn_exhaustive_and_rerank(oracle_mod):
+    O = oracle_mod
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.engine import TrajSet
+    from trajsimimeasures_b200.knn import knn_exhaustive, knn_rerank, recall_at_k
+    qp, qo, ql = D.trajectory_set(12, seed=D.SEED_QUERY)
+    dp, do, dl = D.trajectory_set(3000)
+    Q, Dset = TrajSet.from_packed(qp, qo, ql), TrajSet.from_packed(dp, do, dl)
+    want, _ = O.matrix_idx(O.pairs_f32, 0, qp, qo, ql, dp, do, dl)
+    wv, wi = _stable_topk(want, 10)
+    v, i = knn_exhaustive(Q, Dset, k=10, chunk=700, exact=True)  # several chunks, merged
+    np.testing.assert_array_equal(i.cpu().numpy(), wi)
+    np.testing.assert_array_equal(v.cpu().numpy(), wv)
+    # rerank from a candidate superset that contains the answer
+    rng = np.random.default_rng(0)
+    cand = np.stack([np.concatenate([wi[q], rng.choice(3000, 190, replace=False)]) for q in range(12)])
+    cand = np.array([np.unique(c)[:200] if len(np.unique(c)) >= 200 else np.unique(c) for c in cand], dtype=object)
+    width = min(len(c) for c in cand)
+    cand = np.stack([np.concatenate([wi[q], np.setdiff1d(c, wi[q])])[:width] for q, c in enumerate(cand)])
+    rv, ri = knn_rerank(Q, Dset, torch.from_numpy(cand).cuda(), k=10, exact=True)
+    np.testing.assert_array_equal(ri.cpu().numpy(), wi)
+    np.testing.assert_array_equal(rv.cpu().numpy(), wv)
+    assert recall_at_k(ri, i) == 1.0

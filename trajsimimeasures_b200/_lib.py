@@ -19,7 +19,8 @@ MEASURE_NAMES = {DTW: "dtw", EDR: "edr", LCSS: "lcss", ERP: "erp", DFRECHET: "df
 FLAG_EXACT = 1
 
 # Every symbol include/tsm.h declares (checked by the test suite).
-EXPORTS = ("tsm_version", "tsm_last_error", "tsm_max_supported_len", "tsm_pairs", "tsm_matrix")
+EXPORTS = ("tsm_version", "tsm_last_error", "tsm_max_supported_len", "tsm_pairs", "tsm_matrix",
+           "tsm_sched_workspace_bytes", "tsm_pairs_sched", "tsm_topk_rows")
 
 
 class TsmParams(ctypes.Structure):
@@ -58,6 +59,12 @@ def load():
         lib.tsm_matrix.restype = ctypes.c_int
         lib.tsm_matrix.argtypes = [ctypes.c_int, _vp, _vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _i64, _i32,
                                    ctypes.POINTER(TsmParams), _vp, _i64, _vp, _vp]
+        lib.tsm_sched_workspace_bytes.restype = ctypes.c_int
+        lib.tsm_pairs_sched.restype = ctypes.c_int
+        lib.tsm_pairs_sched.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32,
+                                        ctypes.POINTER(TsmParams), _vp, _vp, _i64, _vp, _vp]
+        lib.tsm_topk_rows.restype = ctypes.c_int
+        lib.tsm_topk_rows.argtypes = [_vp, _i64, _i64, _i64, _i32, _vp, _vp, _vp]
         _lib = lib
     return _lib
 

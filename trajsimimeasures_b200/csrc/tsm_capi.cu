@@ -12,6 +12,8 @@
 #include "tsm.h"
 #include "tsm_tile.cuh"
 #include "tsm_wave.cuh"
+#include "tsm_sched.cuh"
+#include "tsm_topk.cuh"
 
 namespace {
 
@@ -57,9 +59,11 @@ tsm::KParams make_kparams(const tsm_params* p) {
     return k;
 }
 
-int rows_of(const tsm_params* p) {
+// Default rows per thread block: 8 for the DP measures (two packed 8-row
+// blocks per pass), 16 for Hausdorff (amortises the per-segment setup).
+int rows_of(const tsm_params* p, int measure = TSM_DTW) {
     const int r = p ? p->rows_per_thread : 0;
-    return r == 0 ? 8 : r;
+    return r == 0 ? (measure == TSM_HAUSDORFF ? 16 : 8) : r;
 }
 
 bool exact_of(const tsm_params* p) { return p && (p->flags & TSM_FLAG_EXACT); }
@@ -177,7 +181,7 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
     if (n_pairs == 0) return TSM_OK;
     if (!pts || !off_a || !len_a || !off_b || !len_b || !out) return fail(TSM_EINVAL, "tsm_pairs: null pointer");
     if (max_len < 0) return fail(TSM_EINVAL, "tsm_pairs: max_len < 0");
-    const int R = rows_of(params);
+    const int R = rows_of(params, measure);
     const bool exact = exact_of(params);
     cudaStream_t s = (cudaStream_t)stream;
     const tsm::KParams kp = make_kparams(params);
@@ -232,7 +236,7 @@ int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int3
         return fail(TSM_EINVAL, "tsm_matrix: null pointer");
     if (ld_out < nd) return fail(TSM_EINVAL, "tsm_matrix: ld_out < nd");
     if (q_max_len < 0 || d_max_len < 0) return fail(TSM_EINVAL, "tsm_matrix: max_len < 0");
-    const int R = rows_of(params);
+    const int R = rows_of(params, measure);
     const bool exact = exact_of(params);
     cudaStream_t s = (cudaStream_t)stream;
     const tsm::KParams kp = make_kparams(params);
@@ -244,7 +248,7 @@ int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int3
     if (measure == TSM_HAUSDORFF) {
         const void* fn = pick_haus(true, R, exact);
         if (!fn) return fail(TSM_EINVAL, "tsm_matrix: rows_per_thread must be 4, 8 or 16");
-        const int smem = qcap * 16;
+        const int smem = qcap * 20;
         if (smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_matrix: query length %d too long", q_max_len);
         const int threads = 128;
         int chunks = (int)((nd + threads - 1) / threads);
@@ -267,6 +271,80 @@ int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int3
     void* args[] = {&q2, &q_off, &q_len, &d2, &d_off, &d_len, &d_order, &ndd, &chunks, &qcap, &dml, (void*)&kp,
                     &out, &ld, &out_counts};
     return launch(fn, grid, dim3(threads), smem, args, s);
+}
+
+int tsm_topk_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, int32_t k, float* out_d,
+                  int32_t* out_idx, void* stream) {
+    g_err.clear();
+    if (n_rows < 0 || n_cols < 0) return fail(TSM_EINVAL, "tsm_topk_rows: negative size");
+    if (k < 1 || k > tsm::kTopkMax) return fail(TSM_EINVAL, "tsm_topk_rows: k must be in 1..%d", tsm::kTopkMax);
+    if (n_rows == 0) return TSM_OK;
+    if (n_rows > 0x7fffffffLL) return fail(TSM_EINVAL, "tsm_topk_rows: too many rows");
+    if (n_cols > 0x7fffffffLL) return fail(TSM_EINVAL, "tsm_topk_rows: column index exceeds int32");
+    if (!d || !out_d || !out_idx) return fail(TSM_EINVAL, "tsm_topk_rows: null pointer");
+    if (ld < n_cols) return fail(TSM_EINVAL, "tsm_topk_rows: ld < n_cols");
+    tsm::topk_rows_kernel<<<(unsigned)n_rows, tsm::kTopkThreads, 0, (cudaStream_t)stream>>>(d, n_cols, ld, k, out_d,
+                                                                                              out_idx);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "topk_rows_kernel launch");
+    return TSM_OK;
+}
+
+int tsm_sched_workspace_bytes(void) { return 256; }
+
+int tsm_pairs_sched(const float* pts, const int64_t* off_a, const int32_t* len_a, const int64_t* off_b,
+                    const int32_t* len_b, const int32_t* order, const int32_t* tasks, int32_t n_tasks,
+                    int32_t max_len, int32_t warp_smem_floats, const tsm_params* params, float* out,
+                    int32_t* out_counts, int64_t out_stride, void* workspace, void* stream) {
+    g_err.clear();
+    if (n_tasks < 0) return fail(TSM_EINVAL, "tsm_pairs_sched: n_tasks < 0");
+    if (n_tasks == 0) return TSM_OK;
+    if (!pts || !off_a || !len_a || !off_b || !len_b || !order || !tasks || !out || !workspace)
+        return fail(TSM_EINVAL, "tsm_pairs_sched: null pointer");
+    if (max_len < 0 || max_len > kMaxLen) return fail(TSM_EINVAL, "tsm_pairs_sched: max_len out of range");
+    if (warp_smem_floats < 32 || warp_smem_floats % 32 != 0)
+        return fail(TSM_EINVAL, "tsm_pairs_sched: warp_smem_floats must be a positive multiple of 32");
+    if (out_stride < 0) return fail(TSM_EINVAL, "tsm_pairs_sched: out_stride < 0");
+    const int R = rows_of(params);
+    const bool exact = exact_of(params);
+    const void* fn = nullptr;
+    if (R == 4) fn = exact ? (const void*)&tsm::dp_sched_kernel<4, true> : (const void*)&tsm::dp_sched_kernel<4, false>;
+    else if (R == 8) fn = exact ? (const void*)&tsm::dp_sched_kernel<8, true> : (const void*)&tsm::dp_sched_kernel<8, false>;
+    else return fail(TSM_EINVAL, "tsm_pairs_sched: rows_per_thread must be 4 or 8");
+    const int W = 4;
+    const int smem = W * warp_smem_floats * 4;
+    if (smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_pairs_sched: %d bytes of shared memory per CTA", smem);
+    cudaError_t e = set_smem(fn, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaDeviceGetAttribute");
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * W, smem)) != cudaSuccess)
+        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per_sm < 1) return fail(TSM_ETOOLONG, "tsm_pairs_sched: the kernel does not fit on an SM");
+    int grid = sms * per_sm;
+    if ((int64_t)grid * W > (int64_t)n_tasks + 4 * W) grid = (n_tasks + W - 1) / W + 1;  // no more warps than tasks
+    tsm::PairsArgs A;
+    A.pts = reinterpret_cast<const float2*>(pts);
+    A.off_a = off_a;
+    A.len_a = len_a;
+    A.off_b = off_b;
+    A.len_b = len_b;
+    A.order = order;
+    A.max_len = max_len;
+    A.p = make_kparams(params);
+    A.out = out;
+    A.counts = out_counts;
+    A.out_stride = out_stride;
+    const int4* t4 = reinterpret_cast<const int4*>(tasks);
+    int* queue = static_cast<int*>(workspace);
+    int nt = n_tasks, total_warps = grid * W, wf = warp_smem_floats;
+    int tile_cap = wf / 32, g8_cap = wf / 4, wave_cap = wf;
+    void* args[] = {&A, &t4, &nt, &queue, &total_warps, &wf, &tile_cap, &g8_cap, &wave_cap};
+    e = cudaLaunchKernel(fn, dim3(grid), dim3(32 * W), args, (size_t)smem, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaLaunchKernel");
+    return TSM_OK;
 }
 
 }  // extern "C"

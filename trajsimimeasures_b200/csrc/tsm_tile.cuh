@@ -55,56 +55,187 @@ __device__ __forceinline__ float4 col4(const SmemCols& c, int j, const KParams&,
     return c.pt4(j);
 }
 
+// R consecutive rows of a pair's DP: their points (and ERP gap distances)
+// and their current DP values, all in registers.
+template <class C, int R, bool EXACT>
+struct RowBlock {
+    float x[R], y[R], g[R], D[R];
+
+    // rows i0 .. i0+R-1; rows past the end repeat the last point (their
+    // values are never read by a valid cell)
+    __device__ __forceinline__ void load(const float2* __restrict__ rowp, int i0, int nr, float rowb,
+                                         const KParams& p) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float2 q = __ldg(rowp + min(i0 + r, nr - 1));
+            x[r] = q.x;
+            y[r] = q.y;
+            g[r] = C::kGap ? gapdist<EXACT>(q.x, q.y, p) : 0.f;
+            D[r] = rowb;
+        }
+    }
+
+    // One column: top = D(i0-1, j), diag = D(i0-1, j-1); D[] holds column j-1
+    // on entry and column j on exit.  Returns the block's bottom value.
+    __device__ __forceinline__ float step(const float4& c, float top, float diag, float eps2) {
+        float up = top, dg = diag;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float left = D[r];
+            const float nv = C::cell(dg, up, left, d2f(x[r], y[r], c.x, c.y), g[r], c.z, eps2);
+            D[r] = nv;
+            dg = left;
+            up = nv;
+        }
+        return up;
+    }
+
+    __device__ __forceinline__ float pick(int rr) const {
+        float v = 0.f;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (r == rr) v = D[r];
+        return v;
+    }
+};
+
+// Two row blocks of a 2R-row pass packed into float2 lanes: .x = the upper
+// block (rows rb .. rb+R-1), .y = the lower block (rows rb+R .. rb+2R-1),
+// the lower one column behind the upper.
+template <int M, int R, bool EXACT>
+struct RowPair {
+    using C2 = typename Cell2Of<M, EXACT>::type;
+    float2 X[R], Y[R], Gr[R];
+
+    __device__ __forceinline__ void load(const float2* __restrict__ rowp, int rb, int nr, const KParams& p) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float2 u = __ldg(rowp + min(rb + r, nr - 1));
+            const float2 l = __ldg(rowp + min(rb + R + r, nr - 1));
+            X[r] = make_float2(u.x, l.x);
+            Y[r] = make_float2(u.y, l.y);
+            Gr[r] = M == ERP ? make_float2(gapdist<EXACT>(u.x, u.y, p), gapdist<EXACT>(l.x, l.y, p))
+                             : make_float2(0.f, 0.f);
+        }
+    }
+
+    // Din holds both blocks' previous columns, Dout receives the new ones.
+    __device__ __forceinline__ float2 step(const float2 (&Din)[R], float2 (&Dout)[R], float2 nx, float2 ny,
+                                           float2 gc, float2 top, float2 diag, float eps2) const {
+        float2 up = top, dg = diag;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float2 left = Din[r];
+            const float2 nv = C2::cell(dg, up, left, d2f2(X[r], Y[r], nx, ny), Gr[r], gc, eps2);
+            Dout[r] = nv;
+            dg = left;
+            up = nv;
+        }
+        return up;
+    }
+};
+
 // The DP of one pair.  rowp/nr: row trajectory; cols/nc: column trajectory;
 // buf: this thread's boundary row (element j at buf[32*j]); srow/scol: ERP
 // gap totals of the row/column trajectory.  Returns D(nr-1, nc-1).
+//
+// Rows go in passes of 2R: an upper and a lower block of R rows, the lower
+// one column behind the upper, packed in the two halves of float2 registers
+// (one FADD2/FMUL2/FFMA2 does both blocks' cells).  At step j the upper block
+// computes column j from the boundary row, the lower block column j-1 from
+// the upper block's bottom values of columns j-1 and j-2, and writes its own
+// bottom value of column j-1 to the boundary row.  The two cell chains are
+// independent, and one boundary-row load and store are paid per 2R cells.
+// DP values alternate between two register arrays (no copies).  A final pass
+// of at most R rows uses one scalar block.
 template <int M, int R, bool EXACT, class Cols>
 __device__ __forceinline__ float dp_pair(const float2* __restrict__ rowp, int nr, const Cols& cols,
                                          int nc, float* buf, const KParams& p, float srow, float scol) {
     using C = typename CellOf<M, EXACT>::type;
     if (nr <= 0 || nc <= 0) return 0.f;
-    const float topb = C::topb(scol);
+    const float topb = C::topb(scol), rowb = C::rowb(srow);
     for (int j = 0; j < nc; ++j) buf[32 * j] = topb;
     float dlast = 0.f;
-    for (int rb = 0; rb < nr; rb += R) {
-        float rx[R], ry[R], rg[R], D[R];
+    int rb = 0;
+    for (; nr - rb > R; rb += 2 * R) {
+        RowPair<M, R, EXACT> rp;
+        rp.load(rowp, rb, nr, p);
+        float2 DA[R], DB[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int i = min(rb + r, nr - 1);  // rows past the end repeat the last point
-            const float2 q = __ldg(rowp + i);
-            rx[r] = q.x;
-            ry[r] = q.y;
-            rg[r] = C::kGap ? gapdist<EXACT>(q.x, q.y, p) : 0.f;
-            D[r] = C::rowb(srow);
+        for (int r = 0; r < R; ++r) DA[r] = make_float2(rowb, rowb);
+        // step 0: the upper block's column 0 (the lower lane is reset after)
+        float4 c = col4<EXACT>(cols, 0, p, C::kGap);
+        float top = buf[0];
+        const int j1 = min(1, nc - 1);
+        float4 cn = col4<EXACT>(cols, j1, p, C::kGap);
+        float tn = buf[32 * j1];
+        float ub1 = rp.step(DA, DB, make_float2(-c.x, -c.x), make_float2(-c.y, -c.y), make_float2(c.z, c.z),
+                            make_float2(top, rowb), make_float2((rb == 0) ? C::corner() : rowb, rowb), p.eps2)
+                        .x;
+#pragma unroll
+        for (int r = 0; r < R; ++r) DB[r].y = rowb;
+        float ub2 = rowb, udiag = top;
+        float4 cprev = c;
+        // steps 1 .. nc-1: upper column j, lower column j-1; two per iteration
+        // so that DA/DB swap roles without register copies
+        auto pair_step = [&](const float2 (&Din)[R], float2 (&Dout)[R], int j) {
+            c = cn;
+            top = tn;
+            const int jn = min(j + 1, nc - 1);  // prefetch the next column
+            cn = col4<EXACT>(cols, jn, p, C::kGap);
+            tn = buf[32 * jn];
+            const float2 b = rp.step(Din, Dout, make_float2(-c.x, -cprev.x), make_float2(-c.y, -cprev.y),
+                                     make_float2(c.z, cprev.z), make_float2(top, ub1), make_float2(udiag, ub2), p.eps2);
+            buf[32 * (j - 1)] = b.y;
+            udiag = top;
+            ub2 = ub1;
+            ub1 = b.x;
+            cprev = c;
+        };
+        int j = 1;
+        for (; j + 1 < nc; j += 2) {
+            pair_step(DB, DA, j);
+            pair_step(DA, DB, j + 1);
         }
-        float diag = (rb == 0) ? C::corner() : C::rowb(srow);
+        // last step: the lower block's column nc-1 (the upper lane idles)
+        float2 b;
+        int rr = nr - 1 - (rb + R);
+        if (j < nc) {  // one more full step (DB -> DA), then the lower-only step (DA -> DB)
+            pair_step(DB, DA, j);
+            b = rp.step(DA, DB, make_float2(-cprev.x, -cprev.x), make_float2(-cprev.y, -cprev.y),
+                        make_float2(cprev.z, cprev.z), make_float2(ub1, ub1), make_float2(ub2, ub2), p.eps2);
+            if (rb + 2 * R >= nr) {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r == rr) dlast = DB[r].y;
+            }
+        } else {  // the lower-only step from DB -> DA
+            b = rp.step(DB, DA, make_float2(-cprev.x, -cprev.x), make_float2(-cprev.y, -cprev.y),
+                        make_float2(cprev.z, cprev.z), make_float2(ub1, ub1), make_float2(ub2, ub2), p.eps2);
+            if (rb + 2 * R >= nr) {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r == rr) dlast = DA[r].y;
+            }
+        }
+        buf[32 * (nc - 1)] = b.y;
+    }
+    if (rb < nr) {  // last rows (at most R): one block
+        RowBlock<C, R, EXACT> blk;
+        blk.load(rowp, rb, nr, rowb, p);
+        float diag = (rb == 0) ? C::corner() : rowb;
         float4 cn = col4<EXACT>(cols, 0, p, C::kGap);
         float tn = buf[0];
         for (int j = 0; j < nc; ++j) {
             const float4 c = cn;
             const float top = tn;
-            const int jn = min(j + 1, nc - 1);  // prefetch the next column
+            const int jn = min(j + 1, nc - 1);
             cn = col4<EXACT>(cols, jn, p, C::kGap);
             tn = buf[32 * jn];
-            float up = top, dg = diag;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const float left = D[r];
-                const float d2 = d2f(rx[r], ry[r], c.x, c.y);
-                const float nv = C::cell(dg, up, left, d2, rg[r], c.z, p.eps2);
-                D[r] = nv;
-                dg = left;
-                up = nv;
-            }
-            buf[32 * j] = up;
+            blk.step(c, top, diag, p.eps2);
             diag = top;
         }
-        if (rb + R >= nr) {
-            const int rr = nr - 1 - rb;
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-                if (r == rr) dlast = D[r];
-        }
+        dlast = blk.pick(nr - 1 - rb);
     }
     return dlast;
 }
@@ -234,11 +365,14 @@ __device__ __forceinline__ float p2s(float px, float py, float s1x, float s1y, f
 // the last vertex come out exactly 0 (u = dot * (1/len2) can round to 1-ulp,
 // leaving a ~1e-11 residue), as every other vertex already does as the
 // first endpoint of its outgoing segment.
+// Points pb0, pb0 + pstride, ... (blocks of R) of P: a thread takes all
+// points (pb0 = 0, pstride = R) or, in a warp-per-pair task, every 32nd block.
 template <int R, bool EXACT, class Segs>
-__device__ __forceinline__ float directed_max(const float2* __restrict__ P, int np, const Segs& T, int nt) {
+__device__ __forceinline__ float directed_max(const float2* __restrict__ P, int np, const Segs& T, int nt,
+                                             int pb0 = 0, int pstride = R) {
     if (nt < 2 || np <= 0) return 0.f;  // p2t_dist over zero segments is 0.0
     float m = 0.f;
-    for (int pb = 0; pb < np; pb += R) {
+    for (int pb = pb0; pb < np; pb += pstride) {
         float px[R], py[R], best[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -286,6 +420,80 @@ __global__ void __launch_bounds__(128) hausdorff_pairs_kernel(
     out[k] = __fsqrt_rn(fmaxf(m1, m2));
 }
 
+// Query segments staged in shared memory for the matrix kernel:
+// seg[k] = (s1.x, s1.y, s.x, s.y) with s = q[k+1] - q[k] (s = 0 for the last
+// vertex, k = nq-1), sinv[k] = 1/|s|^2 (0 for a zero-length segment).
+template <int R, bool EXACT>
+__device__ __forceinline__ float directed_max_staged(const float2* __restrict__ P, int np, const float4* seg,
+                                                     const float* sinv, int nq) {
+    if (nq < 2 || np <= 0) return 0.f;
+    float m = 0.f;
+    for (int pb = 0; pb < np; pb += R) {
+        float px[R], py[R], best[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float2 q = __ldg(P + min(pb + r, np - 1));
+            px[r] = q.x;
+            py[r] = q.y;
+            best[r] = CUDART_INF_F;
+        }
+        for (int k = 0; k < nq; ++k) {  // nq-1 segments + the last vertex
+            const float4 sg = seg[k];
+            const float inv = sinv[k];
+#pragma unroll
+            for (int r = 0; r < R; ++r) best[r] = fminf(best[r], p2s(px[r], py[r], sg.x, sg.y, sg.z, sg.w, inv));
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (pb + r < np) m = fmaxf(m, best[r]);
+    }
+    return m;
+}
+
+// Query points read back from the staged segments (seg[k].xy = q[k]).
+struct StagedPts {
+    const float4* s;
+    __device__ __forceinline__ float2 pt(int j) const {
+        const float4 v = s[j];
+        return make_float2(v.x, v.y);
+    }
+};
+
+// max over the points of the query (from shared memory) of the min over the
+// segments of a per-thread trajectory T (global memory, computed on the fly).
+template <int R, bool EXACT>
+__device__ __forceinline__ float directed_max_qpts(const StagedPts& P, int np, const float2* __restrict__ T, int nt) {
+    if (nt < 2 || np <= 0) return 0.f;
+    float m = 0.f;
+    for (int pb = 0; pb < np; pb += R) {
+        float px[R], py[R], best[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float2 q = P.pt(min(pb + r, np - 1));
+            px[r] = q.x;
+            py[r] = q.y;
+            best[r] = CUDART_INF_F;
+        }
+        float2 s1 = __ldg(T);
+        float2 s2n = __ldg(T + 1);
+        for (int k = 0; k < nt; ++k) {
+            const float2 s2 = s2n;
+            s2n = __ldg(T + min(k + 2, nt - 1));
+            const float sx = __fsub_rn(s2.x, s1.x), sy = __fsub_rn(s2.y, s1.y);
+            const float len2 = __fmaf_rn(sy, sy, __fmul_rn(sx, sx));
+            const float inv = (sx == 0.f && sy == 0.f) ? 0.f : trcp<EXACT>(len2);
+#pragma unroll
+            for (int r = 0; r < R; ++r) best[r] = fminf(best[r], p2s(px[r], py[r], s1.x, s1.y, sx, sy, inv));
+            s1 = s2;
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (pb + r < np) m = fmaxf(m, best[r]);
+    }
+    return m;
+}
+
+// Dynamic shared memory = q_max_len * (16 + 4) bytes.
 template <int R, bool EXACT>
 __global__ void __launch_bounds__(128) hausdorff_matrix_kernel(
     const float2* __restrict__ q_pts, const int64_t* __restrict__ q_off, const int32_t* __restrict__ q_len,
@@ -293,17 +501,23 @@ __global__ void __launch_bounds__(128) hausdorff_matrix_kernel(
     const int32_t* __restrict__ d_order, int64_t nd, int chunks, int q_max_len, int d_max_len,
     float* __restrict__ out, int64_t ld) {
     extern __shared__ float smem[];
-    float4* cols = reinterpret_cast<float4*>(smem);
+    float4* seg = reinterpret_cast<float4*>(smem);
+    float* sinv = smem + 4 * q_max_len;
     const int64_t qi = blockIdx.x / chunks;
     const int chunk = blockIdx.x % chunks;
     const int nq = q_len[qi];
     const bool qbad = nq < 0 || nq > q_max_len;
-    const float2* qp = q_pts + q_off[qi];
-    if (!qbad)
-        for (int j = threadIdx.x; j < nq; j += blockDim.x) {
-            const float2 v = __ldg(qp + j);
-            cols[j] = make_float4(v.x, v.y, 0.f, 0.f);
+    if (!qbad) {
+        const float2* qp = q_pts + q_off[qi];
+        for (int k = threadIdx.x; k < nq; k += blockDim.x) {
+            const float2 s1 = __ldg(qp + k);
+            const float2 s2 = __ldg(qp + min(k + 1, nq - 1));
+            const float sx = __fsub_rn(s2.x, s1.x), sy = __fsub_rn(s2.y, s1.y);
+            const float len2 = __fmaf_rn(sy, sy, __fmul_rn(sx, sx));
+            seg[k] = make_float4(s1.x, s1.y, sx, sy);
+            sinv[k] = (sx == 0.f && sy == 0.f) ? 0.f : trcp<EXACT>(len2);
         }
+    }
     __syncthreads();
     const int64_t slot = (int64_t)chunk * blockDim.x + threadIdx.x;
     if (slot >= nd) return;
@@ -315,8 +529,8 @@ __global__ void __launch_bounds__(128) hausdorff_matrix_kernel(
         return;
     }
     const float2* dp = d_pts + d_off[dj];
-    const float m1 = directed_max<R, EXACT>(dp, ndl, SmemCols{cols}, nq);
-    const float m2 = directed_max<R, EXACT>(qp, nq, GlobalCols{dp}, ndl);
+    const float m1 = directed_max_staged<R, EXACT>(dp, ndl, seg, sinv, nq);
+    const float m2 = directed_max_qpts<R, EXACT>(StagedPts{seg}, nq, dp, ndl);
     out[o_idx] = __fsqrt_rn(fmaxf(m1, m2));
 }
 

@@ -1,0 +1,106 @@
+"""kNN queries over a trajectory database on the GPU.
+
+The reference answers kNN queries with CPU indices that prune by lower
+bounds and refine with exact measures (DITA for DTW/ERP,
+query/cpp/DITA.cpp:276-431; DFT for Hausdorff/Frechet, query/cpp/DFT.cpp:89-230;
+its GPU refinement bridge Traj::TrajSimiGPU is broken as shipped).  Here:
+
+* ``knn_exhaustive``: exact top-k by evaluating every (query, database) pair
+  with the all-pairs kernel, chunk by chunk over the length-sorted database,
+  and selecting with the top-k kernel (tsm_topk_rows); per chunk the k best
+  are kept, then merged.
+* ``knn_rerank``: exact top-k among given candidates (e.g. a learned filter's
+  top-200): the candidate pairs are evaluated with the paired kernel and the
+  best k selected.  ``recall_at_k`` compares two answers.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .engine import TrajSet, _ptr, _stream_ptr, matrix_raw, measure_id, pairs_raw
+
+
+def topk_rows(d: torch.Tensor, k: int, stream=None):
+    """k smallest per row of a float32 CUDA matrix -> (values [n, k], int32 columns [n, k]),
+    ascending, ties to the smaller column (a stable argsort's first k)."""
+    if d.dtype != torch.float32 or not d.is_cuda or d.dim() != 2 or d.stride(1) != 1:
+        raise ValueError("expected a row-major float32 CUDA matrix")
+    n, m = d.shape
+    vals = torch.empty((n, k), dtype=torch.float32, device=d.device)
+    idx = torch.empty((n, k), dtype=torch.int32, device=d.device)
+    rc = _lib.load().tsm_topk_rows(_ptr(d), n, m, d.stride(0), int(k), _ptr(vals), _ptr(idx), _stream_ptr(stream))
+    _lib.check(rc, "tsm_topk_rows")
+    return vals, idx
+
+
+def _subset(s: TrajSet, idx: torch.Tensor) -> TrajSet:
+    """A view of trajectories idx of s (same point pool)."""
+    lens_h = s.lens_host[idx.cpu().numpy()] if s.lens_host is not None else None
+    out = TrajSet(s.pts, s.off[idx], s.lens[idx], int(lens_h.max()) if lens_h is not None and lens_h.size
+                  else int(s.lens[idx].max().item()), lens_h)
+    out._order = torch.arange(idx.shape[0], dtype=torch.int32, device=s.device)  # idx is length-sorted
+    return out
+
+
+def knn_exhaustive(Q: TrajSet, D: TrajSet, k=10, measure="dtw", *, chunk=1 << 18, eps=0.0, gpoint=(0.0, 0.0),
+                   exact=False, stream=None):
+    """Exact k nearest database trajectories of every query: (dist float32
+    [nq, k], index int64 [nq, k]) ascending, ties to the smaller index."""
+    m = measure_id(measure)
+    order = D.order_by_length().long()
+    best_d, best_i = [], []
+    buf = torch.empty((Q.n, min(chunk, D.n)), dtype=torch.float32, device=Q.device)
+    for s in range(0, D.n, chunk):
+        ids = order[s:s + chunk]
+        sub = _subset(D, ids)
+        out = buf[:, :sub.n]
+        matrix_raw(m, Q, sub, out=out, eps=eps, gpoint=gpoint, exact=exact, stream=stream)
+        v, j = topk_rows(out, min(k, sub.n), stream=stream)
+        best_d.append(v)
+        best_i.append(ids[j.long()])
+    dcat = torch.cat(best_d, dim=1)
+    icat = torch.cat(best_i, dim=1)
+    if len(best_d) == 1:
+        return dcat, icat
+    # merge the per-chunk lists; ties to the smaller database index: order the
+    # concatenated candidates by index first, then a stable top-k by value
+    o = torch.argsort(icat, dim=1)
+    dcat = torch.gather(dcat, 1, o).contiguous()
+    icat = torch.gather(icat, 1, o)
+    v, j = topk_rows(dcat, k, stream=stream)
+    return v, torch.gather(icat, 1, j.long())
+
+
+def knn_rerank(Q: TrajSet, D: TrajSet, cand: torch.Tensor, k=10, measure="dtw", *, eps=0.0, gpoint=(0.0, 0.0),
+               exact=False, stream=None):
+    """Exact top-k among candidate database indices cand [nq, c] (int64):
+    (dist [nq, k], index [nq, k])."""
+    m = measure_id(measure)
+    nq, c = cand.shape
+    shift = D.pts.shape[0]
+    pool = torch.cat([D.pts, Q.pts])  # one point pool for the paired kernel
+    qi = torch.arange(nq, device=Q.device).repeat_interleave(c)
+    di = cand.reshape(-1).long()
+    off_a, len_a = Q.off[qi] + shift, Q.lens[qi]
+    off_b, len_b = D.off[di], D.lens[di]
+    out = torch.empty(nq * c, dtype=torch.float32, device=Q.device)
+    pairs_raw(m, pool, off_a, len_a, off_b, len_b, max(Q.max_len, D.max_len), out=out, eps=eps, gpoint=gpoint,
+              exact=exact, stream=stream)
+    # ties to the smaller database index, as in knn_exhaustive
+    o = torch.argsort(cand, dim=1)
+    dd = torch.gather(out.view(nq, c), 1, o).contiguous()
+    ci = torch.gather(cand, 1, o)
+    v, j = topk_rows(dd, k, stream=stream)
+    return v, torch.gather(ci, 1, j.long())
+
+
+def recall_at_k(approx_idx, exact_idx) -> float:
+    """Mean |approx top-k  intersect  exact top-k| / k over the queries."""
+    a = np.asarray(approx_idx.cpu() if isinstance(approx_idx, torch.Tensor) else approx_idx)
+    e = np.asarray(exact_idx.cpu() if isinstance(exact_idx, torch.Tensor) else exact_idx)
+    k = e.shape[1]
+    return float(np.mean([len(np.intersect1d(a[i], e[i])) / k for i in range(e.shape[0])]))
