@@ -166,80 +166,6 @@ struct LcssCell {
     }
 };
 
-// ---------------------------------------------------------------------------
-// Packed FP32x2 forms (Blackwell FADD2/FMUL2/FFMA2): element .x is a cell of
-// one row block, element .y a cell of another, independent block.  Every
-// element is rounded exactly like the scalar form above, so results are
-// bit-identical; min/max and sqrt stay scalar.
-// ---------------------------------------------------------------------------
-
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-
-template <bool EXACT>
-__device__ __forceinline__ float2 tsqrt2(float2 v) { return make_float2(tsqrt<EXACT>(v.x), tsqrt<EXACT>(v.y)); }
-
-__device__ __forceinline__ float2 min3f2(float2 a, float2 b, float2 c) {
-    return make_float2(min3f(a.x, b.x, c.x), min3f(a.y, b.y, c.y));
-}
-__device__ __forceinline__ float2 max3f2(float2 a, float2 b, float2 c) {
-    return make_float2(max3f(a.x, b.x, c.x), max3f(a.y, b.y, c.y));
-}
-
-// d2 of two cells: x, y = row coordinates, nx, ny = NEGATED column
-// coordinates; x + (-c) rounds exactly like x - c.
-__device__ __forceinline__ float2 d2f2(float2 x, float2 y, float2 nx, float2 ny) {
-    const float2 dx = __fadd2_rn(x, nx);
-    const float2 dy = __fadd2_rn(y, ny);
-    return __ffma2_rn(dy, dy, __fmul2_rn(dx, dx));
-}
-
-template <bool EXACT>
-struct DtwCell2 {
-    __device__ __forceinline__ static float2 cell(float2 dg, float2 up, float2 left, float2 d2, float2, float2,
-                                                  float) {
-        return add2(tsqrt2<EXACT>(d2), min3f2(dg, up, left));
-    }
-};
-template <bool EXACT>
-struct FrechetCell2 {
-    __device__ __forceinline__ static float2 cell(float2 dg, float2 up, float2 left, float2 d2, float2, float2,
-                                                  float) {
-        const float2 m = min3f2(dg, up, left);
-        return make_float2(fmaxf(d2.x, m.x), fmaxf(d2.y, m.y));
-    }
-};
-template <bool EXACT>
-struct ErpCell2 {
-    __device__ __forceinline__ static float2 cell(float2 dg, float2 up, float2 left, float2 d2, float2 grow,
-                                                  float2 gcol, float) {
-        return min3f2(add2(left, gcol), add2(up, grow), add2(dg, tsqrt2<EXACT>(d2)));
-    }
-};
-template <bool EXACT>
-struct EdrCell2 {
-    __device__ __forceinline__ static float2 cell(float2 dg, float2 up, float2 left, float2 d2, float2, float2,
-                                                  float eps2) {
-        const float2 sub = make_float2(d2.x < eps2 ? 0.f : 1.f, d2.y < eps2 ? 0.f : 1.f);
-        const float2 one = make_float2(1.f, 1.f);
-        return min3f2(add2(dg, sub), add2(up, one), add2(left, one));
-    }
-};
-template <bool EXACT>
-struct LcssCell2 {
-    __device__ __forceinline__ static float2 cell(float2 dg, float2 up, float2 left, float2 d2, float2, float2,
-                                                  float eps2) {
-        const float2 m = make_float2(d2.x < eps2 ? 1.f : 0.f, d2.y < eps2 ? 1.f : 0.f);
-        return max3f2(add2(dg, m), up, left);
-    }
-};
-
-template <int M, bool EXACT> struct Cell2Of;
-template <bool E> struct Cell2Of<DTW, E> { using type = DtwCell2<E>; };
-template <bool E> struct Cell2Of<DFRECHET, E> { using type = FrechetCell2<E>; };
-template <bool E> struct Cell2Of<ERP, E> { using type = ErpCell2<E>; };
-template <bool E> struct Cell2Of<EDR, E> { using type = EdrCell2<E>; };
-template <bool E> struct Cell2Of<LCSS, E> { using type = LcssCell2<E>; };
-
 template <int M, bool EXACT> struct CellOf;
 template <bool E> struct CellOf<DTW, E> { using type = DtwCell<E>; };
 template <bool E> struct CellOf<DFRECHET, E> { using type = FrechetCell<E>; };

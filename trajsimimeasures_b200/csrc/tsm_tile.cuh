@@ -90,6 +90,23 @@ struct RowBlock {
         return up;
     }
 
+    // Same column step, reading the previous column from Din and writing the
+    // new one to Dout: alternating two arrays between steps needs no register
+    // copies (an in-place update costs one move per row).
+    __device__ __forceinline__ float step2(const float (&Din)[R], float (&Dout)[R], const float4& c, float top,
+                                           float diag, float eps2) const {
+        float up = top, dg = diag;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float left = Din[r];
+            const float nv = C::cell(dg, up, left, d2f(x[r], y[r], c.x, c.y), g[r], c.z, eps2);
+            Dout[r] = nv;
+            dg = left;
+            up = nv;
+        }
+        return up;
+    }
+
     __device__ __forceinline__ float pick(int rr) const {
         float v = 0.f;
 #pragma unroll
@@ -99,55 +116,22 @@ struct RowBlock {
     }
 };
 
-// Two row blocks of a 2R-row pass packed into float2 lanes: .x = the upper
-// block (rows rb .. rb+R-1), .y = the lower block (rows rb+R .. rb+2R-1),
-// the lower one column behind the upper.
-template <int M, int R, bool EXACT>
-struct RowPair {
-    using C2 = typename Cell2Of<M, EXACT>::type;
-    float2 X[R], Y[R], Gr[R];
-
-    __device__ __forceinline__ void load(const float2* __restrict__ rowp, int rb, int nr, const KParams& p) {
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const float2 u = __ldg(rowp + min(rb + r, nr - 1));
-            const float2 l = __ldg(rowp + min(rb + R + r, nr - 1));
-            X[r] = make_float2(u.x, l.x);
-            Y[r] = make_float2(u.y, l.y);
-            Gr[r] = M == ERP ? make_float2(gapdist<EXACT>(u.x, u.y, p), gapdist<EXACT>(l.x, l.y, p))
-                             : make_float2(0.f, 0.f);
-        }
-    }
-
-    // Din holds both blocks' previous columns, Dout receives the new ones.
-    __device__ __forceinline__ float2 step(const float2 (&Din)[R], float2 (&Dout)[R], float2 nx, float2 ny,
-                                           float2 gc, float2 top, float2 diag, float eps2) const {
-        float2 up = top, dg = diag;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const float2 left = Din[r];
-            const float2 nv = C2::cell(dg, up, left, d2f2(X[r], Y[r], nx, ny), Gr[r], gc, eps2);
-            Dout[r] = nv;
-            dg = left;
-            up = nv;
-        }
-        return up;
-    }
-};
-
 // The DP of one pair.  rowp/nr: row trajectory; cols/nc: column trajectory;
 // buf: this thread's boundary row (element j at buf[32*j]); srow/scol: ERP
 // gap totals of the row/column trajectory.  Returns D(nr-1, nc-1).
 //
 // Rows go in passes of 2R: an upper and a lower block of R rows, the lower
-// one column behind the upper, packed in the two halves of float2 registers
-// (one FADD2/FMUL2/FFMA2 does both blocks' cells).  At step j the upper block
-// computes column j from the boundary row, the lower block column j-1 from
-// the upper block's bottom values of columns j-1 and j-2, and writes its own
-// bottom value of column j-1 to the boundary row.  The two cell chains are
-// independent, and one boundary-row load and store are paid per 2R cells.
-// DP values alternate between two register arrays (no copies).  A final pass
-// of at most R rows uses one scalar block.
+// one column behind the upper.  At step j the upper block computes column j
+// from the boundary row, the lower block column j-1 from the upper block's
+// bottom values of columns j-1 and j-2 (kept in registers), and writes its
+// own bottom value of column j-1 to the boundary row.  The two blocks' cell
+// chains are independent within a step (two chains for the scheduler), and
+// only one boundary-row load and store are paid per 2R cells.  Each block's
+// values alternate between two register arrays, two columns per loop trip,
+// so no register copies are needed.  A final pass of at most R rows uses one
+// block.  (Packing the two blocks into FP32x2 instructions was measured
+// slower: assembling the pairs around the scalar min/max costs more than the
+// packed arithmetic saves.)
 template <int M, int R, bool EXACT, class Cols>
 __device__ __forceinline__ float dp_pair(const float2* __restrict__ rowp, int nr, const Cols& cols,
                                          int nc, float* buf, const KParams& p, float srow, float scol) {
@@ -158,67 +142,64 @@ __device__ __forceinline__ float dp_pair(const float2* __restrict__ rowp, int nr
     float dlast = 0.f;
     int rb = 0;
     for (; nr - rb > R; rb += 2 * R) {
-        RowPair<M, R, EXACT> rp;
-        rp.load(rowp, rb, nr, p);
-        float2 DA[R], DB[R];
+        RowBlock<C, R, EXACT> hi, lo;
+        hi.load(rowp, rb, nr, rowb, p);
+        lo.load(rowp, rb + R, nr, rowb, p);
+        float HA[R], HB[R], LA[R], LB[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) DA[r] = make_float2(rowb, rowb);
-        // step 0: the upper block's column 0 (the lower lane is reset after)
-        float4 c = col4<EXACT>(cols, 0, p, C::kGap);
+        for (int r = 0; r < R; ++r) {
+            HA[r] = rowb;
+            LA[r] = rowb;
+        }
         float top = buf[0];
+        float4 c = col4<EXACT>(cols, 0, p, C::kGap);
         const int j1 = min(1, nc - 1);
         float4 cn = col4<EXACT>(cols, j1, p, C::kGap);
         float tn = buf[32 * j1];
-        float ub1 = rp.step(DA, DB, make_float2(-c.x, -c.x), make_float2(-c.y, -c.y), make_float2(c.z, c.z),
-                            make_float2(top, rowb), make_float2((rb == 0) ? C::corner() : rowb, rowb), p.eps2)
-                        .x;
-#pragma unroll
-        for (int r = 0; r < R; ++r) DB[r].y = rowb;
+        // step 0: the upper block's column 0 (HA -> HB); the lower block waits in LA
+        float ub1 = hi.step2(HA, HB, c, top, (rb == 0) ? C::corner() : rowb, p.eps2);
         float ub2 = rowb, udiag = top;
         float4 cprev = c;
-        // steps 1 .. nc-1: upper column j, lower column j-1; two per iteration
-        // so that DA/DB swap roles without register copies
-        auto pair_step = [&](const float2 (&Din)[R], float2 (&Dout)[R], int j) {
+        // steps 1 .. nc-1: upper column j, lower column j-1
+        auto pair_step = [&](const float (&Hi)[R], float (&Ho)[R], const float (&Li)[R], float (&Lo)[R], int j) {
             c = cn;
             top = tn;
             const int jn = min(j + 1, nc - 1);  // prefetch the next column
             cn = col4<EXACT>(cols, jn, p, C::kGap);
             tn = buf[32 * jn];
-            const float2 b = rp.step(Din, Dout, make_float2(-c.x, -cprev.x), make_float2(-c.y, -cprev.y),
-                                     make_float2(c.z, cprev.z), make_float2(top, ub1), make_float2(udiag, ub2), p.eps2);
-            buf[32 * (j - 1)] = b.y;
+            const float nb = hi.step2(Hi, Ho, c, top, udiag, p.eps2);
+            const float lb = lo.step2(Li, Lo, cprev, ub1, ub2, p.eps2);
+            buf[32 * (j - 1)] = lb;
             udiag = top;
             ub2 = ub1;
-            ub1 = b.x;
+            ub1 = nb;
             cprev = c;
         };
         int j = 1;
         for (; j + 1 < nc; j += 2) {
-            pair_step(DB, DA, j);
-            pair_step(DA, DB, j + 1);
+            pair_step(HB, HA, LA, LB, j);
+            pair_step(HA, HB, LB, LA, j + 1);
         }
-        // last step: the lower block's column nc-1 (the upper lane idles)
-        float2 b;
-        int rr = nr - 1 - (rb + R);
-        if (j < nc) {  // one more full step (DB -> DA), then the lower-only step (DA -> DB)
-            pair_step(DB, DA, j);
-            b = rp.step(DA, DB, make_float2(-cprev.x, -cprev.x), make_float2(-cprev.y, -cprev.y),
-                        make_float2(cprev.z, cprev.z), make_float2(ub1, ub1), make_float2(ub2, ub2), p.eps2);
+        // the lower block's last column; the final arrays depend on nc's parity
+        float lb;
+        const int rr = nr - 1 - (rb + R);
+        if (j < nc) {
+            pair_step(HB, HA, LA, LB, j);
+            lb = lo.step2(LB, LA, cprev, ub1, ub2, p.eps2);
             if (rb + 2 * R >= nr) {
 #pragma unroll
                 for (int r = 0; r < R; ++r)
-                    if (r == rr) dlast = DB[r].y;
+                    if (r == rr) dlast = LA[r];
             }
-        } else {  // the lower-only step from DB -> DA
-            b = rp.step(DB, DA, make_float2(-cprev.x, -cprev.x), make_float2(-cprev.y, -cprev.y),
-                        make_float2(cprev.z, cprev.z), make_float2(ub1, ub1), make_float2(ub2, ub2), p.eps2);
+        } else {
+            lb = lo.step2(LA, LB, cprev, ub1, ub2, p.eps2);
             if (rb + 2 * R >= nr) {
 #pragma unroll
                 for (int r = 0; r < R; ++r)
-                    if (r == rr) dlast = DA[r].y;
+                    if (r == rr) dlast = LB[r];
             }
         }
-        buf[32 * (nc - 1)] = b.y;
+        buf[32 * (nc - 1)] = lb;
     }
     if (rb < nr) {  // last rows (at most R): one block
         RowBlock<C, R, EXACT> blk;
