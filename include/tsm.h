@@ -142,6 +142,25 @@ int tsm_pairs_sched(const float* pts, const int64_t* off_a, const int32_t* len_a
                     int32_t* out_counts, int64_t out_stride, void* workspace, void* stream);
 
 /*
+ * tsm_pairs_sched without a workspace argument: the same persistent launch,
+ * with its scratch (the 8-byte task queue) in a 256-byte array that the
+ * library allocates statically on every GPU that loads it.  No counterpart in
+ * the reference (its GPU calls allocate per call through Numba).  For callers
+ * that cannot allocate device memory where they call (host callbacks,
+ * sections that must not touch the CUDA allocator, plugins whose host owns all
+ * device memory, FFI callers without an allocator); inputs and outputs are
+ * still theirs.  The array is shared by every call: calls that overlap on the
+ * GPU race and give wrong results.  The first call on a device sets the array
+ * up (symbol lookup + clear + device synchronisation): make it before any
+ * stream capture.  Returns TSM_ETOOLONG if the kernel's scratch would exceed
+ * the array.
+ */
+int tsm_pairs_sched_noalloc(const float* pts, const int64_t* off_a, const int32_t* len_a, const int64_t* off_b,
+                            const int32_t* len_b, const int32_t* order, const int32_t* tasks, int32_t n_tasks,
+                            int32_t max_len, int32_t warp_smem_floats, const tsm_params* params, float* out,
+                            int32_t* out_counts, int64_t out_stride, void* stream);
+
+/*
  * Row-wise k smallest (kNN result lists): for each row r < n_rows of the
  * float32 matrix d (row stride ld), the k smallest values in ascending order,
  * ties to the smaller column index (= the first k entries of a stable argsort;

@@ -20,7 +20,7 @@ FLAG_EXACT = 1
 
 # Every symbol include/tsm.h declares (checked by the test suite).
 EXPORTS = ("tsm_version", "tsm_last_error", "tsm_max_supported_len", "tsm_pairs", "tsm_matrix",
-           "tsm_sched_workspace_bytes", "tsm_pairs_sched", "tsm_topk_rows")
+           "tsm_sched_workspace_bytes", "tsm_pairs_sched", "tsm_topk_rows", "tsm_pairs_sched_noalloc")
 
 
 class TsmParams(ctypes.Structure):
@@ -63,6 +63,9 @@ def load():
         lib.tsm_pairs_sched.restype = ctypes.c_int
         lib.tsm_pairs_sched.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32,
                                         ctypes.POINTER(TsmParams), _vp, _vp, _i64, _vp, _vp]
+        lib.tsm_pairs_sched_noalloc.restype = ctypes.c_int
+        lib.tsm_pairs_sched_noalloc.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32,
+                                                ctypes.POINTER(TsmParams), _vp, _vp, _i64, _vp]
         lib.tsm_topk_rows.restype = ctypes.c_int
         lib.tsm_topk_rows.argtypes = [_vp, _i64, _i64, _i64, _i32, _vp, _vp, _vp]
         _lib = lib

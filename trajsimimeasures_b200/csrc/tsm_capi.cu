@@ -164,6 +164,13 @@ int launch(const void* fn, dim3 grid, dim3 block, int smem, void** args, cudaStr
 
 }  // namespace
 
+// Internal (hidden, not part of the ABI): lets other translation units of the
+// library report through tsm_last_error().
+__attribute__((visibility("hidden"))) int tsm_internal_fail(int code, const char* msg) {
+    g_err = msg;
+    return code;
+}
+
 extern "C" {
 
 int tsm_version(void) { return 100; }
