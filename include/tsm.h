@@ -173,6 +173,44 @@ int tsm_pairs_sched_noalloc(const float* pts, const int64_t* off_a, const int32_
 int tsm_topk_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, int32_t k, float* out_d,
                   int32_t* out_idx, void* stream);
 
+/*
+ * Unordered selection for long candidate lists: out_idx int32 [n_rows][k]
+ * receives, per row, the column indices of the k smallest values (the set of
+ * a stable argsort's first k, any order); -1 pads rows shorter than k.  Any k.
+ */
+int tsm_select_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, int64_t k, int32_t* out_idx,
+                    void* stream);
+
+/*
+ * Learned candidate filter (trajectory encoder).  The reference's learned
+ * measures embed trajectories and train on heuristic distances normalised by
+ * their maximum with an MSE loss (nn/MLP_trajsimi_train.py:74-84,197-200); this
+ * encoder (conv 2->64 k=5 + GRU 64->128 + linear 128->128, BF16 weights, FP32
+ * accumulation) is trained the same way on DTW labels from tsm_pairs and
+ * serves as a kNN filter.
+ *   params  float32 [tsm_enc_param_count()] master weights (layout: conv W
+ *           [64][2][5], b [64]; W_ih [384][64], b_ih [384]; W_hh [384][128],
+ *           b_hh [384]; W_o [128][128], b_o [128]; gate order r, z, n)
+ *   pts/off/len  a packed batch of B trajectories, T = max length in it
+ *   nrm     HOST float[4] = (mean_x, mean_y, 1/std_x, 1/std_y) input scaling
+ *   workspace  device memory of tsm_enc_workspace_bytes(B, T, P) bytes
+ */
+int tsm_enc_param_count(void);
+int64_t tsm_enc_workspace_bytes(int32_t B, int32_t T, int32_t P);
+/* emb float32 [B][128] (device) */
+int tsm_enc_forward(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
+                    int32_t T, const float* nrm, void* workspace, float* emb, void* stream);
+/* Forward + pair loss + backward.  Pairs (ia[p], ib[p]) index the batch,
+ * y[p] the target distances; loss = mean_p (||e_ia - e_ib|| - y)^2.
+ * grad float32 [param_count] (overwritten), loss float32 [1], pred [P]
+ * (both device, nullable). */
+int tsm_enc_loss_grad(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
+                      int32_t T, const float* nrm, const int32_t* ia, const int32_t* ib, const float* y, int32_t P,
+                      void* workspace, float* grad, float* loss, float* pred, void* stream);
+/* One Adam step on params with moments m, v (device, param_count each). */
+int tsm_enc_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr, float beta1,
+                 float beta2, float eps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

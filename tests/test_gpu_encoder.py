@@ -1,0 +1,76 @@
+"""GPU tests of the learned filter's hand-written kernels: forward values and
+gradients against an FP64 CPU autograd reference (oracle/encoder_ref.py), and
+a short training run that must learn DTW order (Spearman rho)."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _set(trajs):
+    from trajsimimeasures_b200.engine import TrajSet
+    return TrajSet.from_lists(trajs)
+
+
+def test_encoder_gradients_match_fp64_autograd():
+    from oracle import encoder_ref as R
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.surrogate import Encoder
+    rng = np.random.default_rng(3)
+    pts, off, lens = D._walks(rng, np.array([3, 30, 17, 1, 24, 9]), D.STEP_SIGMA)
+    trajs = D.unpack(pts, off, lens)
+    s = _set(trajs)
+    enc = Encoder.init(s, seed=5)
+    # larger weights than the init so that the gates leave their linear range
+    enc.params.mul_(3.0)
+    ia, ib, y = np.array([0, 1, 2, 4, 5]), np.array([1, 2, 4, 5, 3]), np.array([0.1, 0.5, 0.2, 0.9, 0.3])
+    loss, grad, pred = enc.loss_grad(s, np.arange(6), ia, ib, y)
+    torch.cuda.synchronize()
+    l_ref, g_ref, p_ref = R.loss_grad(enc.params.cpu().numpy(), trajs, enc.nrm, ia, ib, y)
+    np.testing.assert_allclose(pred.cpu().numpy(), p_ref, rtol=2e-5, atol=1e-6)
+    assert abs(loss.item() - l_ref) <= 1e-4 * abs(l_ref) + 1e-7
+    g = grad.cpu().numpy().astype(np.float64)
+    scale = np.abs(g_ref).max()
+    assert np.abs(g - g_ref).max() <= 1e-4 * scale, np.abs(g - g_ref).max() / scale
+    # every parameter block gets a gradient
+    o = 0
+    for name, shape in R.SIZES:
+        n = int(np.prod(shape))
+        assert np.abs(g_ref[o:o + n]).max() > 0, name
+        o += n
+
+
+def test_encoder_forward_long_batch():
+    from oracle import encoder_ref as R
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.surrogate import Encoder
+    rng = np.random.default_rng(4)
+    L = rng.integers(20, 201, 40)
+    pts, off, lens = D._walks(rng, L, D.STEP_SIGMA)
+    trajs = D.unpack(pts, off, lens)
+    s = _set(trajs)
+    enc = Encoder.init(s, seed=6)
+    e = enc.embed(s, batch=24).cpu().numpy()  # two batches (16 + 24 trajectories per GRU CTA tiles)
+    W = R.unpack(enc.params.cpu().numpy())
+    e_ref = R.embed(W, trajs[:6], enc.nrm).detach().numpy()
+    np.testing.assert_allclose(e[:6], e_ref, rtol=1e-4, atol=1e-5)
+
+
+def test_training_learns_dtw_order():
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.engine import TrajSet
+    from trajsimimeasures_b200.surrogate import Encoder, dtw_labels, spearman
+    p, o, l = D.trajectory_set(4000, seed=8)
+    s = TrajSet.from_packed(p, o, l)
+    rng = np.random.default_rng(9)
+    pa, pb = rng.integers(0, 4000, 30000), rng.integers(0, 4000, 30000)
+    lab = dtw_labels(s, pa, pb)
+    y = lab / lab.max()
+    enc = Encoder.init(s, seed=1)
+    hold = slice(27000, None)
+    before = spearman(enc.predict_pairs(s, pa[hold], pb[hold]), y[hold])
+    hist = enc.fit(s, pa[:27000], pb[:27000], y[:27000], epochs=6, batch_pairs=1024, lr=3e-3)
+    after = spearman(enc.predict_pairs(s, pa[hold], pb[hold]), y[hold])
+    assert hist[-1] < hist[0]
+    assert after > 0.8 and after > before + 0.1, (before, after)

@@ -20,7 +20,9 @@ FLAG_EXACT = 1
 
 # Every symbol include/tsm.h declares (checked by the test suite).
 EXPORTS = ("tsm_version", "tsm_last_error", "tsm_max_supported_len", "tsm_pairs", "tsm_matrix",
-           "tsm_sched_workspace_bytes", "tsm_pairs_sched", "tsm_topk_rows", "tsm_pairs_sched_noalloc")
+           "tsm_sched_workspace_bytes", "tsm_pairs_sched", "tsm_topk_rows", "tsm_pairs_sched_noalloc",
+           "tsm_enc_param_count", "tsm_enc_workspace_bytes", "tsm_enc_forward", "tsm_enc_loss_grad", "tsm_enc_adam",
+           "tsm_select_rows")
 
 
 class TsmParams(ctypes.Structure):
@@ -66,6 +68,20 @@ def load():
         lib.tsm_pairs_sched_noalloc.restype = ctypes.c_int
         lib.tsm_pairs_sched_noalloc.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32,
                                                 ctypes.POINTER(TsmParams), _vp, _vp, _i64, _vp]
+        lib.tsm_enc_param_count.restype = ctypes.c_int
+        lib.tsm_enc_workspace_bytes.restype = _i64
+        lib.tsm_enc_workspace_bytes.argtypes = [_i32, _i32, _i32]
+        _fp = ctypes.POINTER(ctypes.c_float)
+        lib.tsm_enc_forward.restype = ctypes.c_int
+        lib.tsm_enc_forward.argtypes = [_vp, _vp, _vp, _vp, _i32, _i32, _fp, _vp, _vp, _vp]
+        lib.tsm_enc_loss_grad.restype = ctypes.c_int
+        lib.tsm_enc_loss_grad.argtypes = [_vp, _vp, _vp, _vp, _i32, _i32, _fp, _vp, _vp, _vp, _i32, _vp, _vp, _vp,
+                                          _vp, _vp]
+        lib.tsm_enc_adam.restype = ctypes.c_int
+        lib.tsm_enc_adam.argtypes = [_vp, _vp, _vp, _vp, _i32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                     ctypes.c_float, _vp]
+        lib.tsm_select_rows.restype = ctypes.c_int
+        lib.tsm_select_rows.argtypes = [_vp, _i64, _i64, _i64, _i64, _vp, _vp]
         lib.tsm_topk_rows.restype = ctypes.c_int
         lib.tsm_topk_rows.argtypes = [_vp, _i64, _i64, _i64, _i32, _vp, _vp, _vp]
         _lib = lib

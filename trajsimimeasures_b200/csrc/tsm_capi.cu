@@ -297,6 +297,21 @@ int tsm_topk_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, in
     return TSM_OK;
 }
 
+int tsm_select_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, int64_t k, int32_t* out_idx,
+                    void* stream) {
+    g_err.clear();
+    if (n_rows < 0 || n_cols < 0 || k < 1) return fail(TSM_EINVAL, "tsm_select_rows: bad size");
+    if (n_rows == 0) return TSM_OK;
+    if (n_rows > 0x7fffffffLL || n_cols > 0x7fffffffLL) return fail(TSM_EINVAL, "tsm_select_rows: too large");
+    if (!d || !out_idx) return fail(TSM_EINVAL, "tsm_select_rows: null pointer");
+    if (ld < n_cols) return fail(TSM_EINVAL, "tsm_select_rows: ld < n_cols");
+    tsm::select_rows_kernel<<<(unsigned)n_rows, tsm::kTopkThreads, 0, (cudaStream_t)stream>>>(d, n_cols, ld, k,
+                                                                                                out_idx);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "select_rows_kernel launch");
+    return TSM_OK;
+}
+
 int tsm_sched_workspace_bytes(void) { return 256; }
 
 int tsm_pairs_sched(const float* pts, const int64_t* off_a, const int32_t* len_a, const int64_t* off_b,

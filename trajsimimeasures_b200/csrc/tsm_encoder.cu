@@ -1,0 +1,640 @@
+// Learned candidate filter: a trajectory encoder trained on DTW distances.
+//
+// Network (per trajectory of n points, coordinates normalised on the host):
+//   conv   a_t = relu(b1 + sum_{k<5, i<2} W1[c][i][k] x_{t+k-2,i})   64 channels, zero padding
+//   GRU    r = s(Wir a + bir + Whr h + bhr),  z = s(Wiz a + biz + Whz h + bhz),
+//          n = tanh(Win a + bin + r * (Whn h + bhn)),  h' = (1-z) n + z h      hidden 128
+//   head   e = Wo h_n + bo                                                      128-d embedding
+//   pair   d(a, b) = ||e_a - e_b||_2, trained with MSE against DTW / max DTW.
+// Conv and GRU weights are used as BF16 values (rounded from FP32 master
+// weights before each forward), all accumulation is FP32; the head is FP32.
+// The reference trains its learned measures the same way (MSE on
+// distance / max distance, nn/MLP_trajsimi_train.py:74-84,197-200).
+//
+// Kernels (all hand-written, SIMT FP32 FMA): at 16 trajectories per CTA the
+// GRU's per-step products are 16 x 384 x 192 multiply-adds, too small and too
+// serial (one step depends on the last) to fill tensor-core tiles; the GRU
+// kernels keep the BF16 weights resident in shared memory for all time steps
+// and step time inside the kernel.
+//
+//   enc_round_bf16    FP32 master -> BF16 weights
+//   enc_conv_fwd      conv + relu -> A [B][T][64]
+//   enc_gru_fwd       persistent GRU over T steps -> H [B][T+1][128] and gate caches
+//   enc_head_fwd      e = Wo h_last + bo
+//   enc_pair_loss     distances, MSE loss, dL/de (atomic)
+//   enc_head_bwd      dWo, dbo, dh_last
+//   enc_gru_bwd       BPTT: gate gradients G [B][T][384] (input side), dA [B][T][64]
+//   enc_gemm_tn       split-K reduction dW[m][n] += sum_k A[k][m] B[k][n]  (weight gradients)
+//   enc_conv_bwd      dW1, db1
+//   enc_adam          Adam step on the FP32 master weights
+#include <cuda_bf16.h>
+#include <cstdio>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tsm.h"
+
+int tsm_internal_fail(int code, const char* msg);
+
+namespace enc {
+
+constexpr int C1 = 64;    // conv channels
+constexpr int KW = 5;     // conv width
+constexpr int HD = 128;   // hidden
+constexpr int G3 = 384;   // 3 gates
+constexpr int ED = 128;   // embedding
+constexpr int S = 16;     // trajectories per GRU CTA
+constexpr int GRU_THREADS = 384;
+
+// parameter offsets in the flat FP32 master buffer
+constexpr int OFF_W1 = 0;                    // [64][2][5]
+constexpr int OFF_B1 = OFF_W1 + C1 * 2 * KW; // [64]
+constexpr int OFF_WIH = OFF_B1 + C1;         // [384][64]
+constexpr int OFF_BIH = OFF_WIH + G3 * C1;   // [384]
+constexpr int OFF_WHH = OFF_BIH + G3;        // [384][128]
+constexpr int OFF_BHH = OFF_WHH + G3 * HD;   // [384]
+constexpr int OFF_WO = OFF_BHH + G3;         // [128][128]
+constexpr int OFF_BO = OFF_WO + ED * HD;     // [128]
+constexpr int N_PARAMS = OFF_BO + ED;
+
+__device__ __forceinline__ float sigm(float x) { return 1.f / (1.f + expf(-x)); }
+
+// FP32 master -> BF16 copies of the conv and GRU weights (head stays FP32).
+__global__ void enc_round_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ q) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < OFF_WO) q[i] = __float2bfloat16_rn(p[i]);
+}
+
+// Normalised input coordinate i of point t of trajectory b (0 outside).
+__device__ __forceinline__ float xin(const float2* pts, int64_t off, int len, int t, int i, float4 nrm) {
+    if (t < 0 || t >= len) return 0.f;
+    const float2 v = pts[off + t];
+    return i == 0 ? (v.x - nrm.x) * nrm.z : (v.y - nrm.y) * nrm.w;
+}
+
+// A[b][t][c] = relu(conv), 0 for t >= len.  One thread per (b, t, c).
+__global__ void enc_conv_fwd(const float2* __restrict__ pts, const int64_t* __restrict__ off,
+                             const int32_t* __restrict__ len, int B, int T, float4 nrm,
+                             const __nv_bfloat16* __restrict__ wq, const float* __restrict__ p,
+                             float* __restrict__ A) {
+    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (int64_t)B * T * C1) return;
+    const int c = gid % C1;
+    const int t = (gid / C1) % T;
+    const int b = gid / ((int64_t)C1 * T);
+    const int n = len[b];
+    float a = 0.f;
+    if (t < n) {
+        float acc = p[OFF_B1 + c];
+#pragma unroll
+        for (int k = 0; k < KW; ++k)
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+                acc = fmaf(__bfloat162float(wq[OFF_W1 + (c * 2 + i) * KW + k]), xin(pts, off[b], n, t + k - 2, i, nrm), acc);
+        a = fmaxf(acc, 0.f);
+    }
+    A[gid] = a;
+}
+
+// Persistent GRU forward.  CTA = S trajectories, 384 threads (one per gate
+// row).  Shared memory: Wih^T [64][384] and Whh^T [128][384] BF16 (thread j
+// reads column j: consecutive threads, consecutive addresses), h [S][128],
+// a [S][64], gate pre-activations gi, gh [S][384].
+// Caches for the backward pass (only steps t < len are written):
+//   H [B][T+1][128] (H[b][0] = 0), R, Z, N, GHN [B][T][128] with
+//   GHN = Whn h + bhn.  hl [B][128] = h after the last valid step.
+__global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
+    const float* __restrict__ A, const int32_t* __restrict__ len, int B, int T, const __nv_bfloat16* __restrict__ wq,
+    const float* __restrict__ p, float* __restrict__ H, float* __restrict__ R, float* __restrict__ Z,
+    float* __restrict__ N, float* __restrict__ GHN, float* __restrict__ hl) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __nv_bfloat16* wih = reinterpret_cast<__nv_bfloat16*>(smraw);        // [64][384]
+    __nv_bfloat16* whh = wih + C1 * G3;                                   // [128][384]
+    float* hs = reinterpret_cast<float*>(whh + HD * G3);                  // [S][128]
+    float* as = hs + S * HD;                                              // [S][64]
+    float* gi = as + S * C1;                                              // [S][384]
+    float* gh = gi + S * G3;                                              // [S][384]
+    __shared__ int lens[S];
+    const int j = threadIdx.x;
+    const int b0 = blockIdx.x * S;
+    for (int e = j; e < G3 * C1; e += GRU_THREADS) {  // transpose into [k][j]
+        const int row = e / C1, col = e % C1;
+        wih[col * G3 + row] = wq[OFF_WIH + e];
+    }
+    for (int e = j; e < G3 * HD; e += GRU_THREADS) {
+        const int row = e / HD, col = e % HD;
+        whh[col * G3 + row] = wq[OFF_WHH + e];
+    }
+    for (int e = j; e < S * HD; e += GRU_THREADS) hs[e] = 0.f;
+    if (j < S) lens[j] = (b0 + j < B) ? len[b0 + j] : 0;
+    const float bih = p[OFF_BIH + j], bhh = p[OFF_BHH + j];
+    __syncthreads();
+    int tmax = 0;
+    for (int s = 0; s < S; ++s) tmax = max(tmax, lens[s]);
+    // H[b][0] = 0, and rows past the trajectory's length are zero too (the
+    // weight-gradient reduction multiplies every row by a gate gradient, 0
+    // past the length; the rows must hold numbers, not stale memory)
+    for (int s = 0; s < S; ++s) {
+        if (b0 + s >= B) break;
+        float* hb = H + (int64_t)(b0 + s) * (T + 1) * HD;
+        for (int e = j; e < HD; e += GRU_THREADS) hb[e] = 0.f;
+        for (int64_t e = (int64_t)(lens[s] + 1) * HD + j; e < (int64_t)(T + 1) * HD; e += GRU_THREADS) hb[e] = 0.f;
+    }
+    for (int t = 0; t < tmax; ++t) {
+        for (int e = j; e < S * C1; e += GRU_THREADS) {
+            const int s = e / C1;
+            as[e] = (b0 + s < B && t < lens[s]) ? A[((int64_t)(b0 + s) * T + t) * C1 + e % C1] : 0.f;
+        }
+        __syncthreads();
+        float ai[S], ah[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            ai[s] = bih;
+            ah[s] = bhh;
+        }
+        for (int k = 0; k < C1; k += 4) {
+            const float w0 = __bfloat162float(wih[(k + 0) * G3 + j]), w1 = __bfloat162float(wih[(k + 1) * G3 + j]);
+            const float w2 = __bfloat162float(wih[(k + 2) * G3 + j]), w3 = __bfloat162float(wih[(k + 3) * G3 + j]);
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const float4 v = *reinterpret_cast<const float4*>(as + s * C1 + k);
+                ai[s] = fmaf(w0, v.x, fmaf(w1, v.y, fmaf(w2, v.z, fmaf(w3, v.w, ai[s]))));
+            }
+        }
+        for (int k = 0; k < HD; k += 4) {
+            const float w0 = __bfloat162float(whh[(k + 0) * G3 + j]), w1 = __bfloat162float(whh[(k + 1) * G3 + j]);
+            const float w2 = __bfloat162float(whh[(k + 2) * G3 + j]), w3 = __bfloat162float(whh[(k + 3) * G3 + j]);
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const float4 v = *reinterpret_cast<const float4*>(hs + s * HD + k);
+                ah[s] = fmaf(w0, v.x, fmaf(w1, v.y, fmaf(w2, v.z, fmaf(w3, v.w, ah[s]))));
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            gi[s * G3 + j] = ai[s];
+            gh[s * G3 + j] = ah[s];
+        }
+        __syncthreads();
+        for (int e = j; e < S * HD; e += GRU_THREADS) {
+            const int s = e / HD, k = e % HD;
+            if (b0 + s < B && t < lens[s]) {
+                const float r = sigm(gi[s * G3 + k] + gh[s * G3 + k]);
+                const float z = sigm(gi[s * G3 + HD + k] + gh[s * G3 + HD + k]);
+                const float ghn = gh[s * G3 + 2 * HD + k];
+                const float n = tanhf(gi[s * G3 + 2 * HD + k] + r * ghn);
+                const float hp = hs[e];
+                const float hn = (1.f - z) * n + z * hp;
+                const int64_t o = ((int64_t)(b0 + s) * T + t) * HD + k;
+                R[o] = r;
+                Z[o] = z;
+                N[o] = n;
+                GHN[o] = ghn;
+                H[((int64_t)(b0 + s) * (T + 1) + t + 1) * HD + k] = hn;
+                hs[e] = hn;
+            }
+        }
+        __syncthreads();
+    }
+    for (int e = j; e < S * HD; e += GRU_THREADS) {
+        const int s = e / HD;
+        if (b0 + s < B) hl[(int64_t)(b0 + s) * HD + e % HD] = hs[e];
+    }
+}
+
+// E[b][o] = bo[o] + sum_k Wo[o][k] hl[b][k].  One thread per (b, o).
+__global__ void enc_head_fwd(const float* __restrict__ hl, int B, const float* __restrict__ p, float* __restrict__ E) {
+    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (int64_t)B * ED) return;
+    const int o = gid % ED;
+    const int64_t b = gid / ED;
+    float acc = p[OFF_BO + o];
+    const float* w = p + OFF_WO + o * HD;
+    const float* h = hl + b * HD;
+    for (int k = 0; k < HD; ++k) acc = fmaf(w[k], h[k], acc);
+    E[gid] = acc;
+}
+
+// One warp per pair: pred = ||E[ia]-E[ib]||, loss += (pred-y)^2 / P,
+// dE[ia] += 2 (pred-y)/P * (E[ia]-E[ib])/pred, dE[ib] -= the same.
+__global__ void enc_pair_loss(const float* __restrict__ E, const int32_t* __restrict__ ia,
+                              const int32_t* __restrict__ ib, const float* __restrict__ y, int P,
+                              float* __restrict__ pred, float* __restrict__ loss, float* __restrict__ dE) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= P) return;
+    const float* ea = E + (int64_t)ia[w] * ED;
+    const float* eb = E + (int64_t)ib[w] * ED;
+    float d[ED / 32];
+    float ss = 0.f;
+#pragma unroll
+    for (int q = 0; q < ED / 32; ++q) {
+        d[q] = ea[lane + 32 * q] - eb[lane + 32 * q];
+        ss = fmaf(d[q], d[q], ss);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    const float pr = sqrtf(ss);
+    const float err = pr - y[w];
+    if (lane == 0) {
+        pred[w] = pr;
+        if (loss) atomicAdd(loss, err * err / P);
+    }
+    if (dE && pr > 0.f) {
+        const float g = 2.f * err / (P * pr);
+#pragma unroll
+        for (int q = 0; q < ED / 32; ++q) {
+            atomicAdd(dE + (int64_t)ia[w] * ED + lane + 32 * q, g * d[q]);
+            atomicAdd(dE + (int64_t)ib[w] * ED + lane + 32 * q, -g * d[q]);
+        }
+    }
+}
+
+// dWo[o][k] += sum_b dE[b][o] hl[b][k]; dbo[o] += sum_b dE[b][o];
+// dhl[b][k] = sum_o Wo[o][k] dE[b][o].
+__global__ void enc_head_bwd_w(const float* __restrict__ dE, const float* __restrict__ hl, int B,
+                               float* __restrict__ grad) {
+    const int o = blockIdx.x;  // 128 blocks
+    const int k = threadIdx.x; // 128 threads
+    float acc = 0.f, accb = 0.f;
+    for (int b = 0; b < B; ++b) {
+        const float g = dE[(int64_t)b * ED + o];
+        acc = fmaf(g, hl[(int64_t)b * HD + k], acc);
+        accb += g;
+    }
+    grad[OFF_WO + o * HD + k] += acc;
+    if (k == 0) grad[OFF_BO + o] += accb;
+}
+
+__global__ void enc_head_bwd_h(const float* __restrict__ dE, int B, const float* __restrict__ p, float* __restrict__ dhl) {
+    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (int64_t)B * HD) return;
+    const int k = gid % HD;
+    const int64_t b = gid / HD;
+    float acc = 0.f;
+    for (int o = 0; o < ED; ++o) acc = fmaf(p[OFF_WO + o * HD + k], dE[b * ED + o], acc);
+    dhl[gid] = acc;
+}
+
+// BPTT.  CTA = S trajectories, 384 threads.  Shared memory: Whh [384][128]
+// and Wih [384][64] BF16 (row-major: thread k reads column k of row j),
+// dh [S][128], dgi/dgh [S][384].  Writes, for every step t < len:
+//   G  [B][T][384]  input-side gate gradients (d pre-activation of r, z, n)
+//   GH [B][T][384]  hidden-side (r, z as G; n multiplied by r)
+//   dA [B][T][64]   gradient of the conv output
+// and zeros for steps t >= len.
+__global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_bwd(
+    const float* __restrict__ dhl, const int32_t* __restrict__ len, int B, int T, const __nv_bfloat16* __restrict__ wq,
+    const float* __restrict__ H, const float* __restrict__ R, const float* __restrict__ Z, const float* __restrict__ N,
+    const float* __restrict__ GHN, float* __restrict__ G, float* __restrict__ GH, float* __restrict__ dA) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __nv_bfloat16* whh = reinterpret_cast<__nv_bfloat16*>(smraw);  // [384][128]
+    __nv_bfloat16* wih = whh + G3 * HD;                             // [384][64]
+    float* dh = reinterpret_cast<float*>(wih + G3 * C1);            // [S][128]
+    float* dhd = dh + S * HD;                                       // [S][128] direct part (dh * z)
+    float* dgi = dhd + S * HD;                                      // [S][384]
+    float* dgh = dgi + S * G3;                                      // [S][384]
+    __shared__ int lens[S];
+    const int tid = threadIdx.x;
+    const int b0 = blockIdx.x * S;
+    for (int e = tid; e < G3 * HD; e += GRU_THREADS) whh[e] = wq[OFF_WHH + e];
+    for (int e = tid; e < G3 * C1; e += GRU_THREADS) wih[e] = wq[OFF_WIH + e];
+    if (tid < S) lens[tid] = (b0 + tid < B) ? len[b0 + tid] : 0;
+    for (int e = tid; e < S * HD; e += GRU_THREADS) {
+        const int s = e / HD;
+        dh[e] = (b0 + s < B) ? dhl[(int64_t)(b0 + s) * HD + e % HD] : 0.f;
+    }
+    __syncthreads();
+    // zero the caches of steps beyond each length
+    for (int s = 0; s < S; ++s) {
+        if (b0 + s >= B) break;
+        const int n0 = lens[s];
+        for (int64_t e = (int64_t)n0 * G3 + tid; e < (int64_t)T * G3; e += GRU_THREADS) {
+            G[(int64_t)(b0 + s) * T * G3 + e] = 0.f;
+            GH[(int64_t)(b0 + s) * T * G3 + e] = 0.f;
+        }
+        for (int64_t e = (int64_t)n0 * C1 + tid; e < (int64_t)T * C1; e += GRU_THREADS)
+            dA[(int64_t)(b0 + s) * T * C1 + e] = 0.f;
+    }
+    int tmax = 0;
+    for (int s = 0; s < S; ++s) tmax = max(tmax, lens[s]);
+    for (int t = tmax - 1; t >= 0; --t) {
+        for (int e = tid; e < S * HD; e += GRU_THREADS) {
+            const int s = e / HD, k = e % HD;
+            float gr = 0.f, gz = 0.f, gn = 0.f, gnh = 0.f, d = 0.f;
+            if (b0 + s < B && t < lens[s]) {
+                const int64_t o = ((int64_t)(b0 + s) * T + t) * HD + k;
+                const float r = R[o], z = Z[o], n = N[o], ghn = GHN[o];
+                const float hp = H[((int64_t)(b0 + s) * (T + 1) + t) * HD + k];
+                const float g = dh[e];
+                const float dn = g * (1.f - z);
+                const float dz = g * (hp - n);
+                d = g * z;
+                gn = dn * (1.f - n * n);
+                gr = gn * ghn * r * (1.f - r);
+                gz = dz * z * (1.f - z);
+                gnh = gn * r;
+            } else {
+                d = dh[e];  // frozen step: dh passes through unchanged
+            }
+            dgi[s * G3 + k] = gr;
+            dgi[s * G3 + HD + k] = gz;
+            dgi[s * G3 + 2 * HD + k] = gn;
+            dgh[s * G3 + k] = gr;
+            dgh[s * G3 + HD + k] = gz;
+            dgh[s * G3 + 2 * HD + k] = gnh;
+            dhd[e] = d;
+        }
+        __syncthreads();
+        for (int e = tid; e < S * G3; e += GRU_THREADS) {
+            const int s = e / G3;
+            if (b0 + s < B && t < lens[s]) {
+                const int64_t o = ((int64_t)(b0 + s) * T + t) * G3 + e % G3;
+                G[o] = dgi[e];
+                GH[o] = dgh[e];
+            }
+        }
+        // outputs: 128 dh values and 64 dA values per trajectory, each a dot
+        // product over the 384 gate gradients
+        for (int e = tid; e < S * (HD + C1); e += GRU_THREADS) {
+            const int s = e / (HD + C1), q = e % (HD + C1);
+            const bool active = b0 + s < B && t < lens[s];
+            if (q < HD) {
+                float acc = dhd[s * HD + q];
+                if (active)
+                    for (int jj = 0; jj < G3; ++jj) acc = fmaf(__bfloat162float(whh[jj * HD + q]), dgh[s * G3 + jj], acc);
+                dhd[s * HD + q] = acc;
+            } else {
+                const int c = q - HD;
+                if (active) {
+                    float acc = 0.f;
+                    for (int jj = 0; jj < G3; ++jj) acc = fmaf(__bfloat162float(wih[jj * C1 + c]), dgi[s * G3 + jj], acc);
+                    dA[((int64_t)(b0 + s) * T + t) * C1 + c] = acc;
+                }
+            }
+        }
+        __syncthreads();
+        for (int e = tid; e < S * HD; e += GRU_THREADS) dh[e] = dhd[e];
+        __syncthreads();
+    }
+}
+
+// C[m][n] += sum_k A[k*lda + m] * Bm[k*ldb + n] over k in this CTA's K slice.
+// Tile 32 x 32 outputs per CTA (256 threads, 4 outputs each), K split across
+// blockIdx.z; partial sums are atomically added.  Weight gradients are
+// reductions over (trajectory, time) with K up to a few 10^5.
+// bgroup > 0: B has one extra row after every bgroup rows (H holds T+1 rows
+// per trajectory, the gate gradients T), i.e. B row = k + k / bgroup.
+__global__ void __launch_bounds__(256) enc_gemm_tn(const float* __restrict__ Am, int64_t lda,
+                                                   const float* __restrict__ Bm, int64_t ldb, int64_t K, int M,
+                                                   int Nn, int64_t kchunk, int bgroup, float* __restrict__ C,
+                                                   int ldc) {
+    __shared__ float as[32][33];
+    __shared__ float bs[32][33];
+    const int m0 = blockIdx.x * 32, n0 = blockIdx.y * 32;
+    const int64_t k_begin = (int64_t)blockIdx.z * kchunk;
+    const int64_t k_end = min(K, k_begin + kchunk);
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // ty 0..7
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int64_t k0 = k_begin; k0 < k_end; k0 += 32) {
+        for (int r = ty; r < 32; r += 8) {
+            const int64_t k = k0 + r;
+            as[r][tx] = (k < k_end && m0 + tx < M) ? Am[k * lda + m0 + tx] : 0.f;
+            const int64_t kb = bgroup > 0 ? k + k / bgroup : k;
+            bs[r][tx] = (k < k_end && n0 + tx < Nn) ? Bm[kb * ldb + n0 + tx] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < 32; ++kk) {
+            const float bv = bs[kk][tx];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] = fmaf(as[kk][ty + 8 * q], bv, acc[q]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int m = m0 + ty + 8 * q, n = n0 + tx;
+        if (m < M && n < Nn) atomicAdd(C + (int64_t)m * ldc + n, acc[q]);
+    }
+}
+
+// Column sums: out[n] += sum_k A[k*lda + n] (bias gradients).
+__global__ void enc_colsum(const float* __restrict__ Am, int64_t lda, int64_t K, int Nn, int64_t kchunk,
+                           float* __restrict__ out) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= Nn) return;
+    const int64_t k_begin = (int64_t)blockIdx.y * kchunk, k_end = min(K, k_begin + kchunk);
+    float acc = 0.f;
+    for (int64_t k = k_begin; k < k_end; ++k) acc += Am[k * lda + n];
+    atomicAdd(out + n, acc);
+}
+
+// Conv weight gradients.  One CTA per (b, t-chunk); thread per (c, i, k) of
+// the 640 weights + 64 biases accumulates over the chunk's steps.
+__global__ void enc_conv_bwd(const float2* __restrict__ pts, const int64_t* __restrict__ off,
+                             const int32_t* __restrict__ len, int B, int T, float4 nrm, const float* __restrict__ A,
+                             const float* __restrict__ dA, int tchunk, float* __restrict__ grad) {
+    const int b = blockIdx.x;
+    const int t0 = blockIdx.y * tchunk;
+    const int n = len[b];
+    const int t1 = min(n, t0 + tchunk);
+    const int q = threadIdx.x;  // 0..703
+    if (q >= C1 * 2 * KW + C1) return;
+    float acc = 0.f;
+    if (q < C1 * 2 * KW) {
+        const int c = q / (2 * KW), i = (q / KW) % 2, k = q % KW;
+        for (int t = t0; t < t1; ++t) {
+            const int64_t o = ((int64_t)b * T + t) * C1 + c;
+            const float g = A[o] > 0.f ? dA[o] : 0.f;
+            acc = fmaf(g, xin(pts, off[b], n, t + k - 2, i, nrm), acc);
+        }
+        atomicAdd(grad + OFF_W1 + q, acc);
+    } else {
+        const int c = q - C1 * 2 * KW;
+        for (int t = t0; t < t1; ++t) {
+            const int64_t o = ((int64_t)b * T + t) * C1 + c;
+            acc += A[o] > 0.f ? dA[o] : 0.f;
+        }
+        atomicAdd(grad + OFF_B1 + c, acc);
+    }
+}
+
+__global__ void enc_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                         float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float bc1, float bc2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+}
+
+}  // namespace enc
+
+// ---------------------------------------------------------------------------
+// Host orchestration (C ABI, declared in include/tsm.h)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct EncWs {  // views into the caller's workspace
+    float *A, *H, *R, *Z, *N, *GHN, *G, *GH, *dA, *hl, *E, *dE, *dhl, *pred, *loss;
+    __nv_bfloat16* wq;
+};
+
+int64_t align64(int64_t n) { return (n + 63) & ~int64_t(63); }
+
+// Lays the workspace out (base != NULL) and returns its size in floats.
+int64_t ws_layout(int B, int T, int P, float* base, EncWs* w) {
+    int64_t o = 0;
+    auto take = [&](float** dst, int64_t n) {
+        if (base) *dst = base + o;
+        o += align64(n);
+    };
+    EncWs tmp;
+    EncWs* x = w ? w : &tmp;
+    const int64_t BT = (int64_t)B * T;
+    take(&x->A, BT * enc::C1);
+    take(&x->H, (int64_t)B * (T + 1) * enc::HD);
+    take(&x->R, BT * enc::HD);
+    take(&x->Z, BT * enc::HD);
+    take(&x->N, BT * enc::HD);
+    take(&x->GHN, BT * enc::HD);
+    take(&x->G, BT * enc::G3);
+    take(&x->GH, BT * enc::G3);
+    take(&x->dA, BT * enc::C1);
+    take(&x->hl, (int64_t)B * enc::HD);
+    take(&x->E, (int64_t)B * enc::ED);
+    take(&x->dE, (int64_t)B * enc::ED);
+    take(&x->dhl, (int64_t)B * enc::HD);
+    take(&x->pred, P > 0 ? P : 1);
+    take(&x->loss, 1);
+    float* wqf = nullptr;
+    take(&wqf, (enc::N_PARAMS + 1) / 2);  // BF16 copy of the weights
+    if (base) x->wq = reinterpret_cast<__nv_bfloat16*>(wqf);
+    return o;
+}
+
+constexpr int kGruFwdSmem = (enc::C1 * enc::G3 + enc::HD * enc::G3) * 2 +
+                            (enc::S * enc::HD + enc::S * enc::C1 + 2 * enc::S * enc::G3) * 4;
+constexpr int kGruBwdSmem = (enc::G3 * enc::HD + enc::G3 * enc::C1) * 2 +
+                            (2 * enc::S * enc::HD + 2 * enc::S * enc::G3) * 4;
+
+int enc_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return TSM_OK;
+    char b[256];
+    snprintf(b, sizeof(b), "%s: %s", what, cudaGetErrorString(e));
+    return tsm_internal_fail(TSM_ECUDA, b);
+}
+
+int enc_args(const void* params, const void* pts, const void* off, const void* len, int B, int T, const float* nrm,
+             const void* ws) {
+    if (!params || !pts || !off || !len || !nrm || !ws) return tsm_internal_fail(TSM_EINVAL, "encoder: null pointer");
+    if (B < 1 || T < 1) return tsm_internal_fail(TSM_EINVAL, "encoder: batch and time must be positive");
+    if ((int64_t)B * T * enc::G3 > (int64_t)1 << 40) return tsm_internal_fail(TSM_EINVAL, "encoder: batch too large");
+    return TSM_OK;
+}
+
+int enc_forward(const float* params, const float* pts, const int64_t* off, const int32_t* len, int B, int T,
+                const float* nrm, EncWs& w, cudaStream_t s) {
+    using namespace enc;
+    const float4 n4 = make_float4(nrm[0], nrm[1], nrm[2], nrm[3]);
+    enc_round_bf16<<<(OFF_WO + 255) / 256, 256, 0, s>>>(params, w.wq);
+    const int64_t tot = (int64_t)B * T * C1;
+    enc_conv_fwd<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(reinterpret_cast<const float2*>(pts), off, len, B, T,
+                                                                n4, w.wq, params, w.A);
+    int rc = enc_check(cudaFuncSetAttribute(enc_gru_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, kGruFwdSmem),
+                       "cudaFuncSetAttribute(enc_gru_fwd)");
+    if (rc) return rc;
+    enc_gru_fwd<<<(B + S - 1) / S, GRU_THREADS, kGruFwdSmem, s>>>(w.A, len, B, T, w.wq, params, w.H, w.R, w.Z, w.N,
+                                                                   w.GHN, w.hl);
+    enc_head_fwd<<<(unsigned)(((int64_t)B * ED + 255) / 256), 256, 0, s>>>(w.hl, B, params, w.E);
+    return enc_check(cudaGetLastError(), "encoder forward launch");
+}
+
+int enc_backward(const float* params, const float* pts, const int64_t* off, const int32_t* len, int B, int T,
+                 const float* nrm, EncWs& w, float* grad, cudaStream_t s) {
+    using namespace enc;
+    const float4 n4 = make_float4(nrm[0], nrm[1], nrm[2], nrm[3]);
+    enc_head_bwd_w<<<ED, HD, 0, s>>>(w.dE, w.hl, B, grad);
+    enc_head_bwd_h<<<(unsigned)(((int64_t)B * HD + 255) / 256), 256, 0, s>>>(w.dE, B, params, w.dhl);
+    int rc = enc_check(cudaFuncSetAttribute(enc_gru_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, kGruBwdSmem),
+                       "cudaFuncSetAttribute(enc_gru_bwd)");
+    if (rc) return rc;
+    enc_gru_bwd<<<(B + S - 1) / S, GRU_THREADS, kGruBwdSmem, s>>>(w.dhl, len, B, T, w.wq, w.H, w.R, w.Z, w.N,
+                                                                   w.GHN, w.G, w.GH, w.dA);
+    // weight gradients: reductions over k = b*T + t
+    const int64_t K = (int64_t)B * T;
+    const int64_t kchunk = 2048;
+    const unsigned kz = (unsigned)((K + kchunk - 1) / kchunk);
+    enc_gemm_tn<<<dim3(G3 / 32, C1 / 32, kz), 256, 0, s>>>(w.G, G3, w.A, C1, K, G3, C1, kchunk, 0,
+                                                           grad + OFF_WIH, C1);  // dWih[j][c] += G . A
+    enc_gemm_tn<<<dim3(G3 / 32, HD / 32, kz), 256, 0, s>>>(w.GH, G3, w.H, HD, K, G3, HD, kchunk, T,
+                                                           grad + OFF_WHH, HD);  // dWhh[j][k] += GH . H[t]
+    enc_colsum<<<dim3((G3 + 127) / 128, kz), 128, 0, s>>>(w.G, G3, K, G3, kchunk, grad + OFF_BIH);
+    enc_colsum<<<dim3((G3 + 127) / 128, kz), 128, 0, s>>>(w.GH, G3, K, G3, kchunk, grad + OFF_BHH);
+    const int tchunk = 64;
+    enc_conv_bwd<<<dim3(B, (T + tchunk - 1) / tchunk), 704, 0, s>>>(reinterpret_cast<const float2*>(pts), off, len,
+                                                                    B, T, n4, w.A, w.dA, tchunk, grad);
+    return enc_check(cudaGetLastError(), "encoder backward launch");
+}
+
+}  // namespace
+
+extern "C" {
+
+int tsm_enc_param_count(void) { return enc::N_PARAMS; }
+
+int64_t tsm_enc_workspace_bytes(int32_t B, int32_t T, int32_t P) {
+    if (B < 1 || T < 1 || P < 0) return -1;
+    return ws_layout(B, T, P, nullptr, nullptr) * 4;
+}
+
+int tsm_enc_forward(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
+                    int32_t T, const float* nrm, void* workspace, float* emb, void* stream) {
+    int rc = enc_args(params, pts, off, len, B, T, nrm, workspace);
+    if (rc) return rc;
+    EncWs w;
+    ws_layout(B, T, 0, static_cast<float*>(workspace), &w);
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = enc_forward(params, pts, off, len, B, T, nrm, w, s);
+    if (rc) return rc;
+    if (emb) rc = enc_check(cudaMemcpyAsync(emb, w.E, (size_t)B * enc::ED * 4, cudaMemcpyDeviceToDevice, s),
+                            "copy embeddings");
+    return rc;
+}
+
+int tsm_enc_loss_grad(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
+                      int32_t T, const float* nrm, const int32_t* ia, const int32_t* ib, const float* y, int32_t P,
+                      void* workspace, float* grad, float* loss, float* pred, void* stream) {
+    int rc = enc_args(params, pts, off, len, B, T, nrm, workspace);
+    if (rc) return rc;
+    if (P < 1 || !ia || !ib || !y || !grad) return tsm_internal_fail(TSM_EINVAL, "tsm_enc_loss_grad: bad pairs");
+    EncWs w;
+    ws_layout(B, T, P, static_cast<float*>(workspace), &w);
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = enc_forward(params, pts, off, len, B, T, nrm, w, s);
+    if (rc) return rc;
+    if ((rc = enc_check(cudaMemsetAsync(w.dE, 0, (size_t)B * enc::ED * 4, s), "memset dE"))) return rc;
+    if ((rc = enc_check(cudaMemsetAsync(w.loss, 0, 4, s), "memset loss"))) return rc;
+    if ((rc = enc_check(cudaMemsetAsync(grad, 0, (size_t)enc::N_PARAMS * 4, s), "memset grad"))) return rc;
+    enc::enc_pair_loss<<<(P * 32 + 255) / 256, 256, 0, s>>>(w.E, ia, ib, y, P, w.pred, w.loss, w.dE);
+    rc = enc_backward(params, pts, off, len, B, T, nrm, w, grad, s);
+    if (rc) return rc;
+    if (loss) rc = enc_check(cudaMemcpyAsync(loss, w.loss, 4, cudaMemcpyDeviceToDevice, s), "copy loss");
+    if (!rc && pred) rc = enc_check(cudaMemcpyAsync(pred, w.pred, (size_t)P * 4, cudaMemcpyDeviceToDevice, s), "copy pred");
+    return rc;
+}
+
+int tsm_enc_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr, float beta1,
+                 float beta2, float eps, void* stream) {
+    if (!params || !grad || !m || !v || step < 1) return tsm_internal_fail(TSM_EINVAL, "tsm_enc_adam: bad arguments");
+    const float bc1 = 1.f - powf(beta1, (float)step), bc2 = 1.f - powf(beta2, (float)step);
+    enc::enc_adam<<<(enc::N_PARAMS + 255) / 256, 256, 0, (cudaStream_t)stream>>>(params, grad, m, v, enc::N_PARAMS, lr,
+                                                                                 beta1, beta2, eps, bc1, bc2);
+    return enc_check(cudaGetLastError(), "enc_adam launch");
+}
+
+}  // extern "C"

@@ -141,3 +141,73 @@ __global__ void __launch_bounds__(kTopkThreads) topk_rows_kernel(const float* __
 }
 
 }  // namespace tsm
+
+namespace tsm {
+
+// Unordered k-smallest selection for long candidate lists (any k <= n_cols):
+// out_i[row][0..k) receives the column indices of the k smallest values of
+// the row (the same set as the first k of a stable argsort), in no particular
+// order.  Same radix select as topk_rows_kernel; the keys below the k-th are
+// compacted straight to global memory, the ties at the k-th key fill the rest
+// in column order.
+__global__ void __launch_bounds__(kTopkThreads) select_rows_kernel(const float* __restrict__ d, int64_t n_cols,
+                                                                   int64_t ld, int64_t k, int32_t* __restrict__ out_i) {
+    __shared__ uint32_t hist[256];
+    __shared__ uint32_t s_prefix, s_need, s_nless;
+    __shared__ uint32_t warp_cnt[kTopkThreads / 32];
+    const float* row = d + (int64_t)blockIdx.x * ld;
+    int32_t* oi = out_i + (int64_t)blockIdx.x * k;
+    const int tid = threadIdx.x;
+    const uint32_t kk = (uint32_t)min(k, n_cols);
+    uint32_t prefix = 0, need = kk;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int i = tid; i < 256; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        const uint32_t hmask = (shift == 24) ? 0u : (0xffffffffu << (shift + 8));
+        for (int64_t c = tid; c < n_cols; c += blockDim.x) {
+            const uint32_t key = fkey(row[c]);
+            if ((key & hmask) == prefix) atomicAdd(&hist[(key >> shift) & 0xffu], 1u);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t acc = 0;
+            int bin = 0;
+            for (; bin < 256; ++bin) {
+                if (acc + hist[bin] >= need) break;
+                acc += hist[bin];
+            }
+            s_prefix = prefix | ((uint32_t)bin << shift);
+            s_need = need - acc;
+        }
+        __syncthreads();
+        prefix = s_prefix;
+        need = s_need;
+        __syncthreads();
+    }
+    if (tid == 0) s_nless = 0;
+    __syncthreads();
+    for (int64_t c = tid; c < n_cols; c += blockDim.x) {
+        if (fkey(row[c]) < prefix) oi[atomicAdd(&s_nless, 1u)] = (int32_t)c;
+    }
+    __syncthreads();
+    const uint32_t nless = s_nless;
+    uint32_t taken = 0;
+    for (int64_t base = 0; base < n_cols && taken < need; base += blockDim.x) {
+        const int64_t c = base + tid;
+        const bool eq = c < n_cols && fkey(row[c]) == prefix;
+        const uint32_t bal = __ballot_sync(0xffffffffu, eq);
+        if ((tid & 31) == 0) warp_cnt[tid >> 5] = __popc(bal);
+        __syncthreads();
+        uint32_t before = taken;
+        for (int w = 0; w < (tid >> 5); ++w) before += warp_cnt[w];
+        before += __popc(bal & ((1u << (tid & 31)) - 1u));
+        if (eq && before < need) oi[nless + before] = (int32_t)c;
+        uint32_t tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += warp_cnt[w];
+        __syncthreads();
+        taken += tot;
+    }
+    for (int64_t i = kk + tid; i < k; i += blockDim.x) oi[i] = -1;
+}
+
+}  // namespace tsm

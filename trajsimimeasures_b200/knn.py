@@ -104,3 +104,66 @@ def recall_at_k(approx_idx, exact_idx) -> float:
     e = np.asarray(exact_idx.cpu() if isinstance(exact_idx, torch.Tensor) else exact_idx)
     k = e.shape[1]
     return float(np.mean([len(np.intersect1d(a[i], e[i])) / k for i in range(e.shape[0])]))
+
+
+def select_rows(d: torch.Tensor, k: int, stream=None) -> torch.Tensor:
+    """Column indices (int32 [n, k], any order) of the k smallest values of
+    each row of a float32 CUDA matrix (the set of a stable argsort's first k)."""
+    if d.dtype != torch.float32 or not d.is_cuda or d.dim() != 2 or d.stride(1) != 1:
+        raise ValueError("expected a row-major float32 CUDA matrix")
+    n, m = d.shape
+    idx = torch.empty((n, k), dtype=torch.int32, device=d.device)
+    rc = _lib.load().tsm_select_rows(_ptr(d), n, m, d.stride(0), int(k), _ptr(idx), _stream_ptr(stream))
+    _lib.check(rc, "tsm_select_rows")
+    return idx
+
+
+class SurrogateIndex:
+    """Database embeddings of a trained encoder, used to pick kNN candidates:
+    the c database trajectories nearest to a query in embedding space
+    (squared L2 via one matrix product), then reranked by exact DP.
+
+    The candidate count is calibrated, not guessed: ``calibrate`` runs the
+    exhaustive search on a sample of queries and takes the smallest count of
+    a ladder whose recall@k reaches the target; if none does within the
+    speed budget, queries fall back to the exhaustive search."""
+
+    LADDER = (200, 500, 1000, 2000, 5000, 10000, 20000, 50000)
+
+    def __init__(self, encoder, D: TrajSet, batch=4096):
+        self.enc = encoder
+        self.D = D
+        self.emb = encoder.embed(D, batch=batch)
+        self.sqn = (self.emb * self.emb).sum(1)
+        self.c = None
+
+    def candidates(self, Q: TrajSet, c: int, chunk=256) -> torch.Tensor:
+        eq = self.enc.embed(Q)
+        out = torch.empty((Q.n, c), dtype=torch.int64, device=Q.device)
+        for q0 in range(0, Q.n, chunk):
+            e = eq[q0:q0 + chunk]
+            d = (e * e).sum(1, keepdim=True) + self.sqn[None, :] - 2.0 * (e @ self.emb.T)
+            out[q0:q0 + e.shape[0]] = select_rows(d.contiguous(), c).long()
+        return out
+
+    def query(self, Q: TrajSet, k=10, c=None, measure="dtw", **kw):
+        c = c or self.c
+        if c is None:  # not calibrated, or the filter could not reach the target: exhaustive
+            return knn_exhaustive(Q, self.D, k, measure, **kw)
+        cand = self.candidates(Q, min(c, self.D.n))
+        return knn_rerank(Q, self.D, cand, k, measure, **kw)
+
+    def calibrate(self, Q_sample: TrajSet, k=10, target=0.99, max_fraction=0.05, measure="dtw", **kw):
+        """-> (chosen count or None, {count: recall}) on the sample."""
+        _, exact = knn_exhaustive(Q_sample, self.D, k, measure, **kw)
+        rec = {}
+        self.c = None
+        for c in self.LADDER:
+            if c > max_fraction * self.D.n and c > self.LADDER[0]:
+                break
+            _, got = self.query(Q_sample, k, c=c, measure=measure, **kw)
+            rec[c] = recall_at_k(got, exact)
+            if rec[c] >= target:
+                self.c = c
+                break
+        return self.c, rec

@@ -1,0 +1,181 @@
+"""Learned DTW surrogate: a trajectory encoder trained on GPU-computed DTW
+distances, used as a kNN candidate filter.
+
+Network and kernels: see the C ABI (tsm_enc_* in include/tsm.h).  Training
+follows the reference's learned-measure protocol (nn/MLP_trajsimi_train.py:
+random pairs from a trajectory pool, targets = heuristic distance / max
+distance, MSE loss, Adam), with the labels computed by this library's own DTW
+kernel (tsm_pairs) on the GPU.
+
+    enc = Encoder.init(pool)                       # normalisation from the pool
+    hist = enc.fit(pool, pa, pb, labels, epochs=…)  # labels already normalised
+    emb = enc.embed(pool)                          # [n, 128] float32 on the device
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from .engine import TrajSet, _ptr, _stream_ptr, pairs_in_set
+
+EMB = 128
+# (fan_in, count) of the parameter blocks in layout order; PyTorch-style
+# uniform(-1/sqrt(k), 1/sqrt(k)) init with k = fan_in (conv: 2*5, GRU: 128,
+# head: 128)
+_BLOCKS = [("conv_w", 10, 64 * 2 * 5), ("conv_b", 10, 64), ("w_ih", 128, 384 * 64), ("b_ih", 128, 384),
+           ("w_hh", 128, 384 * 128), ("b_hh", 128, 384), ("w_o", 128, 128 * 128), ("b_o", 128, 128)]
+
+
+def spearman(a, b) -> float:
+    """Spearman rank correlation (average ranks for ties)."""
+    def ranks(x):
+        x = np.asarray(x, dtype=np.float64)
+        o = np.argsort(x, kind="stable")
+        r = np.empty(len(x))
+        r[o] = np.arange(len(x))
+        _, inv, cnt = np.unique(x, return_inverse=True, return_counts=True)
+        sums = np.bincount(inv, weights=r)
+        return sums[inv] / cnt[inv]
+    ra, rb = ranks(a), ranks(b)
+    ra -= ra.mean()
+    rb -= rb.mean()
+    return float((ra * rb).sum() / math.sqrt((ra * ra).sum() * (rb * rb).sum()))
+
+
+@dataclass
+class Encoder:
+    params: torch.Tensor                  # float32 [n_params] master weights (device)
+    nrm: np.ndarray                       # (mean_x, mean_y, 1/std_x, 1/std_y)
+    m: torch.Tensor = None
+    v: torch.Tensor = None
+    step: int = 0
+    _ws: torch.Tensor = field(default=None, repr=False)
+    _ws_key: tuple = field(default=(0, 0, 0), repr=False)
+
+    @staticmethod
+    def n_params() -> int:
+        return _lib.load().tsm_enc_param_count()
+
+    @classmethod
+    def init(cls, pool: TrajSet, seed=0, device=None):
+        dev = device or pool.device
+        g = np.random.Generator(np.random.PCG64(seed))
+        chunks = [g.uniform(-1 / math.sqrt(k), 1 / math.sqrt(k), n).astype(np.float32) for _, k, n in _BLOCKS]
+        p = np.concatenate(chunks)
+        assert p.size == cls.n_params()
+        pts = pool.pts.double()
+        mean = pts.mean(0).cpu().numpy()
+        std = pts.std(0).cpu().numpy()
+        nrm = np.array([mean[0], mean[1], 1.0 / max(std[0], 1e-12), 1.0 / max(std[1], 1e-12)], dtype=np.float32)
+        t = torch.from_numpy(p).to(dev)
+        return cls(t, nrm, torch.zeros_like(t), torch.zeros_like(t))
+
+    # -- device buffers ---------------------------------------------------------
+    def _workspace(self, B, T, P):
+        key = (B, T, P)
+        if self._ws is None or any(k > h for k, h in zip(key, self._ws_key)):
+            nb = _lib.load().tsm_enc_workspace_bytes(*[max(k, h) for k, h in zip(key, self._ws_key)])
+            if nb < 0:
+                raise ValueError("bad encoder batch shape")
+            self._ws = torch.empty(nb // 4 + 64, dtype=torch.float32, device=self.params.device)
+            self._ws_key = tuple(max(k, h) for k, h in zip(key, self._ws_key))
+        return self._ws
+
+    def _nrm_ptr(self):
+        return (ctypes.c_float * 4)(*[float(x) for x in self.nrm])
+
+    # -- inference ----------------------------------------------------------------
+    def embed(self, s: TrajSet, idx=None, batch=2048, stream=None) -> torch.Tensor:
+        """Embeddings [n, 128] of trajectories idx (default all) of s."""
+        lib = _lib.load()
+        idx = torch.arange(s.n, device=s.device) if idx is None else torch.as_tensor(idx, device=s.device).long()
+        out = torch.empty((idx.shape[0], EMB), dtype=torch.float32, device=s.device)
+        lens_h = s.lens_host if s.lens_host is not None else s.lens.cpu().numpy()
+        idx_h = idx.cpu().numpy()
+        for b0 in range(0, idx.shape[0], batch):
+            sel = idx[b0:b0 + batch]
+            B = int(sel.shape[0])
+            T = max(int(lens_h[idx_h[b0:b0 + batch]].max()), 1)
+            off, ln = s.off[sel].contiguous(), s.lens[sel].contiguous()
+            ws = self._workspace(B, T, 1)
+            rc = lib.tsm_enc_forward(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T, self._nrm_ptr(),
+                                     _ptr(ws), _ptr(out[b0:b0 + B]), _stream_ptr(stream))
+            _lib.check(rc, "tsm_enc_forward")
+        return out
+
+    # -- training -----------------------------------------------------------------
+    def loss_grad(self, s: TrajSet, tidx, ia, ib, y, stream=None):
+        """Loss, gradient and predictions for pairs (ia, ib) over the batch of
+        trajectories tidx of s.  -> (loss tensor [1], grad [n_params], pred [P])."""
+        lib = _lib.load()
+        tidx = torch.as_tensor(tidx, device=s.device).long()
+        B = int(tidx.shape[0])
+        lens_h = s.lens_host if s.lens_host is not None else s.lens.cpu().numpy()
+        T = max(int(lens_h[tidx.cpu().numpy()].max()), 1)
+        off, ln = s.off[tidx].contiguous(), s.lens[tidx].contiguous()
+        ia = torch.as_tensor(ia, device=s.device).int().contiguous()
+        ib = torch.as_tensor(ib, device=s.device).int().contiguous()
+        y = torch.as_tensor(y, device=s.device).float().contiguous()
+        P = int(ia.shape[0])
+        grad = torch.empty_like(self.params)
+        loss = torch.empty(1, dtype=torch.float32, device=s.device)
+        pred = torch.empty(P, dtype=torch.float32, device=s.device)
+        ws = self._workspace(B, T, P)
+        rc = lib.tsm_enc_loss_grad(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T, self._nrm_ptr(),
+                                   _ptr(ia), _ptr(ib), _ptr(y), P, _ptr(ws), _ptr(grad), _ptr(loss), _ptr(pred),
+                                   _stream_ptr(stream))
+        _lib.check(rc, "tsm_enc_loss_grad")
+        return loss, grad, pred
+
+    def adam(self, grad, lr=1e-3, betas=(0.9, 0.999), eps=1e-8, stream=None):
+        self.step += 1
+        rc = _lib.load().tsm_enc_adam(_ptr(self.params), _ptr(grad), _ptr(self.m), _ptr(self.v), self.step,
+                                      float(lr), float(betas[0]), float(betas[1]), float(eps), _stream_ptr(stream))
+        _lib.check(rc, "tsm_enc_adam")
+
+    def fit(self, s: TrajSet, pa, pb, y, *, epochs=5, batch_pairs=1024, lr=1e-3, seed=0, log=None):
+        """Trains on pairs (pa[i], pb[i]) of s with targets y (normalised
+        distances).  Every step encodes the 2*batch_pairs endpoints."""
+        pa, pb, y = np.asarray(pa), np.asarray(pb), np.asarray(y, dtype=np.float32)
+        rng = np.random.Generator(np.random.PCG64(seed))
+        hist = []
+        n = len(pa)
+        for ep in range(epochs):
+            perm = rng.permutation(n)
+            tot, cnt = 0.0, 0
+            for b0 in range(0, n, batch_pairs):
+                sel = perm[b0:b0 + batch_pairs]
+                P = len(sel)
+                tidx = np.concatenate([pa[sel], pb[sel]])
+                loss, grad, _ = self.loss_grad(s, tidx, np.arange(P), P + np.arange(P), y[sel])
+                self.adam(grad, lr=lr * 0.5 * (1 + math.cos(math.pi * (ep + b0 / n) / epochs)))
+                tot += float(loss.item()) * P
+                cnt += P
+            hist.append(tot / cnt)
+            if log:
+                log(f"epoch {ep}: mse {hist[-1]:.3e}")
+        return hist
+
+    def predict_pairs(self, s: TrajSet, pa, pb, batch=4096) -> np.ndarray:
+        """||e_a - e_b|| for pairs of s (normalised-distance units)."""
+        pa = np.asarray(pa)
+        pb = np.asarray(pb)
+        uniq, inv = np.unique(np.concatenate([pa, pb]), return_inverse=True)
+        e = self.embed(s, uniq, batch=batch)
+        ea = e[torch.from_numpy(inv[:len(pa)]).to(e.device)]
+        eb = e[torch.from_numpy(inv[len(pa):]).to(e.device)]
+        return torch.linalg.vector_norm(ea - eb, dim=1).cpu().numpy()
+
+
+def dtw_labels(s: TrajSet, pa, pb, batch=1 << 20):
+    """GPU DTW of pairs (pa, pb) of s (float32, the library's paired kernel)."""
+    out = []
+    for b0 in range(0, len(pa), batch):
+        d, _ = pairs_in_set("dtw", s, pa[b0:b0 + batch], pb[b0:b0 + batch])
+        out.append(d.cpu().numpy())
+    return np.concatenate(out) if out else np.zeros(0, np.float32)
