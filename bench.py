@@ -61,6 +61,16 @@ def parse():
                     help="trajectories per set (smaller cases are for profiling, not bench lines)")
     ap.add_argument("--measures", default=",".join(MEASURES), help="comma-separated subset of the six measures")
     ap.add_argument("--flush-mb", type=int, default=256, help="L2 flush buffer written before each step (0: none)")
+    ap.add_argument("--workload", choices=["allpairs", "uneven", "surrogate", "knn"], default="allpairs",
+                    help="allpairs: the benchmark line; the others measure the uneven-batch, surrogate-training "
+                         "and kNN configurations (one extra JSON line each)")
+    ap.add_argument("--n-pairs", type=int, default=500_000, help="uneven: number of pairs")
+    ap.add_argument("--pool", type=int, default=100_000, help="surrogate: trajectory pool")
+    ap.add_argument("--train-pairs", type=int, default=200_000, help="surrogate: labelled pairs")
+    ap.add_argument("--epochs", type=int, default=20, help="surrogate: training epochs")
+    ap.add_argument("--n-db", type=int, default=1_000_000, help="knn: database size")
+    ap.add_argument("--n-queries", type=int, default=1000, help="knn: queries")
+    ap.add_argument("--checkpoint", default="", help="surrogate: save / knn: load the trained encoder here")
     a = ap.parse_args()
     a.measures = [m for m in a.measures.split(",") if m]
     for m in a.measures:
@@ -232,6 +242,23 @@ def run_reference_arm(args, ws, rank):
 # our arm
 # ---------------------------------------------------------------------------
 
+def dram_traffic(measure):
+    """DRAM bytes per launch (read + write) of the dominant kernel, from the
+    committed ncu capture of the full-size launch; None if not captured."""
+    path = os.path.join(ROOT, "profiles", "hausdorff_allpairs_2000x2000_dram.txt")
+    if measure != "hausdorff" or not os.path.exists(path):
+        return None
+    vals = {}
+    for line in open(path):
+        if ":" in line and not line.startswith("#"):
+            k, v = line.split(":", 1)
+            vals[k.strip()] = v.strip()
+    try:
+        return int(vals["dram__bytes_read.sum"]) + int(vals["dram__bytes_write.sum"])
+    except (KeyError, ValueError):
+        return None
+
+
 def run_ours(args, ws, rank, local):
     import torch
     import torch.distributed as dist
@@ -336,10 +363,13 @@ def run_ours(args, ws, rank, local):
                   "ms": per_ms[m] / args.steps,
                   "fp32_issue_frac": U[m] * args.steps / sec * OPS_PER_UNIT[m] / peak_ops}
     dom = max(MEAS, key=lambda m: per_ms[m])
+    traffic = dram_traffic(dom)
     ach = per[dom]["units_per_s"] * OPS_PER_UNIT[dom]
     roof = {"bound": "fp32-issue", "kernel": f"tsm::dp_matrix_kernel<{dom}>" if dom != "hausdorff"
             else "tsm::hausdorff_matrix_kernel", "achieved": ach / 1e9, "peak": peak_ops / 1e9, "unit": "Gop/s",
-            "frac": ach / peak_ops, "traffic": None,
+            "frac": ach / peak_ops, "traffic": traffic,
+            "traffic_unit": "bytes per launch (ncu dram read + write of one full-size launch; the 16 MB result "
+                            "is written back from L2 after the kernel)" if traffic is not None else None,
             "peak_source": f"{sms} SMs x 128 FP32 lanes x {max_mhz:.0f} MHz max SM clock (not in MEASURED_PEAKS, "
                            "which has HBM copy and bf16 GEMM only)",
             "ops_per_unit": OPS_PER_UNIT[dom], "units_per_launch": U[dom]}
@@ -365,9 +395,195 @@ def run_ours(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# other configurations (one JSON line each; not the benchmark line)
+# ---------------------------------------------------------------------------
+
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def run_uneven(args):
+    """500k pairs, lognormal lengths (median 60, sigma 1, clipped 10..2000),
+    DTW + Frechet + EDR in ONE persistent launch (autotuned tile/bucket shape,
+    CUDA-graph replay), against three plain tsm_pairs launches."""
+    import torch
+    from trajsimimeasures_b200 import datagen as D, sched
+    from trajsimimeasures_b200.engine import pairs_raw, pair_order
+    t0 = time.perf_counter()
+    pts, off, lens, ia, ib = D.pairs_lognormal(args.n_pairs, seed=D.SEED_DB)
+    gen_s = time.perf_counter() - t0
+    dev = torch.device("cuda", 0)
+    up = lambda x, dt: torch.from_numpy(np.ascontiguousarray(x, dtype=dt)).to(dev)  # noqa: E731
+    la, lb = lens[ia], lens[ib]
+    T = (up(pts, np.float32), up(off[ia], np.int64), up(la, np.int32), up(off[ib], np.int64), up(lb, np.int32))
+    ms_ = ["dtw", "dfrechet", "edr"]
+    cells = float((la.astype(np.float64) * lb).sum()) * len(ms_)
+    t0 = time.perf_counter()
+    best, tried = sched.autotune(*T, ms_, eps=EPS, len_a_host=la, len_b_host=lb)
+    tune_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sc = sched.PairsScheduler(*T, ms_, eps=EPS, rows=best[0], warp_floats=best[1], len_a_host=la, len_b_host=lb)
+    plan_s = time.perf_counter() - t0
+    sc.capture()
+    for _ in range(args.warmup):
+        sc.replay()
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(args.steps):
+        sc.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_sched = e0.elapsed_time(e1) / args.steps
+    # baseline: one tsm_pairs launch per measure (tile + wave kernels, shape-sorted order)
+    order = up(pair_order(la, lb), np.int32)
+    out = torch.empty(len(ia), device=dev)
+    cnt = torch.empty(len(ia), dtype=torch.int32, device=dev)
+    mx = int(max(la.max(), lb.max()))
+
+    def plain():
+        for m in ms_:
+            pairs_raw(m, *T[:5], mx, out=out, counts=cnt if m == "edr" else None, order=order, eps=EPS)
+    for _ in range(args.warmup):
+        plain()
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(args.steps):
+        plain()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_plain = e0.elapsed_time(e1) / args.steps
+    kinds = np.bincount(sc.plan.tasks[:, 0], minlength=5).tolist()
+    print(json.dumps({
+        "workload": f"uneven_{args.n_pairs}_pairs_lognormal_dtw+dfrechet+edr", "metric": "DP cells/s",
+        "value": cells / (ms_sched / 1e3), "unit": "cells/s", "pairs_per_s": 3 * len(ia) / (ms_sched / 1e3),
+        "ms_per_launch": ms_sched, "graph_replay": True,
+        "autotuned": {"rows": best[0], "warp_floats": best[1], "candidates_ms": tried},
+        "tasks_by_kind": {"tile": kinds[0], "group8": kinds[1], "wave": kinds[2]},
+        "plain_tsm_pairs_ms": ms_plain, "speedup_vs_plain": ms_plain / ms_sched,
+        "host_s": {"generate": gen_s, "autotune": tune_s, "plan": plan_s}, "steps": args.steps,
+        "cells_per_launch": cells}), flush=True)
+
+
+def _save_encoder(enc, path, extra):
+    import torch
+    torch.save({"params": enc.params.cpu(), "m": enc.m.cpu(), "v": enc.v.cpu(), "step": enc.step,
+                "nrm": enc.nrm, **extra}, path)
+
+
+def _load_encoder(path, dev):
+    import torch
+    from trajsimimeasures_b200.surrogate import Encoder
+    ck = torch.load(path, weights_only=False)
+    enc = Encoder(ck["params"].to(dev), np.asarray(ck["nrm"], np.float32), ck["m"].to(dev), ck["v"].to(dev),
+                  int(ck["step"]))
+    return enc, ck
+
+
+def run_surrogate(args):
+    """Pool of random-walk trajectories, random pairs labelled by the GPU DTW
+    kernel, normalised by the max label; the encoder trained with MSE by the
+    library's own kernels; held-out Spearman rho; FP64-oracle error of the labels."""
+    import torch
+    from oracle import oracle as O
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.engine import TrajSet
+    from trajsimimeasures_b200.surrogate import Encoder, dtw_labels, spearman
+    dev = torch.device("cuda", 0)
+    p, o, l = D.trajectory_set(args.pool, seed=D.SEED_DB)
+    s = TrajSet.from_packed(p, o, l, device=dev)
+    rng = np.random.Generator(np.random.PCG64(D.SEED_DB))
+    n = args.train_pairs
+    pa, pb = rng.integers(0, args.pool, n), rng.integers(0, args.pool, n)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lab = dtw_labels(s, pa, pb)
+    torch.cuda.synchronize()
+    label_s = time.perf_counter() - t0
+    sample = rng.choice(n, 2000, replace=False)
+    d64, _ = O.pairs_idx(O.pairs_f64, 0, p, o, l, pa[sample], pb[sample])
+    label_err = float(np.max(np.abs(lab[sample] - d64) / d64))
+    y = lab / lab.max()
+    ntr = int(0.9 * n)
+    enc = Encoder.init(s, seed=0)
+    rho0 = spearman(enc.predict_pairs(s, pa[ntr:], pb[ntr:]), y[ntr:])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = enc.fit(s, pa[:ntr], pb[:ntr], y[:ntr], epochs=args.epochs, batch_pairs=1024, lr=2e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    pred = enc.predict_pairs(s, pa[ntr:], pb[ntr:])
+    rho = spearman(pred, y[ntr:])
+    if args.checkpoint:
+        _save_encoder(enc, args.checkpoint, {"max_label": float(lab.max()), "rho": rho})
+    print(json.dumps({
+        "workload": f"surrogate_pool{args.pool}_pairs{n}", "metric": "held-out Spearman rho", "value": rho,
+        "rho_untrained": rho0, "mse_first_epoch": hist[0], "mse_last_epoch": hist[-1], "epochs": args.epochs,
+        "train_s": train_s, "train_pairs_per_s": args.epochs * ntr / train_s, "label_s": label_s,
+        "label_pairs_per_s": n / label_s, "label_max_rel_err_vs_fp64": label_err,
+        "checkpoint": args.checkpoint or None}), flush=True)
+
+
+def run_knn(args):
+    """1k queries against a 1M database (random walks, U{20..200}): exhaustive
+    exact GPU DTW top-10 vs the calibrated learned filter + exact rerank."""
+    import torch
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.engine import TrajSet
+    from trajsimimeasures_b200.knn import SurrogateIndex, knn_exhaustive, recall_at_k
+    dev = torch.device("cuda", 0)
+    t0 = time.perf_counter()
+    dp, do, dl = D.trajectory_set(args.n_db, seed=D.SEED_DB)
+    qp, qo, ql = D.trajectory_set(args.n_queries, seed=D.SEED_QUERY)
+    gen_s = time.perf_counter() - t0
+    Dset = TrajSet.from_packed(dp, do, dl, device=dev)
+    Q = TrajSet.from_packed(qp, qo, ql, device=dev)
+    knn_exhaustive(TrajSet.from_packed(qp, qo[:4], ql[:4], device=dev), Dset, 10)  # warm
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    ex_d, ex_i = knn_exhaustive(Q, Dset, 10)
+    e1.record()
+    torch.cuda.synchronize()
+    ex_s = e0.elapsed_time(e1) / 1e3
+    out = {"workload": f"knn_{args.n_queries}q_x_{args.n_db}db_dtw_top10",
+           "exhaustive_queries_per_s": args.n_queries / ex_s, "exhaustive_s": ex_s,
+           "exhaustive_cells_per_s": float(ql.astype(np.float64).sum() * dl.astype(np.float64).sum()) / ex_s}
+    if args.checkpoint and os.path.exists(args.checkpoint):
+        enc, ck = _load_encoder(args.checkpoint, dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        index = SurrogateIndex(enc, Dset)
+        torch.cuda.synchronize()
+        build_s = time.perf_counter() - t0
+        cal = TrajSet.from_packed(*D.trajectory_set(256, seed=D.SEED_QUERY + 1), device=dev)
+        t0 = time.perf_counter()
+        c, rec = index.calibrate(cal, 10, target=0.99)
+        torch.cuda.synchronize()
+        cal_s = time.perf_counter() - t0
+        e0, e1 = _events()
+        e0.record()
+        f_d, f_i = index.query(Q, 10)
+        e1.record()
+        torch.cuda.synchronize()
+        f_s = e0.elapsed_time(e1) / 1e3
+        out.update({"filtered_queries_per_s": args.n_queries / f_s, "filtered_s": f_s, "candidates": c,
+                    "calibration_recall": {str(k): v for k, v in rec.items()},
+                    "recall_at_10": recall_at_k(f_i, ex_i), "speedup_vs_exhaustive": ex_s / f_s,
+                    "index_build_s": build_s, "calibration_s": cal_s, "encoder_rho": ck.get("rho")})
+    out["host_generate_s"] = gen_s
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
+    if args.workload != "allpairs":
+        {"uneven": run_uneven, "surrogate": run_surrogate, "knn": run_knn}[args.workload](args)
+        return
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)
         return

@@ -153,9 +153,17 @@ class SurrogateIndex:
         cand = self.candidates(Q, min(c, self.D.n))
         return knn_rerank(Q, self.D, cand, k, measure, **kw)
 
-    def calibrate(self, Q_sample: TrajSet, k=10, target=0.99, max_fraction=0.05, measure="dtw", **kw):
-        """-> (chosen count or None, {count: recall}) on the sample."""
+    def calibrate(self, Q_sample: TrajSet, k=10, target=0.99, max_fraction=0.05, margin=None, measure="dtw",
+                  **kw):
+        """-> (chosen count or None, {count: recall}) on the sample.
+
+        A count is chosen only if its sample recall clears the target by a
+        margin of two standard errors of a recall measured on n*k answers
+        (default), so that the recall on the full query set does not fall
+        below the target by sampling noise."""
         _, exact = knn_exhaustive(Q_sample, self.D, k, measure, **kw)
+        if margin is None:
+            margin = 2.0 * float(np.sqrt(target * (1.0 - target) / (Q_sample.n * k)))
         rec = {}
         self.c = None
         for c in self.LADDER:
@@ -163,7 +171,7 @@ class SurrogateIndex:
                 break
             _, got = self.query(Q_sample, k, c=c, measure=measure, **kw)
             rec[c] = recall_at_k(got, exact)
-            if rec[c] >= target:
+            if rec[c] >= min(target + margin, 1.0):
                 self.c = c
                 break
         return self.c, rec
