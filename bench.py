@@ -574,6 +574,11 @@ def run_knn(args):
                     "calibration_recall": {str(k): v for k, v in rec.items()},
                     "recall_at_10": recall_at_k(f_i, ex_i), "speedup_vs_exhaustive": ex_s / f_s,
                     "index_build_s": build_s, "calibration_s": cal_s, "encoder_rho": ck.get("rho")})
+        # what training buys: the same filter with the untrained network, same budgets
+        from trajsimimeasures_b200.surrogate import Encoder
+        raw = SurrogateIndex(Encoder.init(Dset, seed=0), Dset)
+        out["recall_at_10_untrained"] = {str(cc): recall_at_k(raw.query(Q, 10, c=cc)[1], ex_i)
+                                         for cc in sorted(set(rec) | ({c} if c else set()))}
     out["host_generate_s"] = gen_s
     print(json.dumps(out), flush=True)
 

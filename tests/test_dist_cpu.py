@@ -93,3 +93,58 @@ def test_two_rank_gloo_shards_match_single_process():
     wfull, _ = O.matrix_idx(O.pairs_f32, 4, p, o, l, p, o, l)
     np.testing.assert_array_equal(full, wfull)
     assert tmax == 11.0
+
+
+def _knn_worker(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import torch
+        from oracle import oracle as O
+        from trajsimimeasures_b200 import datagen as D
+        from trajsimimeasures_b200.knn import knn_sharded, shard_range
+        O.set_threads(1)
+        qp, qo, ql = D.trajectory_set(6, seed=41)
+        dp, do, dl = D.trajectory_set(401, seed=42)
+        s, e = shard_range(401, rank, world)
+        # the oracle stands in for this rank's kernels: local distances, local top-k
+        m, _ = O.matrix_idx(O.pairs_f32, 0, qp, qo, ql, dp, do[s:e], dl[s:e])
+        o = np.argsort(m, axis=1, kind="stable")[:, :10]
+        local = (torch.from_numpy(np.take_along_axis(m, o, 1)), torch.from_numpy(o))
+        gd, gi = knn_sharded(local, 6, 10, s)
+        if rank == 0:
+            q.put((gd.numpy(), gi.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_two_rank_gloo_knn_merge_matches_single_process():
+    from oracle import oracle as O
+    from trajsimimeasures_b200 import datagen as D
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_knn_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    gd, gi = q.get(timeout=240)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    qp, qo, ql = D.trajectory_set(6, seed=41)
+    dp, do, dl = D.trajectory_set(401, seed=42)
+    m, _ = O.matrix_idx(O.pairs_f32, 0, qp, qo, ql, dp, do, dl)
+    o = np.argsort(m, axis=1, kind="stable")[:, :10]
+    np.testing.assert_array_equal(gi, o)
+    np.testing.assert_array_equal(gd, np.take_along_axis(m, o, 1))
+
+
+def test_shard_range_covers():
+    from trajsimimeasures_b200.knn import shard_range
+    for n in (0, 1, 7, 401, 1000):
+        for w in (1, 2, 3, 8):
+            rs = [shard_range(n, r, w) for r in range(w)]
+            assert rs[0][0] == 0 and rs[-1][1] == n
+            assert all(a[1] == b[0] for a, b in zip(rs, rs[1:]))

@@ -58,3 +58,18 @@ def test_knn_exhaustive_and_rerank(oracle_mod):
     np.testing.assert_array_equal(ri.cpu().numpy(), wi)
     np.testing.assert_array_equal(rv.cpu().numpy(), wv)
     assert recall_at_k(ri, i) == 1.0
+
+
+@pytest.mark.parametrize("k", [1, 300, 5000])
+def test_select_rows_is_the_stable_argsort_set(k):
+    from trajsimimeasures_b200.knn import select_rows
+    rng = np.random.default_rng(k)
+    a = rng.random((9, 20000)).astype(np.float32)
+    a[:, ::3] = np.round(a[:, ::3], 3)  # ties at the cut
+    a[0, :] = 1.0
+    i = select_rows(torch.from_numpy(a).cuda(), k).cpu().numpy()
+    want = np.argsort(a, axis=1, kind="stable")[:, :k]
+    for r in range(a.shape[0]):
+        assert set(i[r].tolist()) == set(want[r].tolist())
+    short = select_rows(torch.from_numpy(a[:, :50].copy()).cuda(), 60).cpu().numpy()
+    assert (short[:, 50:] == -1).all() and all(set(row[:50]) == set(range(50)) for row in short)

@@ -248,3 +248,17 @@ def test_lognormal_batch(oracle_mod):
             np.testing.assert_array_equal(cnt, wcnt)
         else:
             assert rel_err(got, d64).max() <= REL_TOL, NAMES[m]
+
+
+def test_matrix_many_equals_per_measure_matrix():
+    """The e2e API (host arrays in, float64 out, results formed on the GPU and
+    copied on a side stream) gives exactly the per-measure results."""
+    from trajsimimeasures_b200 import core, datagen as D
+    t = D.unpack(*D.trajectory_set(90, seed=21))
+    P = D.pad(t)
+    L = np.array([len(x) for x in t])
+    many = core.matrix_many(["dtw", "edr", "lcss", "erp", "dfrechet", "hausdorff"], P, L, P, L, eps=EPS, gpoint=G)
+    for name, m in many.items():
+        one = core.matrix(name, P, L, P, L, eps=EPS, gpoint=G)
+        assert m.dtype == np.float64
+        np.testing.assert_array_equal(m, one, err_msg=name)

@@ -250,29 +250,45 @@ def matrix(measure, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False, rows
 
 def matrix_many(measures, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False, rows=0, stream=None):
     """Several measures over the same Q x D, one upload of each set:
-    {name: float64 [nq, nd] NumPy array}.  Host inputs only (padded arrays
-    with lengths, or lists).  Points go up as float32 from pinned memory; each
-    result comes back once, EDR/LCSS as counts normalised on the host."""
+    {name: float64 [nq, nd] NumPy array}.  Host inputs (padded arrays with
+    lengths, or lists) or TrajSets.
+
+    The float64 results are formed on the GPU as each measure finishes (EDR/LCSS
+    counts normalised in float64 exactly as on the host: count / max(n1, n2),
+    1 - count / min(n1, n2)) and copied into pinned host memory on a side
+    stream, overlapping the next measure's kernel."""
     dev = torch.device("cuda")
     qs = _set_of(Q, lenQ, dev)
     ds = qs if (D is Q and lenD is lenQ) else _set_of(D, lenD, dev)
     g = _gpoint(gpoint)
-    outs = {}
+    s = stream if stream is not None else torch.cuda.current_stream(dev)
+    copy = torch.cuda.Stream(device=dev)
+    with torch.cuda.stream(s):
+        lq = qs.lens.double()[:, None]
+        ld = ds.lens.double()[None, :]
+    host = {}
     for meas in measures:
         m = measure_id(meas)
         out = torch.empty((qs.n, ds.n), dtype=torch.float32, device=dev)
         cnt = torch.empty((qs.n, ds.n), dtype=torch.int32, device=dev) if m in (_lib.EDR, _lib.LCSS) else None
-        matrix_raw(m, qs, ds, out=out, counts=cnt, eps=eps, gpoint=g, exact=exact, rows=rows, stream=stream)
-        outs[_lib.MEASURE_NAMES[m]] = (out, cnt)
-    lq = qs.lens_host.astype(np.int64)[:, None]
-    ld = ds.lens_host.astype(np.int64)[None, :]
-    res = {}
-    for name, (out, cnt) in outs.items():
-        if cnt is not None:
-            res[name] = _normalise_counts(_lib.MEASURES[name], cnt.cpu().numpy(), lq, ld)
-        else:
-            res[name] = out.cpu().numpy().astype(np.float64)
-    return res
+        matrix_raw(m, qs, ds, out=out, counts=cnt, eps=eps, gpoint=g, exact=exact, rows=rows, stream=s)
+        with torch.cuda.stream(s):
+            if m == _lib.EDR:
+                res = cnt.double() / torch.maximum(lq, ld)
+            elif m == _lib.LCSS:
+                res = 1.0 - cnt.double() / torch.minimum(lq, ld)
+            else:
+                res = out.double()
+        done = torch.cuda.Event()
+        done.record(s)
+        h = torch.empty(res.shape, dtype=torch.float64, pin_memory=True)
+        copy.wait_event(done)
+        with torch.cuda.stream(copy):
+            h.copy_(res, non_blocking=True)
+        res.record_stream(copy)
+        host[_lib.MEASURE_NAMES[m]] = h
+    copy.synchronize()
+    return {k: v.numpy() for k, v in host.items()}
 
 
 def dtw_matrix(Q, lenQ, D, lenD, **kw):

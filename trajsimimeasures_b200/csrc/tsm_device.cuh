@@ -99,8 +99,8 @@ template <bool EXACT>
 struct DtwCell {
     static constexpr bool kGap = false;
     __device__ __forceinline__ static float corner() { return 0.f; }
-    __device__ __forceinline__ static float rowb(float /*srow*/) { return CUDART_INF_F; }
-    __device__ __forceinline__ static float topb(float /*scol*/) { return CUDART_INF_F; }
+    __device__ __forceinline__ static float rowb(float /*srow*/, int /*i*/) { return CUDART_INF_F; }
+    __device__ __forceinline__ static float topb(float /*scol*/, int /*j*/) { return CUDART_INF_F; }
     __device__ __forceinline__ static float cell(float dg, float up, float left, float d2,
                                                  float /*grow*/, float /*gcol*/, float /*eps2*/) {
         return __fadd_rn(tsqrt<EXACT>(d2), min3f(dg, up, left));
@@ -113,8 +113,8 @@ template <bool EXACT>
 struct FrechetCell {
     static constexpr bool kGap = false;
     __device__ __forceinline__ static float corner() { return 0.f; }
-    __device__ __forceinline__ static float rowb(float) { return CUDART_INF_F; }
-    __device__ __forceinline__ static float topb(float) { return CUDART_INF_F; }
+    __device__ __forceinline__ static float rowb(float, int) { return CUDART_INF_F; }
+    __device__ __forceinline__ static float topb(float, int) { return CUDART_INF_F; }
     __device__ __forceinline__ static float cell(float dg, float up, float left, float d2,
                                                  float, float, float) {
         return fmaxf(d2, min3f(dg, up, left));
@@ -127,8 +127,8 @@ template <bool EXACT>
 struct ErpCell {
     static constexpr bool kGap = true;
     __device__ __forceinline__ static float corner() { return 0.f; }
-    __device__ __forceinline__ static float rowb(float srow) { return srow; }
-    __device__ __forceinline__ static float topb(float scol) { return scol; }
+    __device__ __forceinline__ static float rowb(float srow, int) { return srow; }
+    __device__ __forceinline__ static float topb(float scol, int) { return scol; }
     __device__ __forceinline__ static float cell(float dg, float up, float left, float d2,
                                                  float grow, float gcol, float) {
         return min3f(__fadd_rn(left, gcol), __fadd_rn(up, grow), __fadd_rn(dg, tsqrt<EXACT>(d2)));
@@ -136,17 +136,21 @@ struct ErpCell {
 };
 
 // EDR count: C = min(dg + sub, up + 1, left + 1), sub = (d2 < eps2) ? 0 : 1,
-// every border 0 (core/edr.py:30,41-44).  Counts are exact in FP32.
+// every border 0 (core/edr.py:30,41-44).  The kernels carry the offset value
+// F(i,j) = C(i,j) - (i+j) instead of C: then F = min(F_dg + sub - 2, F_up,
+// F_left) (two additions fewer per cell), with borders F(i,-1) = 1 - i,
+// F(-1,j) = 1 - j, F(-1,-1) = 2, and C(n1-1,n2-1) = F + n1 + n2 - 2.  All
+// values are small integers, exact in FP32.
 template <bool EXACT>
 struct EdrCell {
     static constexpr bool kGap = false;
-    __device__ __forceinline__ static float corner() { return 0.f; }
-    __device__ __forceinline__ static float rowb(float) { return 0.f; }
-    __device__ __forceinline__ static float topb(float) { return 0.f; }
+    __device__ __forceinline__ static float corner() { return 2.f; }
+    __device__ __forceinline__ static float rowb(float, int i) { return (float)(1 - i); }
+    __device__ __forceinline__ static float topb(float, int j) { return (float)(1 - j); }
     __device__ __forceinline__ static float cell(float dg, float up, float left, float d2,
                                                  float, float, float eps2) {
-        float sub = (d2 < eps2) ? 0.f : 1.f;
-        return min3f(__fadd_rn(dg, sub), __fadd_rn(up, 1.f), __fadd_rn(left, 1.f));
+        const float s = (d2 < eps2) ? -2.f : -1.f;
+        return min3f(__fadd_rn(dg, s), up, left);
     }
 };
 
@@ -157,8 +161,8 @@ template <bool EXACT>
 struct LcssCell {
     static constexpr bool kGap = false;
     __device__ __forceinline__ static float corner() { return 0.f; }
-    __device__ __forceinline__ static float rowb(float) { return 0.f; }
-    __device__ __forceinline__ static float topb(float) { return 0.f; }
+    __device__ __forceinline__ static float rowb(float, int) { return 0.f; }
+    __device__ __forceinline__ static float topb(float, int) { return 0.f; }
     __device__ __forceinline__ static float cell(float dg, float up, float left, float d2,
                                                  float, float, float eps2) {
         float m = (d2 < eps2) ? 1.f : 0.f;
@@ -187,7 +191,7 @@ __device__ __forceinline__ void finalize(float dlast, int n1, int n2, float& out
     } else if constexpr (M == ERP) {
         out = (n1 == 0 || n2 == 0) ? 0.f : dlast;
     } else if constexpr (M == EDR) {
-        count = (n1 == 0 || n2 == 0) ? 0 : __float2int_rn(dlast);
+        count = (n1 == 0 || n2 == 0) ? 0 : __float2int_rn(dlast) + n1 + n2 - 2;  // undo the (i+j) offset
         out = __fdiv_rn((float)count, (float)max(n1, n2));
     } else {  // LCSS
         count = (n1 == 0 || n2 == 0) ? 0 : __float2int_rn(dlast);

@@ -90,7 +90,6 @@ __device__ __forceinline__ void group_task(const PairsArgs& A, int first, int co
         srow = __shfl_sync(0xffffffffu, srow, lane - u);
         scol = __shfl_sync(0xffffffffu, scol, lane - u);
     }
-    const float topb = C::topb(scol), rowb = C::rowb(srow);
     const int n_strips = (nr + R - 1) / R;
     const int T = nc > G ? nc : G;
     const int last = n_strips - 1;
@@ -122,14 +121,14 @@ __device__ __forceinline__ void group_task(const PairsArgs& A, int first, int co
                     rx[r] = px[r];
                     ry[r] = py[r];
                     rg[r] = C::kGap ? gapdist<EXACT>(px[r], py[r], p) : 0.f;
-                    D[r] = rowb;
+                    D[r] = C::rowb(srow, g * R + r);
                     const float2 q = __ldg(rowp + min((g + G) * R + r, nr - 1));
                     px[r] = q.x;
                     py[r] = q.y;
                 }
-                diag = (g == 0) ? C::corner() : rowb;
+                diag = (g == 0) ? C::corner() : C::rowb(srow, g * R - 1);
             }
-            const float top = (u == 0) ? ((m == 0) ? topb : ring[j]) : from_left;
+            const float top = (u == 0) ? ((m == 0) ? C::topb(scol, j) : ring[j]) : from_left;
             const float2 c2 = cnext;
             cnext = __ldg(colp + min(j + 1, nc - 1));
             const float gc = C::kGap ? gapdist<EXACT>(c2.x, c2.y, p) : 0.f;

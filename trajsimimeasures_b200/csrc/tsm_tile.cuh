@@ -63,7 +63,7 @@ struct RowBlock {
 
     // rows i0 .. i0+R-1; rows past the end repeat the last point (their
     // values are never read by a valid cell)
-    __device__ __forceinline__ void load(const float2* __restrict__ rowp, int i0, int nr, float rowb,
+    __device__ __forceinline__ void load(const float2* __restrict__ rowp, int i0, int nr, float srow,
                                          const KParams& p) {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -71,7 +71,7 @@ struct RowBlock {
             x[r] = q.x;
             y[r] = q.y;
             g[r] = C::kGap ? gapdist<EXACT>(q.x, q.y, p) : 0.f;
-            D[r] = rowb;
+            D[r] = C::rowb(srow, i0 + r);
         }
     }
 
@@ -137,19 +137,18 @@ __device__ __forceinline__ float dp_pair(const float2* __restrict__ rowp, int nr
                                          int nc, float* buf, const KParams& p, float srow, float scol) {
     using C = typename CellOf<M, EXACT>::type;
     if (nr <= 0 || nc <= 0) return 0.f;
-    const float topb = C::topb(scol), rowb = C::rowb(srow);
-    for (int j = 0; j < nc; ++j) buf[32 * j] = topb;
+    for (int j = 0; j < nc; ++j) buf[32 * j] = C::topb(scol, j);
     float dlast = 0.f;
     int rb = 0;
     for (; nr - rb > R; rb += 2 * R) {
         RowBlock<C, R, EXACT> hi, lo;
-        hi.load(rowp, rb, nr, rowb, p);
-        lo.load(rowp, rb + R, nr, rowb, p);
+        hi.load(rowp, rb, nr, srow, p);
+        lo.load(rowp, rb + R, nr, srow, p);
         float HA[R], HB[R], LA[R], LB[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            HA[r] = rowb;
-            LA[r] = rowb;
+            HA[r] = hi.D[r];
+            LA[r] = lo.D[r];
         }
         float top = buf[0];
         float4 c = col4<EXACT>(cols, 0, p, C::kGap);
@@ -157,8 +156,8 @@ __device__ __forceinline__ float dp_pair(const float2* __restrict__ rowp, int nr
         float4 cn = col4<EXACT>(cols, j1, p, C::kGap);
         float tn = buf[32 * j1];
         // step 0: the upper block's column 0 (HA -> HB); the lower block waits in LA
-        float ub1 = hi.step2(HA, HB, c, top, (rb == 0) ? C::corner() : rowb, p.eps2);
-        float ub2 = rowb, udiag = top;
+        float ub1 = hi.step2(HA, HB, c, top, (rb == 0) ? C::corner() : C::rowb(srow, rb - 1), p.eps2);
+        float ub2 = C::rowb(srow, rb + R - 1), udiag = top;
         float4 cprev = c;
         // steps 1 .. nc-1: upper column j, lower column j-1
         auto pair_step = [&](const float (&Hi)[R], float (&Ho)[R], const float (&Li)[R], float (&Lo)[R], int j) {
@@ -203,8 +202,8 @@ __device__ __forceinline__ float dp_pair(const float2* __restrict__ rowp, int nr
     }
     if (rb < nr) {  // last rows (at most R): one block
         RowBlock<C, R, EXACT> blk;
-        blk.load(rowp, rb, nr, rowb, p);
-        float diag = (rb == 0) ? C::corner() : rowb;
+        blk.load(rowp, rb, nr, srow, p);
+        float diag = (rb == 0) ? C::corner() : C::rowb(srow, rb - 1);
         float4 cn = col4<EXACT>(cols, 0, p, C::kGap);
         float tn = buf[0];
         for (int j = 0; j < nc; ++j) {

@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(128) dp_wave_kernel(
         srow = __shfl_sync(0xffffffffu, srow, 0);
         scol = __shfl_sync(0xffffffffu, scol, 0);
     }
-    const float topb = C::topb(scol), rowb = C::rowb(srow);
+
     const int n_strips = (nr + R - 1) / R;
     const int T = nc > 32 ? nc : 32;
     const int last_strip = n_strips - 1;
@@ -106,15 +106,15 @@ __global__ void __launch_bounds__(128) dp_wave_kernel(
                     rx[r] = px[r];
                     ry[r] = py[r];
                     rg[r] = C::kGap ? gapdist<EXACT>(px[r], py[r], p) : 0.f;
-                    D[r] = rowb;
+                    D[r] = C::rowb(srow, g * R + r);
                     const float2 q = __ldg(rowp + min((g + 32) * R + r, nr - 1));
                     px[r] = q.x;
                     py[r] = q.y;
                 }
-                diag = (g == 0) ? C::corner() : rowb;
+                diag = (g == 0) ? C::corner() : C::rowb(srow, g * R - 1);
             }
             float top;
-            if (lane == 0) top = (m == 0) ? topb : ring[j];
+            if (lane == 0) top = (m == 0) ? C::topb(scol, j) : ring[j];
             else top = from_left;
             const float4 c = cols[j];
             float up = top, dg = diag;

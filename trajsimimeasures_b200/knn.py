@@ -175,3 +175,39 @@ class SurrogateIndex:
                 self.c = c
                 break
         return self.c, rec
+
+
+def merge_topk(dists: torch.Tensor, idx: torch.Tensor, k: int):
+    """Merge candidate lists [nq, m] (values, global indices) into the k
+    smallest per row, ties to the smaller index (the order of a stable
+    argsort over the whole database).  Device-agnostic tensor ops."""
+    o = torch.argsort(idx, dim=1, stable=True)
+    d = torch.gather(dists, 1, o)
+    i = torch.gather(idx, 1, o)
+    o2 = torch.argsort(d, dim=1, stable=True)[:, :k]
+    return torch.gather(d, 1, o2), torch.gather(i, 1, o2)
+
+
+def shard_range(n: int, rank: int, world: int):
+    """Contiguous database shard [start, end) of a rank (sizes differ by <= 1)."""
+    base, extra = divmod(n, world)
+    start = rank * base + min(rank, extra)
+    return start, start + base + (1 if rank < extra else 0)
+
+
+def knn_sharded(local_topk, Q_n: int, k: int, shard_start: int, group=None):
+    """Multi-GPU kNN merge.  local_topk = (dist [nq, k], index [nq, k]) of this
+    rank's database shard, indices local to the shard; returns the global
+    (dist, index) on every rank after one all-gather of the lists (the only
+    exchange: nq * k * 12 bytes per rank)."""
+    import torch.distributed as dist
+    d, i = local_topk
+    i = i.long() + shard_start
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size(group) == 1:
+        return merge_topk(d, i, k)
+    w = dist.get_world_size(group)
+    ds = [torch.empty_like(d) for _ in range(w)]
+    is_ = [torch.empty_like(i) for _ in range(w)]
+    dist.all_gather(ds, d.contiguous(), group=group)
+    dist.all_gather(is_, i.contiguous(), group=group)
+    return merge_topk(torch.cat(ds, 1), torch.cat(is_, 1), k)
