@@ -61,7 +61,7 @@ def parse():
                     help="trajectories per set (smaller cases are for profiling, not bench lines)")
     ap.add_argument("--measures", default=",".join(MEASURES), help="comma-separated subset of the six measures")
     ap.add_argument("--flush-mb", type=int, default=256, help="L2 flush buffer written before each step (0: none)")
-    ap.add_argument("--workload", choices=["allpairs", "uneven", "surrogate", "knn"], default="allpairs",
+    ap.add_argument("--workload", choices=["allpairs", "uneven", "surrogate", "knn", "sym"], default="allpairs",
                     help="allpairs: the benchmark line; the others measure the uneven-batch, surrogate-training "
                          "and kNN configurations (one extra JSON line each)")
     ap.add_argument("--n-pairs", type=int, default=500_000, help="uneven: number of pairs")
@@ -191,6 +191,32 @@ def cpu_reference_run(q, d, rows, threads):
         rs.close()
     kinds = sorted({v["kind"] for v in per.values()})
     return tot_u, tot_t, per, "+".join(kinds)
+
+
+def parity_sample(q, d, outs, cnts, rows):
+    """Checks rows `rows` of the GPU results of the timed step against the
+    oracle: max/median relative error vs the FP64 restatement for the
+    distance measures, count mismatches vs the FP32 same-arithmetic twin for
+    EDR/LCSS (which must be 0)."""
+    import torch
+    from oracle import oracle as O
+    from trajsimimeasures_b200 import datagen as D
+    qp, qo, ql = q
+    dp, do, dl = d
+    res = {}
+    for name in MEASURES:
+        m = MID[name]
+        if m in (1, 2):
+            _, c32 = O.matrix_idx(O.pairs_f32, m, qp, qo[rows], ql[rows], dp, do, dl, eps=EPS, gpoint=D.BOX_CENTRE)
+            got = cnts[name][torch.as_tensor(rows, device=cnts[name].device)].cpu().numpy()
+            res[name] = {"count_mismatches": int((got != c32).sum()), "pairs": int(got.size)}
+        else:
+            d64, _ = O.matrix_idx(O.pairs_f64, m, qp, qo[rows], ql[rows], dp, do, dl, eps=EPS, gpoint=D.BOX_CENTRE)
+            got = outs[name][torch.as_tensor(rows, device=outs[name].device)].cpu().numpy().astype(np.float64)
+            with np.errstate(invalid="ignore", divide="ignore"):
+                r = np.abs(got - d64) / np.maximum(np.abs(d64), 1e-30)
+            res[name] = {"max_rel_err": float(r.max()), "median_rel_err": float(np.median(r)), "pairs": int(got.size)}
+    return res
 
 
 def cpu_sample_rows(q, d, target_s, threads):
@@ -362,6 +388,8 @@ def run_ours(args, ws, rank, local):
         per[m] = {"units_per_s": U[m] * args.steps / sec, "pairs_per_s": nq * nd * args.steps / sec,
                   "ms": per_ms[m] / args.steps,
                   "fp32_issue_frac": U[m] * args.steps / sec * OPS_PER_UNIT[m] / peak_ops}
+        if m in ("dtw", "erp"):  # one MUFU sqrt per cell; the SFU pipe runs 16 lanes per SM per clock
+            per[m]["sfu_frac"] = U[m] * args.steps / sec / (sms * 16 * max_mhz * 1e6)
     dom = max(MEAS, key=lambda m: per_ms[m])
     traffic = dram_traffic(dom)
     ach = per[dom]["units_per_s"] * OPS_PER_UNIT[dom]
@@ -392,6 +420,7 @@ def run_ours(args, ws, rank, local):
                                 "seconds": tcpu,
                                 "sample": f"rows 0..{len(rows) - 1} of the 2000x2000 block x 6 measures "
                                           "(reference C++ for DTW/ERP/Frechet/Hausdorff, FP64 port for EDR/LCSS)"}
+        line["cpu_baseline"]["parity_rows_0_3"] = parity_sample(q, d, outs, cnts, np.arange(4))
     print(json.dumps(line), flush=True)
 
 
@@ -564,12 +593,29 @@ def run_knn(args):
         c, rec = index.calibrate(cal, 10, target=0.99)
         torch.cuda.synchronize()
         cal_s = time.perf_counter() - t0
-        e0, e1 = _events()
-        e0.record()
-        f_d, f_i = index.query(Q, 10)
-        e1.record()
+        # median of 5 timed queries (one query call is ~0.1 s: single shots are noisy)
+        reps = []
+        for _ in range(5):
+            e0, e1 = _events()
+            e0.record()
+            f_d, f_i = index.query(Q, 10)
+            e1.record()
+            torch.cuda.synchronize()
+            reps.append(e0.elapsed_time(e1) / 1e3)
+        f_s = float(np.median(reps))
+        # phase split of one query call: candidate selection (embedding + scan + select), exact rerank
+        from trajsimimeasures_b200.knn import knn_rerank
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record()
+        cand = index.candidates(Q, min(c, Dset.n)) if c else None
+        ev[1].record()
+        if cand is not None:
+            knn_rerank(Q, Dset, cand, 10)
+        ev[2].record()
         torch.cuda.synchronize()
-        f_s = e0.elapsed_time(e1) / 1e3
+        out["filtered_phase_s"] = {"candidates": ev[0].elapsed_time(ev[1]) / 1e3,
+                                   "rerank": ev[1].elapsed_time(ev[2]) / 1e3}
+        out["filtered_reps_s"] = reps
         out.update({"filtered_queries_per_s": args.n_queries / f_s, "filtered_s": f_s, "candidates": c,
                     "calibration_recall": {str(k): v for k, v in rec.items()},
                     "recall_at_10": recall_at_k(f_i, ex_i), "speedup_vs_exhaustive": ex_s / f_s,
@@ -583,11 +629,50 @@ def run_knn(args):
     print(json.dumps(out), flush=True)
 
 
+def run_sym(args):
+    """Symmetric all-pairs of one 2000-trajectory set (the clustering shape):
+    the upper-triangle driver (tsm_allpairs_sym, each unordered pair once,
+    mirrored) against the full Q == D matrix, per measure, device time."""
+    import torch
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.engine import TrajSet, allpairs_sym_raw, matrix_raw
+    dev = torch.device("cuda", 0)
+    p, o, l = D.trajectory_set(args.n_traj, seed=D.SEED_DB)
+    s = TrajSet.from_packed(p, o, l, device=dev)
+    n = s.n
+    order = s.order_by_length()
+    out = torch.empty((n, n), dtype=torch.float32, device=dev)
+    cnt = torch.empty((n, n), dtype=torch.int32, device=dev)
+    res = {}
+    for name in MEASURES:
+        m = MID[name]
+        c = cnt if m in (1, 2) else None
+        full = lambda: matrix_raw(m, s, s, out=out, counts=c, d_order=order, eps=EPS, gpoint=D.BOX_CENTRE)
+        sym = lambda: allpairs_sym_raw(m, s, out=out, counts=c, eps=EPS, gpoint=D.BOX_CENTRE)
+        t = {}
+        for key, fn in (("full_ms", full), ("sym_ms", sym)):
+            for _ in range(args.warmup):
+                fn()
+            e0, e1 = _events()
+            e0.record()
+            for _ in range(args.steps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            t[key] = e0.elapsed_time(e1) / args.steps
+        t["unique_pairs_per_s_sym"] = n * (n + 1) / 2 / (t["sym_ms"] / 1e3)
+        t["speedup"] = t["full_ms"] / t["sym_ms"]
+        res[name] = t
+    print(json.dumps({"workload": f"allpairs_symmetric_{n}_six_measures", "n_traj": n, "per_measure": res,
+                      "total_full_ms": sum(v["full_ms"] for v in res.values()),
+                      "total_sym_ms": sum(v["sym_ms"] for v in res.values())}), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
     if args.workload != "allpairs":
-        {"uneven": run_uneven, "surrogate": run_surrogate, "knn": run_knn}[args.workload](args)
+        {"uneven": run_uneven, "surrogate": run_surrogate, "knn": run_knn, "sym": run_sym}[args.workload](args)
         return
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)

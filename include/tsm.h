@@ -114,6 +114,23 @@ int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int3
                float* out, int64_t ld_out, int32_t* out_counts, void* stream);
 
 /*
+ * Symmetric all pairs of one set S (the clustering shape):
+ *   out[i*ld_out + j] = out[j*ld_out + i] = measure(S_i, S_j),  i, j < n,
+ * computing each unordered pair once (every measure here is symmetric, and
+ * the kernels' values are bitwise symmetric, so the mirror equals the value
+ * computed the other way round).  Replaces the upper-triangle pair
+ * enumeration + batched core.<measure> calls of test_clustering_time.py:219-269.
+ *   order int32 [n]: a permutation of 0..n-1, S sorted by length (required:
+ *         the triangle is taken in this order, so neighbouring threads get
+ *         trajectories of similar length)
+ *   max_len: upper bound of the lengths in S
+ *   out float32 [n][ld_out]; out_counts int32 [n][ld_out] or NULL (EDR/LCSS)
+ */
+int tsm_allpairs_sym(int measure, const float* pts, const int64_t* off, const int32_t* len, const int32_t* order,
+                     int64_t n, int32_t max_len, const tsm_params* params, float* out, int64_t ld_out,
+                     int32_t* out_counts, void* stream);
+
+/*
  * Scheduled paired batch: one persistent launch over a task list that the
  * planner (trajsimimeasures_b200.sched) builds from the pair lengths.  It
  * replaces the same reference call as tsm_pairs (core.<measure>(t1, len1,

@@ -65,6 +65,13 @@ def test_invalid_arguments_fail_before_cuda(lib):
     rc = lib.tsm_matrix(0, dummy, dummy, dummy, 3, 10, dummy, dummy, dummy, nul, 3, 10, ctypes.byref(p), dummy, 2,
                         nul, nul)
     assert rc == -1 and b"ld_out" in lib.tsm_last_error()
+    rc = lib.tsm_allpairs_sym(0, dummy, dummy, dummy, nul, 3, 10, ctypes.byref(p), dummy, 3, nul, nul)
+    assert rc == -1 and b"null pointer" in lib.tsm_last_error()
+    rc = lib.tsm_allpairs_sym(0, dummy, dummy, dummy, dummy, 3, 10, ctypes.byref(p), dummy, 2, nul, nul)
+    assert rc == -1 and b"ld_out" in lib.tsm_last_error()
+    rc = lib.tsm_allpairs_sym(7, dummy, dummy, dummy, dummy, 3, 10, ctypes.byref(p), dummy, 3, nul, nul)
+    assert rc == -1 and b"unknown measure" in lib.tsm_last_error()
+    assert lib.tsm_allpairs_sym(0, nul, nul, nul, nul, 0, 10, ctypes.byref(p), nul, 0, nul, nul) == 0
     with pytest.raises(_lib.TsmError):
         _lib.check(-1, "x")
 

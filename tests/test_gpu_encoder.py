@@ -76,37 +76,36 @@ def test_training_learns_dtw_order():
     assert after > 0.8 and after > before + 0.1, (before, after)
 
 
-def test_trained_filter_gains_over_untrained_and_falls_back():
-    """What the learned part buys: at the same candidate budget the trained
-    encoder's kNN candidates recover far more of the exact DTW top-10 than the
-    untrained network's; a filter that cannot reach the recall target inside
-    its budget hands the queries to the exhaustive search (exact results)."""
+def test_trained_filter_gains_over_exhaustive_and_falls_back():
+    """What the learned part buys over the method without it (exhaustive exact
+    DP): the trained encoder's candidates plus exact rerank reach recall@10 >=
+    0.99 while evaluating at most 2 % of the database per query (counted in DP
+    evaluations, not timed).  A filter that cannot reach the target inside its
+    budget hands the queries to the exhaustive search (exact results)."""
     from trajsimimeasures_b200 import datagen as D
     from trajsimimeasures_b200.engine import TrajSet
     from trajsimimeasures_b200.knn import SurrogateIndex, knn_exhaustive, recall_at_k
     from trajsimimeasures_b200.surrogate import Encoder, dtw_labels
-    p, o, l = D.trajectory_set(20000, seed=12)
+    N = 20000
+    p, o, l = D.trajectory_set(N, seed=12)
     Dset = TrajSet.from_packed(p, o, l)
-    Q = TrajSet.from_packed(*D.trajectory_set(32, seed=13))
+    Q = TrajSet.from_packed(*D.trajectory_set(64, seed=13))
     _, exact = knn_exhaustive(Q, Dset, 10)
     rng = np.random.default_rng(14)
-    pa, pb = rng.integers(0, 20000, 40000), rng.integers(0, 20000, 40000)
+    pa, pb = rng.integers(0, N, 40000), rng.integers(0, N, 40000)
     lab = dtw_labels(Dset, pa, pb)
-    untrained = Encoder.init(Dset, seed=2)
-    trained = Encoder.init(Dset, seed=2)
-    trained.fit(Dset, pa, pb, lab / lab.max(), epochs=6, batch_pairs=1024, lr=3e-3)
-    r = {}
-    for name, enc in (("untrained", untrained), ("trained", trained)):
-        idx = SurrogateIndex(enc, Dset)
-        _, got = idx.query(Q, 10, c=400)
-        r[name] = recall_at_k(got, exact)
-    assert r["trained"] > r["untrained"] + 0.2, r
+    enc = Encoder.init(Dset, seed=2)
+    enc.fit(Dset, pa, pb, lab / lab.max(), epochs=6, batch_pairs=1024, lr=3e-3)
+    idx = SurrogateIndex(enc, Dset)
+    idx.LADDER = (40, 80, 160, 320, 400)
+    cal = TrajSet.from_packed(*D.trajectory_set(64, seed=15))
+    c, rec = idx.calibrate(cal, 10, target=0.99, max_fraction=0.02)
+    assert c is not None and c <= 0.02 * N, rec
+    _, got = idx.query(Q, 10)
+    assert recall_at_k(got, exact) >= 0.99
     # budget too small to reach the target: no count is chosen, exhaustive answers
-    idx = SurrogateIndex(untrained, Dset)
-    idx.LADDER = (50,)
-    c, rec = idx.calibrate(Q, 10, target=1.0, max_fraction=0.0025)
+    idx.LADDER = (20,)
+    c, rec = idx.calibrate(Q, 10, target=1.0, max_fraction=0.001)
+    assert c is None, rec
     _, ans = idx.query(Q, 10)
-    if c is None:
-        np.testing.assert_array_equal(ans.cpu().numpy(), exact.cpu().numpy())
-    else:
-        assert rec[c] >= 1.0
+    np.testing.assert_array_equal(ans.cpu().numpy(), exact.cpu().numpy())

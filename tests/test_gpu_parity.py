@@ -262,3 +262,44 @@ def test_matrix_many_equals_per_measure_matrix():
         one = core.matrix(name, P, L, P, L, eps=EPS, gpoint=G)
         assert m.dtype == np.float64
         np.testing.assert_array_equal(m, one, err_msg=name)
+
+
+@pytest.mark.parametrize("m", MEAS)
+def test_allpairs_sym_equals_full_matrix(m):
+    """The symmetric driver (upper triangle in length order, mirrored) gives
+    the full Q == D matrix bit for bit, counts included, in both modes, on a
+    ragged set (lengths 1..400, near-duplicates for EDR/LCSS matches) that
+    spans several 128-trajectory chunks."""
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.engine import TrajSet, allpairs_sym_raw, matrix
+    rng = np.random.default_rng(40 + m)
+    lens = np.concatenate([[1, 2, 3, 1, 400], rng.integers(1, 260, 296)])
+    lens[11:41:2] = lens[10:40:2]
+    pts, off, _ = D._walks(rng, lens, D.STEP_SIGMA)
+    for k in range(10, 40, 2):  # near-duplicates: copy k into k+1 with ~1e-4 deg noise
+        a, b, n_k = off[k], off[k + 1], lens[k]
+        pts[b:b + n_k] = pts[a:a + n_k] + rng.normal(0, 1e-4, (n_k, 2)).astype(np.float32)
+    s = TrajSet.from_packed(pts, off, lens)
+    n = s.n
+    for exact in (True, False):
+        full, fcnt = matrix(m, s, s, eps=EPS, gpoint=G, exact=exact)
+        out = torch.full((n, n), -7.0, device="cuda")
+        cnt = torch.full((n, n), -7, dtype=torch.int32, device="cuda") if m in (1, 2) else None
+        allpairs_sym_raw(m, s, out=out, counts=cnt, eps=EPS, gpoint=G, exact=exact)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out.cpu().numpy(), full.cpu().numpy())
+        if cnt is not None:
+            np.testing.assert_array_equal(cnt.cpu().numpy(), fcnt.cpu().numpy())
+
+
+def test_allpairs_sym_reference_signature_full_size(full_set):
+    """core.allpairs on host padded arrays at 2000 trajectories equals
+    core.matrix(S, S) (float64 results, EDR/LCSS normalised)."""
+    from trajsimimeasures_b200 import core, datagen as D
+    (p, o, l), _ = full_set
+    P = D.pad(D.unpack(p, o, l))
+    for name in ("dtw", "edr", "hausdorff"):
+        a = core.allpairs(name, P, l, eps=EPS, gpoint=G)
+        b = core.matrix(name, P, l, P, l, eps=EPS, gpoint=G)
+        assert a.dtype == np.float64 and a.shape == (2000, 2000)
+        np.testing.assert_array_equal(a, b, err_msg=name)

@@ -37,7 +37,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .engine import TrajSet, pack_lists, pair_order, pairs_raw, matrix_raw, measure_id
+from .engine import TrajSet, allpairs_sym_raw, pack_lists, pair_order, pairs_raw, matrix_raw, measure_id
 
 __all__ = ["dtw", "edr", "lcss", "erp", "dfrechet", "hausdorff", "matrix", "dtw_matrix", "edr_matrix",
            "lcss_matrix", "erp_matrix", "dfrechet_matrix", "hausdorff_matrix", "pairs"]
@@ -229,6 +229,11 @@ def matrix(measure, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False, rows
     out = torch.empty((qs.n, ds.n), dtype=torch.float32, device=qs.device)
     cnt = torch.empty((qs.n, ds.n), dtype=torch.int32, device=qs.device) if m in (_lib.EDR, _lib.LCSS) else None
     matrix_raw(m, qs, ds, out=out, counts=cnt, eps=eps, gpoint=_gpoint(gpoint), exact=exact, rows=rows)
+    return _finish_matrix(m, out, cnt, qs, ds, on_device, counts)
+
+
+def _finish_matrix(m, out, cnt, qs, ds, on_device, counts):
+    """float64 results of a float32 matrix (EDR/LCSS: from the counts)."""
     lq = qs.lens_host if qs.lens_host is not None else qs.lens.cpu().numpy()
     ld = ds.lens_host if ds.lens_host is not None else ds.lens.cpu().numpy()
     if on_device:
@@ -246,6 +251,22 @@ def matrix(measure, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False, rows
         return (res, c_h) if counts else res
     res = out.cpu().numpy().astype(np.float64)
     return (res, None) if counts else res
+
+
+def allpairs(measure, S, lenS=None, *, eps=0.0, gpoint=None, exact=False, rows=0, counts=False):
+    """result[i, j] = measure(S_i, S_j) for all pairs of one set, computing
+    each unordered pair once and mirroring it (the clustering driver's upper
+    triangle, test_clustering_time.py:219-269, as one launch).  Same inputs
+    and return types as ``matrix``; equal to ``matrix(measure, S, lenS, S,
+    lenS)`` bit for bit."""
+    m = measure_id(measure)
+    dev = torch.device("cuda")
+    on_device = isinstance(S, TrajSet) or (isinstance(S, torch.Tensor) and S.is_cuda)
+    ss = _set_of(S, lenS, dev)
+    out = torch.empty((ss.n, ss.n), dtype=torch.float32, device=ss.device)
+    cnt = torch.empty((ss.n, ss.n), dtype=torch.int32, device=ss.device) if m in (_lib.EDR, _lib.LCSS) else None
+    allpairs_sym_raw(m, ss, out=out, counts=cnt, eps=eps, gpoint=_gpoint(gpoint), exact=exact, rows=rows)
+    return _finish_matrix(m, out, cnt, ss, ss, on_device, counts)
 
 
 def matrix_many(measures, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False, rows=0, stream=None):

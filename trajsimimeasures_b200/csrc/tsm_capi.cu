@@ -231,6 +231,54 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
     return launch(wfn, grid, dim3(32 * W), smem, args, s);
 }
 
+namespace {
+
+// One matrix launch: Q x D (q_order == nullptr, sym == 0), or the symmetric
+// upper triangle of one set in its length order (q_order == d_order, sym == 1).
+int matrix_launch(const char* who, int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len,
+                  const int32_t* q_order, int64_t nq, int32_t q_max_len, const float* d_pts, const int64_t* d_off,
+                  const int32_t* d_len, const int32_t* d_order, int64_t nd, int32_t d_max_len, int sym,
+                  const tsm_params* params, float* out, int64_t ld_out, int32_t* out_counts, void* stream) {
+    const int R = rows_of(params, measure);
+    const bool exact = exact_of(params);
+    cudaStream_t s = (cudaStream_t)stream;
+    const tsm::KParams kp = make_kparams(params);
+    const float2* q2 = reinterpret_cast<const float2*>(q_pts);
+    const float2* d2 = reinterpret_cast<const float2*>(d_pts);
+    int qcap = q_max_len < 1 ? 1 : q_max_len;
+    int dml = d_max_len;
+    int64_t ndd = nd, ld = ld_out;
+    if (measure == TSM_HAUSDORFF) {
+        const void* fn = pick_haus(true, R, exact);
+        if (!fn) return fail(TSM_EINVAL, "%s: rows_per_thread must be 4, 8 or 16", who);
+        const int smem = qcap * 20;
+        if (smem > kSmemMax) return fail(TSM_ETOOLONG, "%s: query length %d too long", who, q_max_len);
+        const int threads = 128;
+        int chunks = (int)((nd + threads - 1) / threads);
+        if ((int64_t)chunks * nq > 0x7fffffffLL) return fail(TSM_EINVAL, "%s: grid too large", who);
+        dim3 grid((unsigned)(chunks * nq));
+        void* args[] = {&q2,  &q_off, &q_len, &q_order, &d2,  &d_off, &d_len, &d_order,
+                        &ndd, &chunks, &sym,  &qcap,    &dml, &out,   &ld};
+        return launch(fn, grid, dim3(threads), smem, args, s);
+    }
+    if (q_max_len > kMatrixQueryMax)
+        return fail(TSM_ETOOLONG, "%s: q_max_len %d > %d (use the pairs form)", who, q_max_len, kMatrixQueryMax);
+    const void* fn = exact ? pick_dp_m<true>(measure, true, R) : pick_dp_m<false>(measure, true, R);
+    if (!fn) return fail(TSM_EINVAL, "%s: rows_per_thread must be 4, 8 or 16", who);
+    const int W = warps_for(qcap, qcap * 16);
+    const int threads = 32 * W;
+    const int smem = qcap * 16 + W * 32 * qcap * 4;
+    if (smem > kSmemMax) return fail(TSM_ETOOLONG, "%s: boundary rows need %d bytes", who, smem);
+    int chunks = (int)((nd + threads - 1) / threads);
+    if ((int64_t)chunks * nq > 0x7fffffffLL) return fail(TSM_EINVAL, "%s: grid too large", who);
+    dim3 grid((unsigned)(chunks * nq));
+    void* args[] = {&q2,   &q_off, &q_len, &q_order,   &d2,  &d_off, &d_len, &d_order, &ndd,
+                    &chunks, &sym, &qcap,  &dml, (void*)&kp, &out, &ld,   &out_counts};
+    return launch(fn, grid, dim3(threads), smem, args, s);
+}
+
+}  // namespace
+
 int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len, int64_t nq,
                int32_t q_max_len, const float* d_pts, const int64_t* d_off, const int32_t* d_len,
                const int32_t* d_order, int64_t nd, int32_t d_max_len, const tsm_params* params,
@@ -243,41 +291,23 @@ int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int3
         return fail(TSM_EINVAL, "tsm_matrix: null pointer");
     if (ld_out < nd) return fail(TSM_EINVAL, "tsm_matrix: ld_out < nd");
     if (q_max_len < 0 || d_max_len < 0) return fail(TSM_EINVAL, "tsm_matrix: max_len < 0");
-    const int R = rows_of(params, measure);
-    const bool exact = exact_of(params);
-    cudaStream_t s = (cudaStream_t)stream;
-    const tsm::KParams kp = make_kparams(params);
-    const float2* q2 = reinterpret_cast<const float2*>(q_pts);
-    const float2* d2 = reinterpret_cast<const float2*>(d_pts);
-    int qcap = q_max_len < 1 ? 1 : q_max_len;
-    int dml = d_max_len;
-    int64_t ndd = nd, ld = ld_out;
-    if (measure == TSM_HAUSDORFF) {
-        const void* fn = pick_haus(true, R, exact);
-        if (!fn) return fail(TSM_EINVAL, "tsm_matrix: rows_per_thread must be 4, 8 or 16");
-        const int smem = qcap * 20;
-        if (smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_matrix: query length %d too long", q_max_len);
-        const int threads = 128;
-        int chunks = (int)((nd + threads - 1) / threads);
-        if ((int64_t)chunks * nq > 0x7fffffffLL) return fail(TSM_EINVAL, "tsm_matrix: grid too large");
-        dim3 grid((unsigned)(chunks * nq));
-        void* args[] = {&q2, &q_off, &q_len, &d2, &d_off, &d_len, &d_order, &ndd, &chunks, &qcap, &dml, &out, &ld};
-        return launch(fn, grid, dim3(threads), smem, args, s);
-    }
-    if (q_max_len > kMatrixQueryMax)
-        return fail(TSM_ETOOLONG, "tsm_matrix: q_max_len %d > %d (use the pairs form)", q_max_len, kMatrixQueryMax);
-    const void* fn = exact ? pick_dp_m<true>(measure, true, R) : pick_dp_m<false>(measure, true, R);
-    if (!fn) return fail(TSM_EINVAL, "tsm_matrix: rows_per_thread must be 4, 8 or 16");
-    const int W = warps_for(qcap, qcap * 16);
-    const int threads = 32 * W;
-    const int smem = qcap * 16 + W * 32 * qcap * 4;
-    if (smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_matrix: boundary rows need %d bytes", smem);
-    int chunks = (int)((nd + threads - 1) / threads);
-    if ((int64_t)chunks * nq > 0x7fffffffLL) return fail(TSM_EINVAL, "tsm_matrix: grid too large");
-    dim3 grid((unsigned)(chunks * nq));
-    void* args[] = {&q2, &q_off, &q_len, &d2, &d_off, &d_len, &d_order, &ndd, &chunks, &qcap, &dml, (void*)&kp,
-                    &out, &ld, &out_counts};
-    return launch(fn, grid, dim3(threads), smem, args, s);
+    return matrix_launch("tsm_matrix", measure, q_pts, q_off, q_len, nullptr, nq, q_max_len, d_pts, d_off, d_len,
+                         d_order, nd, d_max_len, 0, params, out, ld_out, out_counts, stream);
+}
+
+int tsm_allpairs_sym(int measure, const float* pts, const int64_t* off, const int32_t* len, const int32_t* order,
+                     int64_t n, int32_t max_len, const tsm_params* params, float* out, int64_t ld_out,
+                     int32_t* out_counts, void* stream) {
+    g_err.clear();
+    if (measure < TSM_DTW || measure > TSM_HAUSDORFF)
+        return fail(TSM_EINVAL, "tsm_allpairs_sym: unknown measure %d", measure);
+    if (n < 0) return fail(TSM_EINVAL, "tsm_allpairs_sym: negative set size");
+    if (n == 0) return TSM_OK;
+    if (!pts || !off || !len || !order || !out) return fail(TSM_EINVAL, "tsm_allpairs_sym: null pointer");
+    if (ld_out < n) return fail(TSM_EINVAL, "tsm_allpairs_sym: ld_out < n");
+    if (max_len < 0) return fail(TSM_EINVAL, "tsm_allpairs_sym: max_len < 0");
+    return matrix_launch("tsm_allpairs_sym", measure, pts, off, len, order, n, max_len, pts, off, len, order, n,
+                         max_len, 1, params, out, ld_out, out_counts, stream);
 }
 
 int tsm_topk_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, int32_t k, float* out_d,

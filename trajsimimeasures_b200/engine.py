@@ -170,6 +170,19 @@ def matrix_raw(measure, q: TrajSet, d: TrajSet, *, out, counts=None, d_order=Non
     return out
 
 
+def allpairs_sym_raw(measure, s: TrajSet, *, out, counts=None, eps=0.0, gpoint=(0.0, 0.0), exact=False, rows=0,
+                     stream=None):
+    """tsm_allpairs_sym on a device-resident set: the full symmetric n x n
+    matrix from the upper triangle (no copies, no sync)."""
+    m = measure_id(measure)
+    lib = _lib.load()
+    p = _lib.params(eps, gpoint, exact, rows)
+    rc = lib.tsm_allpairs_sym(m, _ptr(s.pts), _ptr(s.off), _ptr(s.lens), _ptr(s.order_by_length()), s.n, s.max_len,
+                              ctypes.byref(p), _ptr(out), int(out.stride(0)), _ptr(counts), _stream_ptr(stream))
+    _lib.check(rc, "tsm_allpairs_sym")
+    return out
+
+
 def matrix(measure, q: TrajSet, d: TrajSet, *, eps=0.0, gpoint=(0.0, 0.0), exact=False, rows=0,
            stream=None, with_counts=None):
     """All pairs Q x D on the device -> (out float32 [nq, nd], counts int32 or None)."""
