@@ -50,7 +50,7 @@ WORKLOAD = "allpairs_2000x2000_six_measures"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -119,10 +119,27 @@ class ClockSampler:
         try:
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                       "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.p = None
+            return
+        t0 = time.time()  # nvidia-smi takes a moment to start: wait for its first sample
+        while time.time() - t0 < 10 and self._lines() < 1 and self.p.poll() is None:
+            time.sleep(0.05)
+        self.skip = 0
+
+    def _lines(self):
+        self.f.flush()
+        try:
+            return sum(1 for ln in open(self.path) if ln.count(",") >= 8)
+        except OSError:
+            return 0
+
+    def mark(self):
+        """Samples before this call (the warm-up, idle) are not reported."""
+        if self.p is not None:
+            self.skip = self._lines()
 
     def stop(self):
         if self.p is None:
@@ -135,7 +152,8 @@ class ClockSampler:
         self.f.close()
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        lines = [ln for ln in open(self.path) if ln.count(",") >= 8][getattr(self, "skip", 0):]
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -325,7 +343,7 @@ def run_ours(args, ws, rank, local):
     clk = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
     if clk:
         clk.start()
-        time.sleep(0.3)
+        clk.mark()
     per_ms = {m: 0.0 for m in MEAS}
     step_ms = []
     launches = 0

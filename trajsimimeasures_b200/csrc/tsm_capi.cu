@@ -251,7 +251,7 @@ int matrix_launch(const char* who, int measure, const float* q_pts, const int64_
     if (measure == TSM_HAUSDORFF) {
         const void* fn = pick_haus(true, R, exact);
         if (!fn) return fail(TSM_EINVAL, "%s: rows_per_thread must be 4, 8 or 16", who);
-        const int smem = qcap * 20;
+        const int smem = ((qcap + 1) / 2) * 40;  // staged segment pairs
         if (smem > kSmemMax) return fail(TSM_ETOOLONG, "%s: query length %d too long", who, q_max_len);
         const int threads = 128;
         int chunks = (int)((nd + threads - 1) / threads);

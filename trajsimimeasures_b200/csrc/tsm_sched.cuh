@@ -219,8 +219,8 @@ __device__ __forceinline__ void hausdorff_task(const PairsArgs& A, int first, in
         } else {
             const float2* a = A.pts + A.off_a[k];
             const float2* b = A.pts + A.off_b[k];
-            o = __fsqrt_rn(fmaxf(directed_max<R, EXACT>(a, na, GlobalCols{b}, nb),
-                                 directed_max<R, EXACT>(b, nb, GlobalCols{a}, na)));
+            o = __fsqrt_rn(fmaxf(directed_max2<R, EXACT>(GlobalCols{a}, na, b, nb),
+                                 directed_max2<R, EXACT>(GlobalCols{b}, nb, a, na)));
         }
         A.out[HAUSDORFF * A.out_stride + k] = o;
     }
@@ -241,8 +241,8 @@ __device__ __forceinline__ void hausdorff_warp_task(const PairsArgs& A, int firs
     }
     const float2* a = A.pts + A.off_a[k];
     const float2* b = A.pts + A.off_b[k];
-    float m = fmaxf(directed_max<R, EXACT>(a, na, GlobalCols{b}, nb, lane * R, 32 * R),
-                    directed_max<R, EXACT>(b, nb, GlobalCols{a}, na, lane * R, 32 * R));
+    float m = fmaxf(directed_max2<R, EXACT>(GlobalCols{a}, na, b, nb, lane * R, 32 * R),
+                    directed_max2<R, EXACT>(GlobalCols{b}, nb, a, na, lane * R, 32 * R));
     // non-negative floats order like their bit patterns
     m = __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(m)));
     if (lane == 0) A.out[HAUSDORFF * A.out_stride + k] = __fsqrt_rn(m);

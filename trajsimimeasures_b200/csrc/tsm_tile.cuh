@@ -453,7 +453,8 @@ __global__ void __launch_bounds__(128) dp_matrix_kernel(
 // u < 1e-5 -> the reference takes min(|p-s1|^2, |p-s2|^2) = |p-s1|^2 (t = 0);
 // u > 1 -> |p-s2|^2 (t = 1).  A zero-length segment has inv = 0, so t = 0 and
 // the result is |p - s1|^2 as in hausdorff.py:30-31.  mul.sat clamps u to
-// [0, 1] (NaN to 0) in the multiply itself.
+// [0, 1] (NaN to 0) in the multiply itself.  This scalar form is the
+// definition (and the oracle twin's formula); the kernels use p2s_pair.
 __device__ __forceinline__ float p2s(float px, float py, float s1x, float s1y, float sx, float sy,
                                      float inv) {
     const float ax = __fsub_rn(px, s1x), ay = __fsub_rn(py, s1y);
@@ -465,41 +466,84 @@ __device__ __forceinline__ float p2s(float px, float py, float s1x, float s1y, f
     return __fmaf_rn(ey, ey, __fmul_rn(ex, ex));
 }
 
-// max over the points of P of (min over the segments of T): hausdorff.py:48-69
-// per point, then the max of the host reduction at :121 over valid points.
-// The loop also visits T's last vertex as a zero-length segment (k = nt-1).
-// In exact arithmetic that distance is never below the last segment's, so
-// the min is the reference's; in FP32 it makes a point that coincides with
-// the last vertex come out exactly 0 (u = dot * (1/len2) can round to 1-ulp,
-// leaving a ~1e-11 residue), as every other vertex already does as the
-// first endpoint of its outgoing segment.
-// Points pb0, pb0 + pstride, ... (blocks of R) of P: a thread takes all
-// points (pb0 = 0, pstride = R) or, in a warp-per-pair task, every 32nd block.
-template <int R, bool EXACT, class Segs>
-__device__ __forceinline__ float directed_max(const float2* __restrict__ P, int np, const Segs& T, int nt,
-                                             int pb0 = 0, int pstride = R) {
-    if (nt < 2 || np <= 0) return 0.f;  // p2t_dist over zero segments is 0.0
+// The kernels evaluate p2s two segments at a time in FP32x2: for a point p
+// and consecutive segments k, k+1 of one trajectory, the vector quantities
+// (a, dot, foot offset, squared distance) are f32x2 pairs, while the clamp
+// u -> t and the running min stay scalar (f32x2 has no saturation and no
+// min).  Segments are kept negated (-s1, -s, -1/|s|^2), so a - b becomes an
+// f32x2 add and the foot a - t s an f32x2 fma: every value is bit-identical
+// to p2s above, and min(best, d_k, d_k+1) is one three-input min.  Per two
+// evaluations: 8 f32x2 + 2 scalar FMA-pipe and 5 ALU instructions, against
+// 18 + 6 for two scalar p2s calls.
+struct SegPair {
+    float2 n1x, n1y;  // -s1 of segments k, k+1
+    float2 nsx, nsy;  // -(s2 - s1)
+    float2 ninv;      // -1/|s|^2 (0 for a zero-length segment)
+};
+
+// p2s of one point (pair-broadcast px2 = (px, px), py2) against segments
+// k and k+1, folded into best.
+__device__ __forceinline__ float p2s_pair(float2 px2, float2 py2, const SegPair& g, float best) {
+    const float2 ax = __fadd2_rn(px2, g.n1x), ay = __fadd2_rn(py2, g.n1y);
+    const float2 ndot = __ffma2_rn(ay, g.nsy, __fmul2_rn(ax, g.nsx));  // -(a.s)
+    float u0, u1;
+    asm("mul.rn.sat.f32 %0, %1, %2;" : "=f"(u0) : "f"(ndot.x), "f"(g.ninv.x));
+    asm("mul.rn.sat.f32 %0, %1, %2;" : "=f"(u1) : "f"(ndot.y), "f"(g.ninv.y));
+    const float2 t = make_float2((u0 < 1e-5f) ? 0.f : u0, (u1 < 1e-5f) ? 0.f : u1);
+    const float2 ex = __ffma2_rn(t, g.nsx, ax), ey = __ffma2_rn(t, g.nsy, ay);
+    const float2 d2 = __ffma2_rn(ey, ey, __fmul2_rn(ex, ex));
+    return min3f(best, d2.x, d2.y);
+}
+
+// Segment k of trajectory T (k = n-1: the last vertex as a zero-length
+// segment), negated, into lane `hi` of a SegPair.
+template <bool EXACT>
+__device__ __forceinline__ void seg_lane(SegPair& g, int hi, float2 s1, float2 s2) {
+    const float sx = __fsub_rn(s2.x, s1.x), sy = __fsub_rn(s2.y, s1.y);
+    const float len2 = __fmaf_rn(sy, sy, __fmul_rn(sx, sx));
+    const float inv = (sx == 0.f && sy == 0.f) ? 0.f : trcp<EXACT>(len2);
+    if (hi) {
+        g.n1x.y = -s1.x; g.n1y.y = -s1.y; g.nsx.y = -sx; g.nsy.y = -sy; g.ninv.y = -inv;
+    } else {
+        g.n1x.x = -s1.x; g.n1y.x = -s1.y; g.nsx.x = -sx; g.nsy.x = -sy; g.ninv.x = -inv;
+    }
+}
+
+// Staged query segments for the packed matrix kernel: pair j holds segments
+// 2j and 2j+1 of the query (the last vertex counted as segment nq-1; an odd
+// count repeats it), as float4 (n1x, n1y) + float4 (nsx, nsy) + float2 ninv.
+__device__ __forceinline__ SegPair staged_pair(const float4* A, const float4* B, const float2* C, int j) {
+    const float4 a = A[j], b = B[j];
+    SegPair g;
+    g.n1x = make_float2(a.x, a.y);
+    g.n1y = make_float2(a.z, a.w);
+    g.nsx = make_float2(b.x, b.y);
+    g.nsy = make_float2(b.z, b.w);
+    g.ninv = C[j];
+    return g;
+}
+
+// directed_max with P from global memory and T staged as segment pairs.
+template <int R>
+__device__ __forceinline__ float directed_max_staged2(const float2* __restrict__ P, int np, const float4* A,
+                                                      const float4* B, const float2* C, int nq) {
+    if (nq < 2 || np <= 0) return 0.f;
+    const int npair = (nq + 1) >> 1;
     float m = 0.f;
-    for (int pb = pb0; pb < np; pb += pstride) {
-        float px[R], py[R], best[R];
+    for (int pb = 0; pb < np; pb += R) {
+        float2 px[R], py[R];
+        float best[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const float2 q = __ldg(P + min(pb + r, np - 1));
-            px[r] = q.x;
-            py[r] = q.y;
+            px[r] = make_float2(q.x, q.x);
+            py[r] = make_float2(q.y, q.y);
             best[r] = CUDART_INF_F;
         }
-        float2 s1 = T.pt(0);
-        float2 s2n = T.pt(1);
-        for (int k = 0; k < nt; ++k) {  // nt-1 segments + the last vertex
-            const float2 s2 = s2n;
-            s2n = T.pt(min(k + 2, nt - 1));
-            const float sx = __fsub_rn(s2.x, s1.x), sy = __fsub_rn(s2.y, s1.y);
-            const float len2 = __fmaf_rn(sy, sy, __fmul_rn(sx, sx));
-            const float inv = (sx == 0.f && sy == 0.f) ? 0.f : trcp<EXACT>(len2);
+        for (int j = 0; j < npair; ++j) {
+            const SegPair g = staged_pair(A, B, C, j);
 #pragma unroll
-            for (int r = 0; r < R; ++r) best[r] = fminf(best[r], p2s(px[r], py[r], s1.x, s1.y, sx, sy, inv));
-            s1 = s2;
+            for (int r = 0; r < R; ++r) best[r] = p2s_pair(px[r], py[r], g, best[r]);
         }
 #pragma unroll
         for (int r = 0; r < R; ++r)
@@ -508,6 +552,114 @@ __device__ __forceinline__ float directed_max(const float2* __restrict__ P, int 
     return m;
 }
 
+// max over the points of P of (min over the segments of T), hausdorff.py:48-69
+// per point, then the max of the host reduction at :121 over valid points.
+// T's segment pairs are built on the fly from global memory.  The loop also
+// visits T's last vertex as a zero-length segment: in exact arithmetic that
+// distance is never below the last segment's, so the min is the reference's;
+// in FP32 it makes a point that coincides with the last vertex come out
+// exactly 0 (u = dot * (1/len2) can round to 1-ulp, leaving a ~1e-11
+// residue), as every other vertex already does as the first endpoint of its
+// outgoing segment.  Points pb0, pb0 + pstride, ... (blocks of R) of P: a
+// thread takes all points (pb0 = 0, pstride = R) or, in a warp-per-pair
+// task, every 32nd block.
+template <int R, bool EXACT, class Pts>
+__device__ __forceinline__ float directed_max2(const Pts& P, int np, const float2* __restrict__ T, int nt,
+                                               int pb0 = 0, int pstride = R) {
+    if (nt < 2 || np <= 0) return 0.f;  // p2t_dist over zero segments is 0.0
+    float m = 0.f;
+    for (int pb = pb0; pb < np; pb += pstride) {
+        float2 px[R], py[R];
+        float best[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float2 q = P.pt(min(pb + r, np - 1));
+            px[r] = make_float2(q.x, q.x);
+            py[r] = make_float2(q.y, q.y);
+            best[r] = CUDART_INF_F;
+        }
+        float2 v0 = __ldg(T);
+        float2 v1 = __ldg(T + 1);
+        for (int k = 0; k < nt; k += 2) {  // segments k, k+1 (segment nt-1 is the last vertex)
+            const float2 v2 = __ldg(T + min(k + 2, nt - 1));
+            SegPair g;
+            seg_lane<EXACT>(g, 0, v0, v1);
+            if (k + 1 < nt) seg_lane<EXACT>(g, 1, v1, v2);
+            else seg_lane<EXACT>(g, 1, v0, v0);  // odd count: repeat the last vertex
+#pragma unroll
+            for (int r = 0; r < R; ++r) best[r] = p2s_pair(px[r], py[r], g, best[r]);
+            v0 = v2;
+            v1 = __ldg(T + min(k + 3, nt - 1));
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (pb + r < np) m = fmaxf(m, best[r]);
+    }
+    return m;
+}
+
+// The staged query's points, read back from the negated segment starts.
+struct StagedNegPts {
+    const float4* A;
+    __device__ __forceinline__ float2 pt(int k) const {
+        const float4 a = A[k >> 1];
+        return make_float2(-((k & 1) ? a.y : a.x), -((k & 1) ? a.w : a.z));
+    }
+};
+
+// Matrix kernel: CTA (s, chunk) stages query i's segment pairs in shared
+// memory once; each thread takes one database trajectory.  Query order and
+// symmetric mode as in dp_matrix_kernel.  Dynamic shared memory =
+// ceil(q_max_len/2) * 40 bytes.
+template <int R, bool EXACT>
+__global__ void __launch_bounds__(128) hausdorff_matrix_kernel(
+    const float2* __restrict__ q_pts, const int64_t* __restrict__ q_off, const int32_t* __restrict__ q_len,
+    const int32_t* __restrict__ q_order, const float2* __restrict__ d_pts, const int64_t* __restrict__ d_off,
+    const int32_t* __restrict__ d_len, const int32_t* __restrict__ d_order, int64_t nd, int chunks, int sym,
+    int q_max_len, int d_max_len, float* __restrict__ out, int64_t ld) {
+    extern __shared__ float4 smem4[];
+    const int cap_pairs = (q_max_len + 1) >> 1;
+    float4* A = smem4;
+    float4* B = smem4 + cap_pairs;
+    float2* C = reinterpret_cast<float2*>(smem4 + 2 * cap_pairs);
+    const int64_t qs = blockIdx.x / chunks;
+    const int chunk = blockIdx.x % chunks;
+    if (sym && (int64_t)(chunk + 1) * blockDim.x <= qs) return;
+    const int64_t qi = q_order ? (int64_t)q_order[qs] : qs;
+    const int nq = q_len[qi];
+    const bool qbad = nq < 0 || nq > q_max_len;
+    if (!qbad && nq > 0) {
+        const float2* qp = q_pts + q_off[qi];
+        const int npair = (nq + 1) >> 1;
+        for (int j = threadIdx.x; j < npair; j += blockDim.x) {
+            SegPair g;
+            const int k0 = 2 * j, k1 = min(2 * j + 1, nq - 1);
+            seg_lane<EXACT>(g, 0, __ldg(qp + k0), __ldg(qp + min(k0 + 1, nq - 1)));
+            seg_lane<EXACT>(g, 1, __ldg(qp + k1), __ldg(qp + min(k1 + 1, nq - 1)));
+            A[j] = make_float4(g.n1x.x, g.n1x.y, g.n1y.x, g.n1y.y);
+            B[j] = make_float4(g.nsx.x, g.nsx.y, g.nsy.x, g.nsy.y);
+            C[j] = g.ninv;
+        }
+    }
+    __syncthreads();
+    const int64_t slot = (int64_t)chunk * blockDim.x + threadIdx.x;
+    if (slot >= nd || (sym && slot < qs)) return;
+    const int64_t dj = d_order ? (int64_t)d_order[slot] : slot;
+    const int ndl = d_len[dj];
+    const int64_t o_idx = qi * ld + dj;
+    const bool mirror = sym && dj != qi;
+    float v = CUDART_NAN_F;
+    if (!(qbad || ndl < 0 || ndl > d_max_len)) {
+        const float2* dp = d_pts + d_off[dj];
+        const float m1 = directed_max_staged2<R>(dp, ndl, A, B, C, nq);
+        const float m2 = directed_max2<R, EXACT>(StagedNegPts{A}, nq, dp, ndl);
+        v = __fsqrt_rn(fmaxf(m1, m2));
+    }
+    out[o_idx] = v;
+    if (mirror) out[dj * ld + qi] = v;
+}
+
+// Pairs kernel: one thread per pair, both trajectories from global memory.
 template <int R, bool EXACT>
 __global__ void __launch_bounds__(128) hausdorff_pairs_kernel(
     const float2* __restrict__ pts, const int64_t* __restrict__ off_a, const int32_t* __restrict__ len_a,
@@ -523,128 +675,9 @@ __global__ void __launch_bounds__(128) hausdorff_pairs_kernel(
     }
     const float2* a = pts + off_a[k];
     const float2* b = pts + off_b[k];
-    const float m1 = directed_max<R, EXACT>(a, na, GlobalCols{b}, nb);
-    const float m2 = directed_max<R, EXACT>(b, nb, GlobalCols{a}, na);
+    const float m1 = directed_max2<R, EXACT>(GlobalCols{a}, na, b, nb);
+    const float m2 = directed_max2<R, EXACT>(GlobalCols{b}, nb, a, na);
     out[k] = __fsqrt_rn(fmaxf(m1, m2));
-}
-
-// Query segments staged in shared memory for the matrix kernel:
-// seg[k] = (s1.x, s1.y, s.x, s.y) with s = q[k+1] - q[k] (s = 0 for the last
-// vertex, k = nq-1), sinv[k] = 1/|s|^2 (0 for a zero-length segment).
-template <int R, bool EXACT>
-__device__ __forceinline__ float directed_max_staged(const float2* __restrict__ P, int np, const float4* seg,
-                                                     const float* sinv, int nq) {
-    if (nq < 2 || np <= 0) return 0.f;
-    float m = 0.f;
-    for (int pb = 0; pb < np; pb += R) {
-        float px[R], py[R], best[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const float2 q = __ldg(P + min(pb + r, np - 1));
-            px[r] = q.x;
-            py[r] = q.y;
-            best[r] = CUDART_INF_F;
-        }
-        for (int k = 0; k < nq; ++k) {  // nq-1 segments + the last vertex
-            const float4 sg = seg[k];
-            const float inv = sinv[k];
-#pragma unroll
-            for (int r = 0; r < R; ++r) best[r] = fminf(best[r], p2s(px[r], py[r], sg.x, sg.y, sg.z, sg.w, inv));
-        }
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-            if (pb + r < np) m = fmaxf(m, best[r]);
-    }
-    return m;
-}
-
-// Query points read back from the staged segments (seg[k].xy = q[k]).
-struct StagedPts {
-    const float4* s;
-    __device__ __forceinline__ float2 pt(int j) const {
-        const float4 v = s[j];
-        return make_float2(v.x, v.y);
-    }
-};
-
-// max over the points of the query (from shared memory) of the min over the
-// segments of a per-thread trajectory T (global memory, computed on the fly).
-template <int R, bool EXACT>
-__device__ __forceinline__ float directed_max_qpts(const StagedPts& P, int np, const float2* __restrict__ T, int nt) {
-    if (nt < 2 || np <= 0) return 0.f;
-    float m = 0.f;
-    for (int pb = 0; pb < np; pb += R) {
-        float px[R], py[R], best[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const float2 q = P.pt(min(pb + r, np - 1));
-            px[r] = q.x;
-            py[r] = q.y;
-            best[r] = CUDART_INF_F;
-        }
-        float2 s1 = __ldg(T);
-        float2 s2n = __ldg(T + 1);
-        for (int k = 0; k < nt; ++k) {
-            const float2 s2 = s2n;
-            s2n = __ldg(T + min(k + 2, nt - 1));
-            const float sx = __fsub_rn(s2.x, s1.x), sy = __fsub_rn(s2.y, s1.y);
-            const float len2 = __fmaf_rn(sy, sy, __fmul_rn(sx, sx));
-            const float inv = (sx == 0.f && sy == 0.f) ? 0.f : trcp<EXACT>(len2);
-#pragma unroll
-            for (int r = 0; r < R; ++r) best[r] = fminf(best[r], p2s(px[r], py[r], s1.x, s1.y, sx, sy, inv));
-            s1 = s2;
-        }
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-            if (pb + r < np) m = fmaxf(m, best[r]);
-    }
-    return m;
-}
-
-// Dynamic shared memory = q_max_len * (16 + 4) bytes.  Query order and
-// symmetric mode as in dp_matrix_kernel.
-template <int R, bool EXACT>
-__global__ void __launch_bounds__(128) hausdorff_matrix_kernel(
-    const float2* __restrict__ q_pts, const int64_t* __restrict__ q_off, const int32_t* __restrict__ q_len,
-    const int32_t* __restrict__ q_order, const float2* __restrict__ d_pts, const int64_t* __restrict__ d_off,
-    const int32_t* __restrict__ d_len, const int32_t* __restrict__ d_order, int64_t nd, int chunks, int sym,
-    int q_max_len, int d_max_len, float* __restrict__ out, int64_t ld) {
-    extern __shared__ float smem[];
-    float4* seg = reinterpret_cast<float4*>(smem);
-    float* sinv = smem + 4 * q_max_len;
-    const int64_t qs = blockIdx.x / chunks;
-    const int chunk = blockIdx.x % chunks;
-    if (sym && (int64_t)(chunk + 1) * blockDim.x <= qs) return;
-    const int64_t qi = q_order ? (int64_t)q_order[qs] : qs;
-    const int nq = q_len[qi];
-    const bool qbad = nq < 0 || nq > q_max_len;
-    if (!qbad) {
-        const float2* qp = q_pts + q_off[qi];
-        for (int k = threadIdx.x; k < nq; k += blockDim.x) {
-            const float2 s1 = __ldg(qp + k);
-            const float2 s2 = __ldg(qp + min(k + 1, nq - 1));
-            const float sx = __fsub_rn(s2.x, s1.x), sy = __fsub_rn(s2.y, s1.y);
-            const float len2 = __fmaf_rn(sy, sy, __fmul_rn(sx, sx));
-            seg[k] = make_float4(s1.x, s1.y, sx, sy);
-            sinv[k] = (sx == 0.f && sy == 0.f) ? 0.f : trcp<EXACT>(len2);
-        }
-    }
-    __syncthreads();
-    const int64_t slot = (int64_t)chunk * blockDim.x + threadIdx.x;
-    if (slot >= nd || (sym && slot < qs)) return;
-    const int64_t dj = d_order ? (int64_t)d_order[slot] : slot;
-    const int ndl = d_len[dj];
-    const int64_t o_idx = qi * ld + dj;
-    const bool mirror = sym && dj != qi;
-    float v = CUDART_NAN_F;
-    if (!(qbad || ndl < 0 || ndl > d_max_len)) {
-        const float2* dp = d_pts + d_off[dj];
-        const float m1 = directed_max_staged<R, EXACT>(dp, ndl, seg, sinv, nq);
-        const float m2 = directed_max_qpts<R, EXACT>(StagedPts{seg}, nq, dp, ndl);
-        v = __fsqrt_rn(fmaxf(m1, m2));
-    }
-    out[o_idx] = v;
-    if (mirror) out[dj * ld + qi] = v;
 }
 
 }  // namespace tsm
