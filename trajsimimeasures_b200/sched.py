@@ -13,8 +13,9 @@ launch (tsm_pairs_sched) whose warps pull tasks from a device queue:
     group8 (one pair per 8 lanes)   nc <= warp_floats/4
     wave   (one pair per warp)      nc <= warp_floats
   Hausdorff items are always one pair per lane.
-* inside a bucket items are sorted by their cost so a warp's lanes/groups get
-  near-equal trip counts, then cut into warp tasks;
+* inside a bucket items are sorted so a warp's lanes/groups get near-equal
+  trip counts, then cut into warp tasks: one-pair-per-lane buckets by loop
+  shape (row passes, then columns), the group buckets by step count;
 * all tasks are sorted by estimated cost, largest first (longest-processing-
   time-first), so the long pairs start at once and short tasks fill the tail.
 
@@ -79,19 +80,23 @@ def plan_pairs(len_a, len_b, measures, rows=8, warp_floats=4096) -> Plan:
     orders, tasks, costs = [], [], []
     pos = 0
 
-    def emit(kind, m, idx, per_task, cost_of):
+    def emit(kind, m, idx, per_task, cost_of, shape_of=None):
+        """Orders a bucket's items and cuts them into tasks of per_task items.
+        shape_of (int64, larger = heavier), when given, is the sort key: lanes
+        that run their own loops (one pair per lane) waste the steps by which
+        their trip counts differ, so such tasks group items of equal loop
+        shape, not merely of equal cost.  Otherwise the items go by cost."""
         nonlocal pos
         if idx.size == 0:
             return
-        c = cost_of[idx]
-        o = idx[np.argsort(-c, kind="stable")]
-        cs = cost_of[o]
+        key = cost_of[idx] if shape_of is None else shape_of[idx]
+        o = idx[np.argsort(-key, kind="stable")]
         starts = np.arange(0, o.size, per_task)
         cnt = np.minimum(per_task, o.size - starts)
         t = np.stack([np.full(starts.size, kind), np.full(starts.size, m), pos + starts, cnt], axis=1)
         orders.append(o.astype(np.int32))
         tasks.append(t.astype(np.int32))
-        costs.append(cs[starts].astype(np.float64))  # the first item of a task is its largest
+        costs.append(np.maximum.reduceat(cost_of[o], starts).astype(np.float64))  # a task lasts as long as its largest item
         pos += o.size
 
     all_idx = np.arange(n, dtype=np.int64)
@@ -99,14 +104,17 @@ def plan_pairs(len_a, len_b, measures, rows=8, warp_floats=4096) -> Plan:
         if m == _lib.HAUSDORFF:
             units = (la * lb + lb * la).astype(np.float64)  # segments + the last vertex, both directions
             big = units > HAUSDORFF_WARP_UNITS
-            emit(KIND_HAUSDORFF, m, all_idx[~big], 32, units * 1.8)
+            hshape = ((nr + rows - 1) // rows) * 65536 + nc  # point blocks of the longer side, then the shorter side
+            emit(KIND_HAUSDORFF, m, all_idx[~big], 32, units * 1.8, hshape)
             emit(KIND_HAUSDORFF_WARP, m, all_idx[big], 1, units * 1.8 / 32 + 64 * (la + lb))
             continue
         tile = nc <= tile_cap
         g8 = ~tile & (nc <= g8_cap)
         wave = ~tile & ~g8
         passes = (nr + 2 * rows - 1) // (2 * rows)
-        emit(KIND_TILE, m, all_idx[tile], 32, (passes * 2 * rows * (nc + 1)).astype(np.float64))
+        # a tile lane runs passes x (nc + 1) steps: group by passes, then by nc
+        emit(KIND_TILE, m, all_idx[tile], 32, (passes * 2 * rows * (nc + 1)).astype(np.float64),
+             passes * 65536 + nc)
         emit(KIND_GROUP8, m, all_idx[g8], 4, (_steps(nr, nc, rows, 8) * rows * 1.3).astype(np.float64))
         emit(KIND_WAVE, m, all_idx[wave], 1, (_steps(nr, nc, rows, 32) * rows * 1.3).astype(np.float64))
     if not tasks:
