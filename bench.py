@@ -503,13 +503,14 @@ def run_uneven(args):
     e1.record()
     torch.cuda.synchronize()
     ms_plain = e0.elapsed_time(e1) / args.steps
-    kinds = np.bincount(sc.plan.tasks[:, 0], minlength=5).tolist()
+    kinds = np.bincount(sc.plan.tasks[:, 0], minlength=7).tolist()
     print(json.dumps({
         "workload": f"uneven_{args.n_pairs}_pairs_lognormal_dtw+dfrechet+edr", "metric": "DP cells/s",
         "value": cells / (ms_sched / 1e3), "unit": "cells/s", "pairs_per_s": 3 * len(ia) / (ms_sched / 1e3),
         "ms_per_launch": ms_sched, "graph_replay": True,
         "autotuned": {"rows": best[0], "warp_floats": best[1], "candidates_ms": tried},
-        "tasks_by_kind": {"tile": kinds[0], "group8": kinds[1], "wave": kinds[2]},
+        "tasks_by_kind": {"tile": kinds[0], "group4": kinds[5], "group8": kinds[1], "group16": kinds[6],
+                          "wave": kinds[2]},
         "plain_tsm_pairs_ms": ms_plain, "speedup_vs_plain": ms_plain / ms_sched,
         "host_s": {"generate": gen_s, "autotune": tune_s, "plan": plan_s}, "steps": args.steps,
         "cells_per_launch": cells}), flush=True)

@@ -160,12 +160,21 @@ def test_sched_plan_covers_every_item_once():
         for kind, m, first, cnt in t:
             idx = pl.order[first:first + cnt]
             seen[m][idx] += 1
-            cap = {0: wf // 32, 1: wf // 4, 2: wf, 3: 1 << 30, 4: 1 << 30}[kind]
-            assert cnt <= {0: 32, 1: 4, 2: 1, 3: 32, 4: 1}[kind]
+            cap = {0: wf // 32, 5: wf // 8, 1: wf // 4, 6: wf // 2, 2: wf, 3: 1 << 30, 4: 1 << 30}[kind]
+            assert cnt <= {0: 32, 5: 8, 1: 4, 6: 2, 2: 1, 3: 32, 4: 1}[kind]
             assert nc[idx].max() <= cap
             assert (kind in (3, 4)) == (m == 5)
         for m, v in seen.items():
             assert np.all(v == 1), m
+        # a pair keeps its lanes for at most max_steps steps unless even a whole warp cannot do that
+        nr = np.maximum(la, lb)
+        for kind, m, first, cnt in t:
+            idx = pl.order[first:first + cnt]
+            if kind == 0:
+                assert np.all(2 * sched.tile_steps(nr[idx], nc[idx], rows) <= sched.MAX_STEPS)
+            elif kind in (5, 1, 6):
+                G = {5: 4, 1: 8, 6: 16}[kind]
+                assert np.all(sched.group_steps(nr[idx], nc[idx], rows, G) <= sched.MAX_STEPS)
 
 
 def test_sched_plan_rejects_pairs_beyond_capacity():

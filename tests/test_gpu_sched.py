@@ -34,15 +34,17 @@ def _batch(n, seed):
     return (pts, off, lens, ia, ib), t
 
 
-@pytest.mark.parametrize("rows,wf", [(8, 4096), (4, 2048), (8, 8192)])
-def test_sched_mixed_measures_bit_identical(oracle_mod, rows, wf):
+@pytest.mark.parametrize("rows,wf,max_steps", [(8, 4096, 8192), (4, 2048, 8192), (8, 8192, 8192), (8, 2048, 1024),
+                                               (8, 4096, 1 << 20)])
+def test_sched_mixed_measures_bit_identical(oracle_mod, rows, wf, max_steps):
     O = oracle_mod
-    from trajsimimeasures_b200.sched import PairsScheduler, KIND_GROUP8, KIND_WAVE
+    from trajsimimeasures_b200 import sched
     (pts, off, lens, ia, ib), t = _batch(20_000, seed=21)
-    s = PairsScheduler(*t, ALL, eps=EPS, gpoint=G, exact=True, rows=rows, warp_floats=wf,
-                       len_a_host=lens[ia], len_b_host=lens[ib])
+    s = sched.PairsScheduler(*t, ALL, eps=EPS, gpoint=G, exact=True, rows=rows, warp_floats=wf,
+                             max_steps=max_steps, len_a_host=lens[ia], len_b_host=lens[ib])
     kinds = set(s.plan.tasks[:, 0].tolist())
-    assert KIND_GROUP8 in kinds and (KIND_WAVE in kinds or wf >= 8192)
+    assert {sched.KIND_TILE, sched.KIND_HAUSDORFF, sched.KIND_HAUSDORFF_WARP} <= kinds
+    assert len(kinds & set(sched.GROUP_KIND.values())) >= 2
     s.run()
     torch.cuda.synchronize()
     out = s.out.cpu().numpy()

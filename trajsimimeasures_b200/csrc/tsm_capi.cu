@@ -392,8 +392,7 @@ int tsm_pairs_sched(const float* pts, const int64_t* off_a, const int32_t* len_a
     const int4* t4 = reinterpret_cast<const int4*>(tasks);
     int* queue = static_cast<int*>(workspace);
     int nt = n_tasks, total_warps = grid * W, wf = warp_smem_floats;
-    int tile_cap = wf / 32, g8_cap = wf / 4, wave_cap = wf;
-    void* args[] = {&A, &t4, &nt, &queue, &total_warps, &wf, &tile_cap, &g8_cap, &wave_cap};
+    void* args[] = {&A, &t4, &nt, &queue, &total_warps, &wf};
     e = cudaLaunchKernel(fn, dim3(grid), dim3(32 * W), args, (size_t)smem, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaLaunchKernel");
     return TSM_OK;

@@ -5,9 +5,10 @@
 //   kind 0  tile:   up to 32 pairs, one per lane (dp_pair: two skewed row
 //                   blocks per thread, boundary row in shared memory); for
 //                   pairs whose shorter side fits the tile capacity.
-//   kind 1  group8: up to 4 pairs, one per 8-lane group (group wavefront);
-//                   medium pairs.
-//   kind 2  wave:   1 pair per warp (group wavefront with G = 32); long pairs.
+//   kind 5/1/6/2  group4 / group8 / group16 / wave: up to 32/G pairs, one
+//                   per G-lane group (G = 4, 8, 16, 32), super-strip
+//                   wavefront (group_task); the planner picks G per pair so
+//                   that the longest pairs finish within a step budget.
 //   kind 3  hausdorff: up to 32 pairs, one per lane (no shared memory).
 //   kind 4  hausdorff, 1 pair per warp: the lanes split the points of both
 //                   trajectories, a warp max-reduction combines them.
@@ -20,20 +21,23 @@
 // resets both counters, so the next launch (or CUDA-graph replay) starts from
 // zero without a memset.  The queue is the only scratch memory.
 //
-// Group wavefront (G lanes per pair): the rows of the pair are cut into
-// strips of R rows dealt round-robin to the G lanes; local lane u computes
-// column j of its round-m strip at local step m*T + u + j (T = max(ncols,
-// G)).  The top value comes from lane u-1 by a width-G shuffle, lane 0 of a
-// round reads lane G-1's previous round from the group's ring (one row of
-// ncols floats in shared memory).  G = 1 would be the tile kernel; G = 32 the
-// wave kernel.
+// Group wavefront (G lanes per pair): see group_task.  G = 1 would be the
+// tile kernel's one pair per lane.
 #pragma once
 
 #include "tsm_tile.cuh"
 
 namespace tsm {
 
-enum TaskKind : int { TASK_TILE = 0, TASK_GROUP8 = 1, TASK_WAVE = 2, TASK_HAUSDORFF = 3, TASK_HAUSDORFF_WARP = 4 };
+enum TaskKind : int {
+    TASK_TILE = 0,
+    TASK_GROUP8 = 1,
+    TASK_WAVE = 2,  // G = 32
+    TASK_HAUSDORFF = 3,
+    TASK_HAUSDORFF_WARP = 4,
+    TASK_GROUP4 = 5,
+    TASK_GROUP16 = 6
+};
 
 // Everything a task needs besides its shared-memory slice.
 struct PairsArgs {
@@ -50,12 +54,25 @@ struct PairsArgs {
     int64_t out_stride;  // out[measure * out_stride + pair]
 };
 
-// One pair per G-lane group; `first` .. `first + count` of the order list,
-// group q of the warp takes pair first + q.  ring: this warp's shared
-// memory, cap floats per group.
+// One pair per G-lane group (G = 4, 8, 16 or 32); `first` .. `first + count`
+// of the order list, group q of the warp takes pair first + q.  ring_base:
+// this warp's shared memory, cap floats per group.
+//
+// Super-strips: the rows go in strips of G*R, lane u holding rows
+// u*R .. u*R+R-1 of the strip in registers.  Lane u computes column j of the
+// strip at step s = u + j, taking its top value from lane u-1 (computed at
+// step s-1) by a width-G shuffle; lane 0 takes it from the ring, which holds
+// the bottom row of the strip above (the top border before the first strip)
+// and which lane G-1 overwrites column by column, G-1 steps behind lane 0's
+// reads.  A strip takes nc + G - 1 steps.  The step loop has no per-lane
+// state besides j: it is unrolled by two, with the R values of a lane
+// alternating between two register arrays (no copies), and the column points
+// are fetched two steps ahead into two registers that alternate the same way.
 template <int M, int R, int G, bool EXACT>
 __device__ __forceinline__ void group_task(const PairsArgs& A, int first, int count, float* ring_base, int cap) {
     using C = typename CellOf<M, EXACT>::type;
+    constexpr unsigned kFull = 0xffffffffu;
+    constexpr int SS = G * R;  // rows per super-strip
     const int lane = threadIdx.x & 31;
     const int grp = lane / G;
     const int u = lane % G;
@@ -87,77 +104,89 @@ __device__ __forceinline__ void group_task(const PairsArgs& A, int first, int co
             srow = gapsum<EXACT>(rowp, nr, p);
             scol = gapsum<EXACT>(colp, nc, p);
         }
-        srow = __shfl_sync(0xffffffffu, srow, lane - u);
-        scol = __shfl_sync(0xffffffffu, scol, lane - u);
+        srow = __shfl_sync(kFull, srow, lane - u);
+        scol = __shfl_sync(kFull, scol, lane - u);
     }
-    const int n_strips = (nr + R - 1) / R;
-    const int T = nc > G ? nc : G;
-    const int last = n_strips - 1;
-    const int total = (valid && nr > 0 && nc > 0) ? (last / G) * T + (last % G) + nc : 0;  // live pairs only
-    const int steps = __reduce_max_sync(0xffffffffu, total);
-    const int res_u = valid && nr > 0 ? last % G : -1;
-    const int res_r = (nr - 1) - last * R;
-
     const bool live = valid && nr > 0 && nc > 0;  // no loads at all for an empty trajectory
-    float rx[R], ry[R], rg[R], D[R], px[R], py[R];
+    if (live)
+        for (int j = u; j < nc; j += G) ring[j] = C::topb(scol, j);
+    const int n_ss = live ? (nr + SS - 1) / SS : 0;
+    const int max_ss = __reduce_max_sync(kFull, n_ss);
+    const int max_span = __reduce_max_sync(kFull, live ? nc + G - 1 : 0);
+    const int last_u = ((nr - 1) % SS) / R;  // the lane and register of row nr-1 in the last strip
+    const int last_r = (nr - 1) % R;
+    float px[R], py[R];  // this lane's rows of the next strip
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const float2 q = live ? __ldg(rowp + min(u * R + r, nr - 1)) : make_float2(0.f, 0.f);
         px[r] = q.x;
         py[r] = q.y;
-        rx[r] = ry[r] = rg[r] = D[r] = 0.f;
     }
-    float diag = 0.f, bottom = 0.f, dlast = 0.f;
-    int j = -u, m = 0;
-    float2 cnext = live ? __ldg(colp) : make_float2(0.f, 0.f);
-    for (int t = 0; t < steps; ++t) {
-        const float from_left = __shfl_up_sync(0xffffffffu, bottom, 1, G);
-        const int g = G * m + u;
-        const bool act = j >= 0 && j < nc && g < n_strips;
-        if (act) {
-            if (j == 0) {
+    float dlast = 0.f;
+    __syncwarp();
+    for (int ss = 0; ss < max_ss; ++ss) {
+        const int row0 = ss * SS + u * R;
+        const bool on = live && ss < n_ss && row0 < nr;
+        float rx[R], ry[R], rg[R], DA[R], DB[R];
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    rx[r] = px[r];
-                    ry[r] = py[r];
-                    rg[r] = C::kGap ? gapdist<EXACT>(px[r], py[r], p) : 0.f;
-                    D[r] = C::rowb(srow, g * R + r);
-                    const float2 q = __ldg(rowp + min((g + G) * R + r, nr - 1));
-                    px[r] = q.x;
-                    py[r] = q.y;
-                }
-                diag = (g == 0) ? C::corner() : C::rowb(srow, g * R - 1);
-            }
-            const float top = (u == 0) ? ((m == 0) ? C::topb(scol, j) : ring[j]) : from_left;
-            const float2 c2 = cnext;
-            cnext = __ldg(colp + min(j + 1, nc - 1));
-            const float gc = C::kGap ? gapdist<EXACT>(c2.x, c2.y, p) : 0.f;
-            float up = top, dg = diag;
+        for (int r = 0; r < R; ++r) {
+            rx[r] = px[r];
+            ry[r] = py[r];
+            rg[r] = C::kGap ? gapdist<EXACT>(px[r], py[r], p) : 0.f;
+            DA[r] = DB[r] = C::rowb(srow, row0 + r);
+        }
+        if (on && ss + 1 < n_ss) {
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                const float left = D[r];
-                const float nv = C::cell(dg, up, left, d2f(rx[r], ry[r], c2.x, c2.y), rg[r], gc, p.eps2);
-                D[r] = nv;
-                dg = left;
-                up = nv;
+                const float2 q = __ldg(rowp + min(row0 + SS + r, nr - 1));
+                px[r] = q.x;
+                py[r] = q.y;
             }
-            diag = top;
-            bottom = up;
-            if (u == G - 1) ring[j] = up;
-            if (g == last && j == nc - 1) {
+        }
+        float diag = (row0 == 0) ? C::corner() : C::rowb(srow, row0 - 1);
+        float bottom = 0.f;
+        // column j is used at step u + j: even steps take cE, odd steps cO
+        const int je = u & 1, jo = je ^ 1;
+        float2 cE = on ? __ldg(colp + min(je, nc - 1)) : make_float2(0.f, 0.f);
+        float2 cO = on ? __ldg(colp + min(jo, nc - 1)) : make_float2(0.f, 0.f);
+        auto step = [&](const float (&Din)[R], float (&Dout)[R], float2& cs, int s) {
+            const float from_left = __shfl_up_sync(kFull, bottom, 1, G);
+            const int j = s - u;
+            if (on && (unsigned)j < (unsigned)nc) {
+                const float top = (u == 0) ? ring[j] : from_left;
+                const float2 c = cs;
+                cs = __ldg(colp + min(j + 2, nc - 1));
+                const float gc = C::kGap ? gapdist<EXACT>(c.x, c.y, p) : 0.f;
+                float up = top, dg = diag;
 #pragma unroll
-                for (int r = 0; r < R; ++r)
-                    if (r == res_r) dlast = D[r];
+                for (int r = 0; r < R; ++r) {
+                    const float left = Din[r];
+                    const float nv = C::cell(dg, up, left, d2f(rx[r], ry[r], c.x, c.y), rg[r], gc, p.eps2);
+                    Dout[r] = nv;
+                    dg = left;
+                    up = nv;
+                }
+                diag = top;
+                bottom = up;
+                if (u == G - 1) ring[j] = up;
             }
-            if (j == nc - 1) cnext = __ldg(colp);  // next round restarts at column 0
+            __syncwarp();
+        };
+        int s = 0;
+        for (; s + 1 < max_span; s += 2) {
+            step(DA, DB, cE, s);
+            step(DB, DA, cO, s + 1);
         }
-        if (++j == T) {
-            j = 0;
-            ++m;
+        if (s < max_span) step(DA, DB, cE, s);
+        if (on && ss == n_ss - 1 && u == last_u) {
+            // the lane's last column nc-1 was step u + nc - 1: even steps wrote DB, odd ones DA
+            const bool in_b = ((u + nc - 1) & 1) == 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (r == last_r) dlast = in_b ? DB[r] : DA[r];
         }
-        __syncwarp();
     }
-    if (valid && u == res_u) {
+    if (live && u == last_u) {
         float o;
         int c;
         finalize<M>(dlast, na, nb, o, c);
@@ -165,7 +194,7 @@ __device__ __forceinline__ void group_task(const PairsArgs& A, int first, int co
         if ((M == EDR || M == LCSS) && A.counts) A.counts[M * A.out_stride + k] = c;
     }
     // degenerate pairs (a zero length) have no steps: lane 0 of the group writes them
-    if (valid && (nr == 0 || nc == 0) && u == 0) {
+    if (valid && !live && u == 0) {
         float o;
         int c;
         finalize<M>(0.f, na, nb, o, c);
@@ -250,14 +279,16 @@ __device__ __forceinline__ void hausdorff_warp_task(const PairsArgs& A, int firs
 }
 
 template <int R, bool EXACT>
-__device__ __forceinline__ void run_task(const int4 task, const PairsArgs& A, float* wsm, int tile_cap, int g8_cap,
-                                         int wave_cap) {
+__device__ __forceinline__ void run_task(const int4 task, const PairsArgs& A, float* wsm, int warp_floats) {
     const int kind = task.x, m = task.y, first = task.z, count = task.w;
-#define TSM_TASK(MM)                                                                       \
-    case MM:                                                                               \
-        if (kind == TASK_TILE) tile_task<MM, R, EXACT>(A, first, count, wsm, tile_cap);     \
-        else if (kind == TASK_GROUP8) group_task<MM, R, 8, EXACT>(A, first, count, wsm, g8_cap); \
-        else group_task<MM, R, 32, EXACT>(A, first, count, wsm, wave_cap);                  \
+    // a G-lane group's ring holds warp_floats * G / 32 floats; a tile lane's boundary row warp_floats / 32
+#define TSM_TASK(MM)                                                                                     \
+    case MM:                                                                                             \
+        if (kind == TASK_TILE) tile_task<MM, R, EXACT>(A, first, count, wsm, warp_floats / 32);           \
+        else if (kind == TASK_GROUP4) group_task<MM, R, 4, EXACT>(A, first, count, wsm, warp_floats / 8);  \
+        else if (kind == TASK_GROUP8) group_task<MM, R, 8, EXACT>(A, first, count, wsm, warp_floats / 4);  \
+        else if (kind == TASK_GROUP16) group_task<MM, R, 16, EXACT>(A, first, count, wsm, warp_floats / 2); \
+        else group_task<MM, R, 32, EXACT>(A, first, count, wsm, warp_floats);                            \
         break;
     if (kind == TASK_HAUSDORFF) {
         hausdorff_task<R, EXACT>(A, first, count);
@@ -283,8 +314,7 @@ __device__ __forceinline__ void run_task(const int4 task, const PairsArgs& A, fl
 // before the first launch (self-resetting afterwards).
 template <int R, bool EXACT>
 __global__ void __launch_bounds__(128) dp_sched_kernel(PairsArgs A, const int4* __restrict__ tasks, int n_tasks,
-                                                       int* __restrict__ queue, int total_warps, int warp_floats,
-                                                       int tile_cap, int g8_cap, int wave_cap) {
+                                                       int* __restrict__ queue, int total_warps, int warp_floats) {
     extern __shared__ float smem[];
     const int lane = threadIdx.x & 31;
     float* wsm = smem + (threadIdx.x >> 5) * warp_floats;
@@ -293,7 +323,7 @@ __global__ void __launch_bounds__(128) dp_sched_kernel(PairsArgs A, const int4* 
         if (lane == 0) t = atomicAdd(queue, 1);
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= n_tasks) break;
-        run_task<R, EXACT>(tasks[t], A, wsm, tile_cap, g8_cap, wave_cap);
+        run_task<R, EXACT>(tasks[t], A, wsm, warp_floats);
     }
     if (lane == 0) {
         // every warp has made its last fetch before it counts itself out, so

@@ -7,15 +7,16 @@ Here a batch of pairs (any lengths up to the per-warp capacity, any mix of
 the six measures) is planned once on the host and executed by ONE persistent
 launch (tsm_pairs_sched) whose warps pull tasks from a device queue:
 
-* every (pair, measure) item goes to a bucket by the shorter side nc of its
-  DP (rows = the longer trajectory):
-    tile   (one pair per lane)      nc <= warp_floats/32
-    group8 (one pair per 8 lanes)   nc <= warp_floats/4
-    wave   (one pair per warp)      nc <= warp_floats
-  Hausdorff items are always one pair per lane.
-* inside a bucket items are sorted so a warp's lanes/groups get near-equal
-  trip counts, then cut into warp tasks: one-pair-per-lane buckets by loop
-  shape (row passes, then columns), the group buckets by step count;
+* every (pair, measure) item goes to a bucket by the shape of its DP (rows =
+  the longer trajectory, nr; columns = the shorter, nc):
+    tile   (one pair per lane)        nc <= warp_floats/32 and a short loop
+    groupG (one pair per G lanes)     G = 4, 8, 16 or 32 (wave), the smallest
+                                      G whose super-strip loop takes at most
+                                      max_steps steps, nc <= warp_floats*G/32
+  Hausdorff items are one pair per lane, or one per warp when long.
+* inside a bucket items are sorted by loop shape (row passes or super-strips,
+  then columns) so a warp's lanes/groups get equal trip counts, then cut into
+  warp tasks;
 * all tasks are sorted by estimated cost, largest first (longest-processing-
   time-first), so the long pairs start at once and short tasks fill the tail.
 
@@ -36,18 +37,27 @@ import torch
 from . import _lib
 from .engine import _ptr, _stream_ptr, measure_id
 
-KIND_TILE, KIND_GROUP8, KIND_WAVE, KIND_HAUSDORFF, KIND_HAUSDORFF_WARP = 0, 1, 2, 3, 4
+KIND_TILE, KIND_GROUP8, KIND_WAVE, KIND_HAUSDORFF, KIND_HAUSDORFF_WARP, KIND_GROUP4, KIND_GROUP16 = 0, 1, 2, 3, 4, 5, 6
+GROUP_KIND = {4: KIND_GROUP4, 8: KIND_GROUP8, 16: KIND_GROUP16, 32: KIND_WAVE}
+# A pair may keep its lanes for at most this many loop steps (one step = R
+# cells per lane) before the planner spreads it over more lanes.
+MAX_STEPS = 8192
 # Hausdorff pairs with more point-segment evaluations than this run one per
 # warp (the lanes split the points) instead of one per lane.
 HAUSDORFF_WARP_UNITS = 1 << 17
 CANDIDATES = [(8, 4096), (8, 2048), (8, 8192), (4, 4096)]
 
 
-def _steps(nr, nc, rows, G):
-    strips = (nr + rows - 1) // rows
-    last = np.maximum(strips - 1, 0)
-    T = np.maximum(nc, G)
-    return (last // G) * T + (last % G) + nc
+def group_steps(nr, nc, rows, G):
+    """Loop steps of a pair on a G-lane group: super-strips of G*rows rows,
+    nc + G - 1 steps each."""
+    return ((nr + G * rows - 1) // (G * rows)) * (nc + G - 1)
+
+
+def tile_steps(nr, nc, rows):
+    """Loop steps of a pair on one lane of a tile task: passes of 2*rows rows,
+    nc + 1 steps each (one step = 2*rows cells)."""
+    return ((nr + 2 * rows - 1) // (2 * rows)) * (nc + 1)
 
 
 @dataclass
@@ -65,13 +75,13 @@ class Plan:
         return int(self.tasks.shape[0])
 
 
-def plan_pairs(len_a, len_b, measures, rows=8, warp_floats=4096) -> Plan:
+def plan_pairs(len_a, len_b, measures, rows=8, warp_floats=4096, max_steps=MAX_STEPS) -> Plan:
     """Buckets, orders and cuts the (pair, measure) items into warp tasks."""
     la = np.asarray(len_a, dtype=np.int64)
     lb = np.asarray(len_b, dtype=np.int64)
     n = la.shape[0]
     nr, nc = np.maximum(la, lb), np.minimum(la, lb)
-    tile_cap, g8_cap, wave_cap = warp_floats // 32, warp_floats // 4, warp_floats
+    tile_cap, wave_cap = warp_floats // 32, warp_floats
     ms = [measure_id(m) for m in measures]
     dp_ms = [m for m in ms if m != _lib.HAUSDORFF]
     if dp_ms and n and nc.max() > wave_cap:
@@ -108,15 +118,26 @@ def plan_pairs(len_a, len_b, measures, rows=8, warp_floats=4096) -> Plan:
             emit(KIND_HAUSDORFF, m, all_idx[~big], 32, units * 1.8, hshape)
             emit(KIND_HAUSDORFF_WARP, m, all_idx[big], 1, units * 1.8 / 32 + 64 * (la + lb))
             continue
-        tile = nc <= tile_cap
-        g8 = ~tile & (nc <= g8_cap)
-        wave = ~tile & ~g8
+        # a tile step does 2*rows cells per lane, about two group steps' work
+        tile = (nc <= tile_cap) & (2 * tile_steps(nr, nc, rows) <= max_steps)
         passes = (nr + 2 * rows - 1) // (2 * rows)
         # a tile lane runs passes x (nc + 1) steps: group by passes, then by nc
         emit(KIND_TILE, m, all_idx[tile], 32, (passes * 2 * rows * (nc + 1)).astype(np.float64),
              passes * 65536 + nc)
-        emit(KIND_GROUP8, m, all_idx[g8], 4, (_steps(nr, nc, rows, 8) * rows * 1.3).astype(np.float64))
-        emit(KIND_WAVE, m, all_idx[wave], 1, (_steps(nr, nc, rows, 32) * rows * 1.3).astype(np.float64))
+        todo = ~tile
+        gsize = np.zeros(n, np.int64)
+        for G in (4, 8, 16, 32):  # the smallest group within the step budget
+            fits = todo & (nc <= warp_floats * G // 32)
+            pick = fits & (group_steps(nr, nc, rows, G) <= max_steps)
+            if G == 32:
+                pick = fits  # the widest group takes what is left
+            gsize[pick] = G
+            todo &= ~pick
+        for G in (4, 8, 16, 32):
+            sel = gsize == G
+            strips = (nr + G * rows - 1) // (G * rows)
+            emit(GROUP_KIND[G], m, all_idx[sel], 32 // G,
+                 (group_steps(nr, nc, rows, G) * rows * 1.3).astype(np.float64), strips * 65536 + nc)
     if not tasks:
         return Plan(np.zeros(0, np.int32), np.zeros((0, 4), np.int32), rows, warp_floats, ms, 0, np.zeros(0))
     order = np.concatenate(orders)
@@ -135,11 +156,11 @@ class PairsScheduler:
     counts[measure_id, pair] (int32, EDR/LCSS)."""
 
     def __init__(self, pts, off_a, len_a, off_b, len_b, measures, *, eps=0.0, gpoint=(0.0, 0.0), exact=False,
-                 rows=8, warp_floats=4096, len_a_host=None, len_b_host=None, plan=None):
+                 rows=8, warp_floats=4096, max_steps=MAX_STEPS, len_a_host=None, len_b_host=None, plan=None):
         self.dev = pts.device
         la = np.asarray(len_a_host if len_a_host is not None else len_a.cpu().numpy())
         lb = np.asarray(len_b_host if len_b_host is not None else len_b.cpu().numpy())
-        self.plan = plan or plan_pairs(la, lb, measures, rows, warp_floats)
+        self.plan = plan or plan_pairs(la, lb, measures, rows, warp_floats, max_steps)
         self.pts, self.off_a, self.len_a, self.off_b, self.len_b = pts, off_a, len_a, off_b, len_b
         self.n = int(off_a.shape[0])
         self.order = torch.from_numpy(self.plan.order).to(self.dev)
