@@ -58,6 +58,24 @@ __device__ __forceinline__ float d2f(float ax, float ay, float bx, float by) {
     return __fmaf_rn(dy, dy, __fmul_rn(dx, dx));
 }
 
+// The same squared distance with the row point held negated, nr = -r: the
+// difference c + nr = -(r - c) is exactly the negated scalar difference
+// (round-to-nearest is symmetric) and the squares do not see the sign, so
+// the value is bit-identical to d2f(r.x, r.y, c.x, c.y).  PACKED: the
+// difference is one f32x2 add instead of two scalar adds.  Measured on B200
+// (same inputs, same outputs): the packed add is faster for every measure
+// with per-lane global columns (paired batches, 5-15 %) and for DTW, EDR,
+// LCSS and ERP with columns staged in shared memory (all-pairs, 0.5-4 %);
+// discrete Frechet with shared-memory columns is 2 % faster with the scalar
+// adds (kPackedSmem in the cell policies).
+template <bool PACKED>
+__device__ __forceinline__ float d2nr(float2 nr, float2 c) {
+    float2 d;
+    if constexpr (PACKED) d = __fadd2_rn(nr, c);
+    else d = make_float2(__fadd_rn(nr.x, c.x), __fadd_rn(nr.y, c.y));
+    return __fmaf_rn(d.y, d.y, __fmul_rn(d.x, d.x));
+}
+
 // Kernel parameters (device copy of tsm_params, pre-digested on the host).
 struct KParams {
     float eps2;        // (float)(eps*eps)
@@ -98,6 +116,7 @@ __device__ __forceinline__ float gapsum(const float2* __restrict__ t, int n, con
 template <bool EXACT>
 struct DtwCell {
     static constexpr bool kGap = false;
+    static constexpr bool kPackedSmem = true;  // f32x2 difference with shared-memory columns (see d2nr)
     __device__ __forceinline__ static float corner() { return 0.f; }
     __device__ __forceinline__ static float rowb(float /*srow*/, int /*i*/) { return CUDART_INF_F; }
     __device__ __forceinline__ static float topb(float /*scol*/, int /*j*/) { return CUDART_INF_F; }
@@ -112,6 +131,7 @@ struct DtwCell {
 template <bool EXACT>
 struct FrechetCell {
     static constexpr bool kGap = false;
+    static constexpr bool kPackedSmem = false;  // f32x2 difference with shared-memory columns (see d2nr)
     __device__ __forceinline__ static float corner() { return 0.f; }
     __device__ __forceinline__ static float rowb(float, int) { return CUDART_INF_F; }
     __device__ __forceinline__ static float topb(float, int) { return CUDART_INF_F; }
@@ -126,6 +146,7 @@ struct FrechetCell {
 template <bool EXACT>
 struct ErpCell {
     static constexpr bool kGap = true;
+    static constexpr bool kPackedSmem = true;  // f32x2 difference with shared-memory columns (see d2nr)
     __device__ __forceinline__ static float corner() { return 0.f; }
     __device__ __forceinline__ static float rowb(float srow, int) { return srow; }
     __device__ __forceinline__ static float topb(float scol, int) { return scol; }
@@ -144,6 +165,7 @@ struct ErpCell {
 template <bool EXACT>
 struct EdrCell {
     static constexpr bool kGap = false;
+    static constexpr bool kPackedSmem = true;  // f32x2 difference with shared-memory columns (see d2nr)
     __device__ __forceinline__ static float corner() { return 2.f; }
     __device__ __forceinline__ static float rowb(float, int i) { return (float)(1 - i); }
     __device__ __forceinline__ static float topb(float, int j) { return (float)(1 - j); }
@@ -160,6 +182,7 @@ struct EdrCell {
 template <bool EXACT>
 struct LcssCell {
     static constexpr bool kGap = false;
+    static constexpr bool kPackedSmem = true;  // f32x2 difference with shared-memory columns (see d2nr)
     __device__ __forceinline__ static float corner() { return 0.f; }
     __device__ __forceinline__ static float rowb(float, int) { return 0.f; }
     __device__ __forceinline__ static float topb(float, int) { return 0.f; }

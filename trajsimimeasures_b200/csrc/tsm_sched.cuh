@@ -127,11 +127,11 @@ __device__ __forceinline__ void group_task(const PairsArgs& A, int first, int co
     for (int ss = 0; ss < max_ss; ++ss) {
         const int row0 = ss * SS + u * R;
         const bool on = live && ss < n_ss && row0 < nr;
-        float rx[R], ry[R], rg[R], DA[R], DB[R];
+        float2 rn[R];  // negated row points (d2nr)
+        float rg[R], DA[R], DB[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            rx[r] = px[r];
-            ry[r] = py[r];
+            rn[r] = make_float2(-px[r], -py[r]);
             rg[r] = C::kGap ? gapdist<EXACT>(px[r], py[r], p) : 0.f;
             DA[r] = DB[r] = C::rowb(srow, row0 + r);
         }
@@ -161,7 +161,7 @@ __device__ __forceinline__ void group_task(const PairsArgs& A, int first, int co
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const float left = Din[r];
-                    const float nv = C::cell(dg, up, left, d2f(rx[r], ry[r], c.x, c.y), rg[r], gc, p.eps2);
+                    const float nv = C::cell(dg, up, left, d2nr<true>(rn[r], c), rg[r], gc, p.eps2);
                     Dout[r] = nv;
                     dg = left;
                     up = nv;

@@ -22,6 +22,8 @@
 // and a __syncthreads per anti-diagonal), core/hausdorff.py:12-93.
 #pragma once
 
+#include <type_traits>
+
 #include "tsm_device.cuh"
 
 namespace tsm {
@@ -55,11 +57,12 @@ __device__ __forceinline__ float4 col4(const SmemCols& c, int j, const KParams&,
     return c.pt4(j);
 }
 
-// R consecutive rows of a pair's DP: their points (and ERP gap distances)
-// and their current DP values, all in registers.
-template <class C, int R, bool EXACT>
+// R consecutive rows of a pair's DP: their points (negated, for d2nr), their
+// ERP gap distances and their current DP values, all in registers.
+template <class C, int R, bool EXACT, bool PACKED = true>
 struct RowBlock {
-    float x[R], y[R], g[R], D[R];
+    float2 n[R];
+    float g[R], D[R];
 
     // rows i0 .. i0+R-1; rows past the end repeat the last point (their
     // values are never read by a valid cell)
@@ -68,8 +71,7 @@ struct RowBlock {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const float2 q = __ldg(rowp + min(i0 + r, nr - 1));
-            x[r] = q.x;
-            y[r] = q.y;
+            n[r] = make_float2(-q.x, -q.y);
             g[r] = C::kGap ? gapdist<EXACT>(q.x, q.y, p) : 0.f;
             D[r] = C::rowb(srow, i0 + r);
         }
@@ -82,7 +84,7 @@ struct RowBlock {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const float left = D[r];
-            const float nv = C::cell(dg, up, left, d2f(x[r], y[r], c.x, c.y), g[r], c.z, eps2);
+            const float nv = C::cell(dg, up, left, d2nr<PACKED>(n[r], make_float2(c.x, c.y)), g[r], c.z, eps2);
             D[r] = nv;
             dg = left;
             up = nv;
@@ -99,7 +101,7 @@ struct RowBlock {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const float left = Din[r];
-            const float nv = C::cell(dg, up, left, d2f(x[r], y[r], c.x, c.y), g[r], c.z, eps2);
+            const float nv = C::cell(dg, up, left, d2nr<PACKED>(n[r], make_float2(c.x, c.y)), g[r], c.z, eps2);
             Dout[r] = nv;
             dg = left;
             up = nv;
@@ -115,6 +117,13 @@ struct RowBlock {
         return v;
     }
 };
+
+// The f32x2 form of the cell distance (d2nr): always with per-lane global
+// columns, per measure (C::kPackedSmem) with shared-memory columns.
+template <class C, class Cols>
+constexpr bool kPacked() {
+    return std::is_same<Cols, SmemCols>::value ? C::kPackedSmem : true;
+}
 
 // Lower-block-first form of the two-block pass (used by dp_pair for EDR and
 // LCSS with shared-memory columns, where it was measured 3-5 % faster; the
@@ -132,7 +141,7 @@ __device__ __forceinline__ float dp_pair_lower_first(const float2* __restrict__ 
     float dlast = 0.f;
     int rb = 0;
     for (; nr - rb > R; rb += 2 * R) {
-        RowBlock<C, R, EXACT> hi, lo;
+        RowBlock<C, R, EXACT, kPacked<C, Cols>()> hi, lo;
         hi.load(rowp, rb, nr, srow, p);
         lo.load(rowp, rb + R, nr, srow, p);
         float HA[R], HB[R], LA[R], LB[R];
@@ -181,7 +190,7 @@ __device__ __forceinline__ float dp_pair_lower_first(const float2* __restrict__ 
         buf[32 * (nc - 1)] = lb;
     }
     if (rb < nr) {  // last rows (at most R): one block, ping-pong over column pairs
-        RowBlock<C, R, EXACT> blk;
+        RowBlock<C, R, EXACT, kPacked<C, Cols>()> blk;
         blk.load(rowp, rb, nr, srow, p);
         float DA[R], DB[R];
 #pragma unroll
@@ -226,9 +235,10 @@ struct LowerFirst<LCSS, SmemCols> {
     static constexpr bool value = true;
 };
 
-// The DP of one pair.  rowp/nr: row trajectory; cols/nc: column trajectory;
-// buf: this thread's boundary row (element j at buf[32*j]); srow/scol: ERP
-// gap totals of the row/column trajectory.  Returns D(nr-1, nc-1).
+// The DP of one pair, prefetching form (dp_pair's default).  rowp/nr: row
+// trajectory; cols/nc: column trajectory; buf: this thread's boundary row
+// (element j at buf[32*j]); srow/scol: ERP gap totals of the row/column
+// trajectory.  Returns D(nr-1, nc-1).
 //
 // Rows go in passes of 2R: an upper and a lower block of R rows, the lower
 // one column behind the upper.  At step j the upper block computes column j
@@ -243,16 +253,14 @@ struct LowerFirst<LCSS, SmemCols> {
 // slower: assembling the pairs around the scalar min/max costs more than the
 // packed arithmetic saves.)
 template <int M, int R, bool EXACT, class Cols>
-__device__ __forceinline__ float dp_pair(const float2* __restrict__ rowp, int nr, const Cols& cols,
-                                         int nc, float* buf, const KParams& p, float srow, float scol) {
+__device__ __forceinline__ float dp_pair_prefetch(const float2* __restrict__ rowp, int nr, const Cols& cols,
+                                                  int nc, float* buf, const KParams& p, float srow, float scol) {
     using C = typename CellOf<M, EXACT>::type;
-    if (nr <= 0 || nc <= 0) return 0.f;
-    if constexpr (LowerFirst<M, Cols>::value) return dp_pair_lower_first<M, R, EXACT>(rowp, nr, cols, nc, buf, p, srow, scol);
     for (int j = 0; j < nc; ++j) buf[32 * j] = C::topb(scol, j);
     float dlast = 0.f;
     int rb = 0;
     for (; nr - rb > R; rb += 2 * R) {
-        RowBlock<C, R, EXACT> hi, lo;
+        RowBlock<C, R, EXACT, kPacked<C, Cols>()> hi, lo;
         hi.load(rowp, rb, nr, srow, p);
         lo.load(rowp, rb + R, nr, srow, p);
         float HA[R], HB[R], LA[R], LB[R];
@@ -312,7 +320,7 @@ __device__ __forceinline__ float dp_pair(const float2* __restrict__ rowp, int nr
         buf[32 * (nc - 1)] = lb;
     }
     if (rb < nr) {  // last rows (at most R): one block
-        RowBlock<C, R, EXACT> blk;
+        RowBlock<C, R, EXACT, kPacked<C, Cols>()> blk;
         blk.load(rowp, rb, nr, srow, p);
         float diag = (rb == 0) ? C::corner() : C::rowb(srow, rb - 1);
         float4 cn = col4<EXACT>(cols, 0, p, C::kGap);
@@ -330,6 +338,20 @@ __device__ __forceinline__ float dp_pair(const float2* __restrict__ rowp, int nr
     }
     return dlast;
 }
+
+// The DP of one pair: the lower-block-first pass where it was measured
+// faster (EDR and LCSS with shared-memory columns), else the prefetching one.
+template <int M, int R, bool EXACT, class Cols>
+__device__ __forceinline__ float dp_pair(const float2* __restrict__ rowp, int nr, const Cols& cols,
+                                         int nc, float* buf, const KParams& p, float srow, float scol) {
+    if (nr <= 0 || nc <= 0) return 0.f;
+    if constexpr (LowerFirst<M, Cols>::value) {
+        return dp_pair_lower_first<M, R, EXACT>(rowp, nr, cols, nc, buf, p, srow, scol);
+    } else {
+        return dp_pair_prefetch<M, R, EXACT>(rowp, nr, cols, nc, buf, p, srow, scol);
+    }
+}
+
 
 // Pairs mode ------------------------------------------------------------------
 // Block = 32*W threads, dynamic shared memory = W*32*cap floats.

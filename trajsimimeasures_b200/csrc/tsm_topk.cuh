@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(kTopkThreads) topk_rows_kernel(const float* __
                                                                  int64_t ld, int k, float* __restrict__ out_d,
                                                                  int32_t* __restrict__ out_i) {
     __shared__ uint32_t hist[256];
-    __shared__ uint32_t s_prefix, s_need, s_nless, s_neq;
+    __shared__ uint32_t s_prefix, s_need, s_nless;
     __shared__ uint64_t cand[kTopkMax];  // (key << 32) | column, sorted at the end
     __shared__ uint32_t ties[kTopkMax];
     const float* row = d + (int64_t)blockIdx.x * ld;
@@ -71,10 +71,7 @@ __global__ void __launch_bounds__(kTopkThreads) topk_rows_kernel(const float* __
         __syncthreads();
     }
     // prefix = T, the kk-th smallest key; `need` keys equal to T belong to the result
-    if (tid == 0) {
-        s_nless = 0;
-        s_neq = 0;
-    }
+    if (tid == 0) s_nless = 0;
     __syncthreads();
     for (int64_t c = tid; c < n_cols; c += blockDim.x) {
         const uint32_t key = fkey(row[c]);
