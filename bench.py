@@ -471,7 +471,8 @@ def run_uneven(args):
     best, tried = sched.autotune(*T, ms_, eps=EPS, len_a_host=la, len_b_host=lb)
     tune_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    sc = sched.PairsScheduler(*T, ms_, eps=EPS, rows=best[0], warp_floats=best[1], len_a_host=la, len_b_host=lb)
+    sc = sched.PairsScheduler(*T, ms_, eps=EPS, rows=best[0], warp_floats=best[1], max_steps=best[2], len_a_host=la,
+                              len_b_host=lb)
     plan_s = time.perf_counter() - t0
     sc.capture()
     for _ in range(args.warmup):
@@ -508,7 +509,7 @@ def run_uneven(args):
         "workload": f"uneven_{args.n_pairs}_pairs_lognormal_dtw+dfrechet+edr", "metric": "DP cells/s",
         "value": cells / (ms_sched / 1e3), "unit": "cells/s", "pairs_per_s": 3 * len(ia) / (ms_sched / 1e3),
         "ms_per_launch": ms_sched, "graph_replay": True,
-        "autotuned": {"rows": best[0], "warp_floats": best[1], "candidates_ms": tried},
+        "autotuned": {"rows": best[0], "warp_floats": best[1], "max_steps": best[2], "candidates_ms": tried},
         "tasks_by_kind": {"tile": kinds[0], "group4": kinds[5], "group8": kinds[1], "group16": kinds[6],
                           "wave": kinds[2]},
         "plain_tsm_pairs_ms": ms_plain, "speedup_vs_plain": ms_plain / ms_sched,

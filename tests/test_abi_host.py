@@ -154,7 +154,15 @@ def test_sched_plan_covers_every_item_once():
         pl = sched.plan_pairs(la, lb, ["dtw", "dfrechet", "edr", "hausdorff"], rows=rows, warp_floats=wf)
         t = pl.tasks
         assert t.dtype == np.int32 and t.shape[1] == 4
-        assert np.all(np.diff(pl.cost) <= 0)  # largest first
+        # long tasks first, largest first; then one measure after the other, each largest first
+        long = pl.cost > pl.cost.sum() / sched.WARPS / 4
+        n_long = int(long.sum())
+        assert np.all(long[:n_long]) and not np.any(long[n_long:])
+        assert np.all(np.diff(pl.cost[:n_long]) <= 0)
+        rest_m = t[n_long:, 1]
+        assert np.sum(np.diff(rest_m) != 0) == len(set(rest_m.tolist())) - 1  # contiguous measure blocks
+        for m in set(rest_m.tolist()):
+            assert np.all(np.diff(pl.cost[n_long:][rest_m == m]) <= 0)
         nc = np.minimum(la, lb)
         seen = {m: np.zeros(len(la), np.int64) for m in (0, 4, 1, 5)}
         for kind, m, first, cnt in t:
@@ -191,5 +199,5 @@ def test_autotune_signature_and_cache(tmp_path, monkeypatch):
     a = sched.signature([10, 20, 300], [40, 50, 60], ["dtw", "edr"])
     b = sched.signature([10, 20, 300], [40, 50, 60], ["edr", "dtw"])
     assert a == b
-    sched.save_cache({"k": {"best": [8, 4096]}})
-    assert sched.load_cache()["k"]["best"] == [8, 4096]
+    sched.save_cache({"k": {"best": [8, 4096, 8192]}})
+    assert sched.load_cache()["k"]["best"] == [8, 4096, 8192]

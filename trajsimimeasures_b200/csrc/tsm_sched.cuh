@@ -25,6 +25,8 @@
 // tile kernel's one pair per lane.
 #pragma once
 
+#include <type_traits>
+
 #include "tsm_tile.cuh"
 
 namespace tsm {
@@ -53,6 +55,9 @@ struct PairsArgs {
     int32_t* counts;
     int64_t out_stride;  // out[measure * out_stride + pair]
 };
+
+// Group tasks stage their column points in shared memory when they fit.
+constexpr bool kGroupStageCols = true;
 
 // One pair per G-lane group (G = 4, 8, 16 or 32); `first` .. `first + count`
 // of the order list, group q of the warp takes pair first + q.  ring_base:
@@ -110,6 +115,14 @@ __device__ __forceinline__ void group_task(const PairsArgs& A, int first, int co
     const bool live = valid && nr > 0 && nc > 0;  // no loads at all for an empty trajectory
     if (live)
         for (int j = u; j < nc; j += G) ring[j] = C::topb(scol, j);
+    // The column points go to shared memory after the ring (float2, 8-byte
+    // aligned) when every group of the warp has room for them: the step loop
+    // then reads them there instead of from global memory.
+    const int ring_len = (nc + 1) & ~1;
+    const bool staged = kGroupStageCols && __all_sync(kFull, !live || ring_len + 2 * nc <= cap);
+    float2* scols = reinterpret_cast<float2*>(ring + ring_len);
+    if (staged && live)
+        for (int j = u; j < nc; j += G) scols[j] = __ldg(colp + j);
     const int n_ss = live ? (nr + SS - 1) / SS : 0;
     const int max_ss = __reduce_max_sync(kFull, n_ss);
     const int max_span = __reduce_max_sync(kFull, live ? nc + G - 1 : 0);
@@ -124,68 +137,77 @@ __device__ __forceinline__ void group_task(const PairsArgs& A, int first, int co
     }
     float dlast = 0.f;
     __syncwarp();
-    for (int ss = 0; ss < max_ss; ++ss) {
-        const int row0 = ss * SS + u * R;
-        const bool on = live && ss < n_ss && row0 < nr;
-        float2 rn[R];  // negated row points (d2nr)
-        float rg[R], DA[R], DB[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            rn[r] = make_float2(-px[r], -py[r]);
-            rg[r] = C::kGap ? gapdist<EXACT>(px[r], py[r], p) : 0.f;
-            DA[r] = DB[r] = C::rowb(srow, row0 + r);
-        }
-        if (on && ss + 1 < n_ss) {
+    auto sweep = [&](auto staged_tag) {
+        constexpr bool ST = decltype(staged_tag)::value;
+        auto col = [&](int j) -> float2 {
+            if constexpr (ST) return scols[j];
+            else return __ldg(colp + j);
+        };
+        for (int ss = 0; ss < max_ss; ++ss) {
+            const int row0 = ss * SS + u * R;
+            const bool on = live && ss < n_ss && row0 < nr;
+            float2 rn[R];  // negated row points (d2nr)
+            float rg[R], DA[R], DB[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                const float2 q = __ldg(rowp + min(row0 + SS + r, nr - 1));
-                px[r] = q.x;
-                py[r] = q.y;
+                rn[r] = make_float2(-px[r], -py[r]);
+                rg[r] = C::kGap ? gapdist<EXACT>(px[r], py[r], p) : 0.f;
+                DA[r] = DB[r] = C::rowb(srow, row0 + r);
             }
-        }
-        float diag = (row0 == 0) ? C::corner() : C::rowb(srow, row0 - 1);
-        float bottom = 0.f;
-        // column j is used at step u + j: even steps take cE, odd steps cO
-        const int je = u & 1, jo = je ^ 1;
-        float2 cE = on ? __ldg(colp + min(je, nc - 1)) : make_float2(0.f, 0.f);
-        float2 cO = on ? __ldg(colp + min(jo, nc - 1)) : make_float2(0.f, 0.f);
-        auto step = [&](const float (&Din)[R], float (&Dout)[R], float2& cs, int s) {
-            const float from_left = __shfl_up_sync(kFull, bottom, 1, G);
-            const int j = s - u;
-            if (on && (unsigned)j < (unsigned)nc) {
-                const float top = (u == 0) ? ring[j] : from_left;
-                const float2 c = cs;
-                cs = __ldg(colp + min(j + 2, nc - 1));
-                const float gc = C::kGap ? gapdist<EXACT>(c.x, c.y, p) : 0.f;
-                float up = top, dg = diag;
+            if (on && ss + 1 < n_ss) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    const float left = Din[r];
-                    const float nv = C::cell(dg, up, left, d2nr<true>(rn[r], c), rg[r], gc, p.eps2);
-                    Dout[r] = nv;
-                    dg = left;
-                    up = nv;
+                    const float2 q = __ldg(rowp + min(row0 + SS + r, nr - 1));
+                    px[r] = q.x;
+                    py[r] = q.y;
                 }
-                diag = top;
-                bottom = up;
-                if (u == G - 1) ring[j] = up;
             }
-            __syncwarp();
-        };
-        int s = 0;
-        for (; s + 1 < max_span; s += 2) {
-            step(DA, DB, cE, s);
-            step(DB, DA, cO, s + 1);
-        }
-        if (s < max_span) step(DA, DB, cE, s);
-        if (on && ss == n_ss - 1 && u == last_u) {
-            // the lane's last column nc-1 was step u + nc - 1: even steps wrote DB, odd ones DA
-            const bool in_b = ((u + nc - 1) & 1) == 0;
+            float diag = (row0 == 0) ? C::corner() : C::rowb(srow, row0 - 1);
+            float bottom = 0.f;
+            // column j is used at step u + j: even steps take cE, odd steps cO
+            const int je = u & 1, jo = je ^ 1;
+            float2 cE = on ? col(min(je, nc - 1)) : make_float2(0.f, 0.f);
+            float2 cO = on ? col(min(jo, nc - 1)) : make_float2(0.f, 0.f);
+            auto step = [&](const float (&Din)[R], float (&Dout)[R], float2& cs, int s) {
+                const float from_left = __shfl_up_sync(kFull, bottom, 1, G);
+                const int j = s - u;
+                if (on && (unsigned)j < (unsigned)nc) {
+                    const float top = (u == 0) ? ring[j] : from_left;
+                    const float2 c = cs;
+                    cs = col(min(j + 2, nc - 1));
+                    const float gc = C::kGap ? gapdist<EXACT>(c.x, c.y, p) : 0.f;
+                    float up = top, dg = diag;
 #pragma unroll
-            for (int r = 0; r < R; ++r)
-                if (r == last_r) dlast = in_b ? DB[r] : DA[r];
+                    for (int r = 0; r < R; ++r) {
+                        const float left = Din[r];
+                        const float nv = C::cell(dg, up, left, d2nr<true>(rn[r], c), rg[r], gc, p.eps2);
+                        Dout[r] = nv;
+                        dg = left;
+                        up = nv;
+                    }
+                    diag = top;
+                    bottom = up;
+                    if (u == G - 1) ring[j] = up;
+                }
+                __syncwarp();
+            };
+            int s = 0;
+            for (; s + 1 < max_span; s += 2) {
+                step(DA, DB, cE, s);
+                step(DB, DA, cO, s + 1);
+            }
+            if (s < max_span) step(DA, DB, cE, s);
+            if (on && ss == n_ss - 1 && u == last_u) {
+                // the lane's last column nc-1 was step u + nc - 1: even steps wrote DB, odd ones DA
+                const bool in_b = ((u + nc - 1) & 1) == 0;
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r == last_r) dlast = in_b ? DB[r] : DA[r];
+            }
         }
-    }
+    };
+    if (staged) sweep(std::true_type{});
+    else sweep(std::false_type{});
     if (live && u == last_u) {
         float o;
         int c;

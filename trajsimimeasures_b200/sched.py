@@ -17,10 +17,11 @@ launch (tsm_pairs_sched) whose warps pull tasks from a device queue:
 * inside a bucket items are sorted by loop shape (row passes or super-strips,
   then columns) so a warp's lanes/groups get equal trip counts, then cut into
   warp tasks;
-* all tasks are sorted by estimated cost, largest first (longest-processing-
-  time-first), so the long pairs start at once and short tasks fill the tail.
+* the long tasks go first, largest first (longest-processing-time-first), so
+  no long pair starts near the end; the rest follow one measure after the
+  other, each largest first (task_order).
 
-The autotuner picks (rows per strip, shared memory per warp) for a batch by
+The autotuner picks (rows per strip, shared memory per warp, step budget) for a batch by
 timing candidate plans on the device; choices are cached as JSON keyed by GPU
 name, measures and a length-distribution signature.
 """
@@ -42,10 +43,15 @@ GROUP_KIND = {4: KIND_GROUP4, 8: KIND_GROUP8, 16: KIND_GROUP16, 32: KIND_WAVE}
 # A pair may keep its lanes for at most this many loop steps (one step = R
 # cells per lane) before the planner spreads it over more lanes.
 MAX_STEPS = 8192
+# Resident warps of a launch, for the task order when the caller gives none
+# (B200: 148 SMs x 12 warps at 16 KB of shared memory per warp).
+WARPS = 148 * 12
 # Hausdorff pairs with more point-segment evaluations than this run one per
 # warp (the lanes split the points) instead of one per lane.
 HAUSDORFF_WARP_UNITS = 1 << 17
-CANDIDATES = [(8, 4096), (8, 2048), (8, 8192), (4, 4096)]
+# (rows per strip, shared-memory floats per warp, step budget) tried by the autotuner
+CANDIDATES = [(8, 4096, 8192), (8, 4096, 16384), (8, 3072, 8192), (8, 2048, 8192), (8, 8192, 8192),
+              (4, 4096, 8192)]
 
 
 def group_steps(nr, nc, rows, G):
@@ -75,8 +81,10 @@ class Plan:
         return int(self.tasks.shape[0])
 
 
-def plan_pairs(len_a, len_b, measures, rows=8, warp_floats=4096, max_steps=MAX_STEPS) -> Plan:
-    """Buckets, orders and cuts the (pair, measure) items into warp tasks."""
+def plan_pairs(len_a, len_b, measures, rows=8, warp_floats=4096, max_steps=MAX_STEPS, warps=None) -> Plan:
+    """Buckets, orders and cuts the (pair, measure) items into warp tasks.
+    warps: the number of warps the launch keeps resident (for task_order)."""
+    warps = WARPS if warps is None else warps
     la = np.asarray(len_a, dtype=np.int64)
     lb = np.asarray(len_b, dtype=np.int64)
     n = la.shape[0]
@@ -143,9 +151,29 @@ def plan_pairs(len_a, len_b, measures, rows=8, warp_floats=4096, max_steps=MAX_S
     order = np.concatenate(orders)
     T = np.concatenate(tasks)
     C = np.concatenate(costs)
-    s = np.argsort(-C, kind="stable")
+    s = task_order(T[:, 1], C, warps)
     return Plan(order, np.ascontiguousarray(T[s]), rows, warp_floats, ms,
                 int(max(la.max(initial=0), lb.max(initial=0))), C[s])
+
+
+def task_order(measure, cost, warps=WARPS):
+    """Queue order of the tasks: the long ones first, largest first
+    (longest-processing-time-first, so that no long task starts near the
+    end), then the rest one measure after the other, each largest first.
+
+    A task is long when it costs more than a quarter of the batch's cost per
+    resident warp.  Grouping the rest by measure keeps the instructions that
+    the SMs run at any one time to one measure's code: with the measures
+    interleaved, the persistent kernel stalls on instruction fetch."""
+    cost = np.asarray(cost, dtype=np.float64)
+    if cost.size == 0:
+        return np.zeros(0, np.int64)
+    lpt = np.argsort(-cost, kind="stable")
+    long = cost[lpt] > cost.sum() / max(int(warps), 1) / 4
+    rest = lpt[~long]
+    m = np.asarray(measure)[rest]
+    by_total = sorted(set(m.tolist()), key=lambda x: -cost[rest][m == x].sum())
+    return np.concatenate([lpt[long]] + [rest[m == x] for x in by_total])
 
 
 class PairsScheduler:
@@ -240,23 +268,23 @@ def save_cache(c: dict):
 
 def autotune(pts, off_a, len_a, off_b, len_b, measures, *, eps=0.0, gpoint=(0.0, 0.0), exact=False,
              candidates=CANDIDATES, reps=3, use_cache=True, len_a_host=None, len_b_host=None):
-    """Times each (rows, warp_floats) candidate on this batch; returns
-    (best (rows, warp_floats), {candidate: ms}).  Cached per GPU/signature."""
+    """Times each (rows, warp_floats, max_steps) candidate on this batch;
+    returns (best (rows, warp_floats, max_steps), {candidate: ms}).  Cached
+    per GPU/signature."""
     la = np.asarray(len_a_host if len_a_host is not None else len_a.cpu().numpy())
     lb = np.asarray(len_b_host if len_b_host is not None else len_b.cpu().numpy())
     gpu = torch.cuda.get_device_name(pts.device)
     key = f"{gpu}|{signature(la, lb, measures)}|{'exact' if exact else 'fast'}"
     cache = load_cache() if use_cache else {}
-    if key in cache:
-        r, w = cache[key]["best"]
-        return (int(r), int(w)), cache[key].get("ms", {})
+    if key in cache and len(cache[key].get("best", ())) == 3:
+        return tuple(int(x) for x in cache[key]["best"]), cache[key].get("ms", {})
     times = {}
     nc_max = int(np.minimum(la, lb).max(initial=0))
-    for rows, wf in candidates:
+    for rows, wf, mst in candidates:
         if any(measure_id(m) != _lib.HAUSDORFF for m in measures) and nc_max > wf:
             continue
         s = PairsScheduler(pts, off_a, len_a, off_b, len_b, measures, eps=eps, gpoint=gpoint, exact=exact,
-                           rows=rows, warp_floats=wf, len_a_host=la, len_b_host=lb)
+                           rows=rows, warp_floats=wf, max_steps=mst, len_a_host=la, len_b_host=lb)
         s.run()
         torch.cuda.synchronize(pts.device)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -265,12 +293,12 @@ def autotune(pts, off_a, len_a, off_b, len_b, measures, *, eps=0.0, gpoint=(0.0,
             s.run()
         ev[1].record()
         torch.cuda.synchronize(pts.device)
-        times[f"{rows},{wf}"] = ev[0].elapsed_time(ev[1]) / reps
+        times[f"{rows},{wf},{mst}"] = ev[0].elapsed_time(ev[1]) / reps
     if not times:
         raise ValueError("no candidate can hold these pairs")
     best = min(times, key=times.get)
-    r, w = (int(x) for x in best.split(","))
+    choice = tuple(int(x) for x in best.split(","))
     if use_cache:
-        cache[key] = {"best": [r, w], "ms": times}
+        cache[key] = {"best": list(choice), "ms": times}
         save_cache(cache)
-    return (r, w), times
+    return choice, times
