@@ -102,7 +102,7 @@ __device__ __forceinline__ void group_task(const PairsArgs& A, int first, int co
     const int nc = valid ? (a_rows ? nb : na) : 0;
     const float2* rowp = valid ? A.pts + (a_rows ? A.off_a[k] : A.off_b[k]) : A.pts;
     const float2* colp = valid ? A.pts + (a_rows ? A.off_b[k] : A.off_a[k]) : A.pts;
-    float* ring = ring_base + grp * cap;
+    float* const region = ring_base + grp * cap;
     float srow = 0.f, scol = 0.f;
     if constexpr (M == ERP) {
         if (valid && u == 0) {
@@ -113,16 +113,18 @@ __device__ __forceinline__ void group_task(const PairsArgs& A, int first, int co
         scol = __shfl_sync(kFull, scol, lane - u);
     }
     const bool live = valid && nr > 0 && nc > 0;  // no loads at all for an empty trajectory
-    if (live)
-        for (int j = u; j < nc; j += G) ring[j] = C::topb(scol, j);
-    // The column points go to shared memory after the ring (float2, 8-byte
-    // aligned) when every group of the warp has room for them: the step loop
-    // then reads them there instead of from global memory.
-    const int ring_len = (nc + 1) & ~1;
-    const bool staged = kGroupStageCols && __all_sync(kFull, !live || ring_len + 2 * nc <= cap);
-    float2* scols = reinterpret_cast<float2*>(ring + ring_len);
-    if (staged && live)
-        for (int j = u; j < nc; j += G) scols[j] = __ldg(colp + j);
+    // Shared-memory layout of a group's region (cap floats).  The column points
+    // are staged there (float2) when every group of the warp has room: the step
+    // loop then reads them from shared memory instead of global memory.  The
+    // groups' copies start 2*G*grp floats apart modulo 32 banks, so the warp's
+    // column loads (G consecutive points per group) take the minimum two
+    // wavefronts; the rings (one float per column, read by lane 0 and written
+    // by lane G-1 of every group at the same column) start grp floats further
+    // apart, so those accesses fall in distinct banks too.
+    const int col_skew = (2 * G * grp) & 31;
+    const bool staged = kGroupStageCols && __all_sync(kFull, !live || col_skew + 3 * nc + grp <= cap);
+    float2* scols = reinterpret_cast<float2*>(region + col_skew);
+    float* ring = staged ? region + col_skew + 2 * nc + grp : region + (nc + grp <= cap ? grp : 0);
     const int n_ss = live ? (nr + SS - 1) / SS : 0;
     const int max_ss = __reduce_max_sync(kFull, n_ss);
     const int max_span = __reduce_max_sync(kFull, live ? nc + G - 1 : 0);
@@ -135,6 +137,17 @@ __device__ __forceinline__ void group_task(const PairsArgs& A, int first, int co
         px[r] = q.x;
         py[r] = q.y;
     }
+    if (staged && live) {
+        // asynchronous 8-byte copies, all in flight at once (with the row
+        // loads above), then one wait
+        for (int j = u; j < nc; j += G) {
+            const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(scols + j));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(colp + j) : "memory");
+        }
+    }
+    if (live)
+        for (int j = u; j < nc; j += G) ring[j] = C::topb(scol, j);
+    if (staged && live) asm volatile("cp.async.wait_all;" ::: "memory");
     float dlast = 0.f;
     __syncwarp();
     auto sweep = [&](auto staged_tag) {

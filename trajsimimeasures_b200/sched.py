@@ -42,7 +42,7 @@ KIND_TILE, KIND_GROUP8, KIND_WAVE, KIND_HAUSDORFF, KIND_HAUSDORFF_WARP, KIND_GRO
 GROUP_KIND = {4: KIND_GROUP4, 8: KIND_GROUP8, 16: KIND_GROUP16, 32: KIND_WAVE}
 # A pair may keep its lanes for at most this many loop steps (one step = R
 # cells per lane) before the planner spreads it over more lanes.
-MAX_STEPS = 8192
+MAX_STEPS = 4096
 # Resident warps of a launch, for the task order when the caller gives none
 # (B200: 148 SMs x 12 warps at 16 KB of shared memory per warp).
 WARPS = 148 * 12
@@ -50,8 +50,8 @@ WARPS = 148 * 12
 # warp (the lanes split the points) instead of one per lane.
 HAUSDORFF_WARP_UNITS = 1 << 17
 # (rows per strip, shared-memory floats per warp, step budget) tried by the autotuner
-CANDIDATES = [(8, 4096, 8192), (8, 4096, 16384), (8, 3072, 8192), (8, 2048, 8192), (8, 8192, 8192),
-              (4, 4096, 8192)]
+CANDIDATES = [(8, 3072, 4096), (8, 3072, 2048), (8, 4096, 4096), (8, 4096, 8192), (8, 2048, 4096),
+              (8, 8192, 4096), (4, 4096, 4096)]
 
 
 def group_steps(nr, nc, rows, G):
