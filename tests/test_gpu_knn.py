@@ -73,3 +73,33 @@ def test_select_rows_is_the_stable_argsort_set(k):
         assert set(i[r].tolist()) == set(want[r].tolist())
     short = select_rows(torch.from_numpy(a[:, :50].copy()).cuda(), 60).cpu().numpy()
     assert (short[:, 50:] == -1).all() and all(set(row[:50]) == set(range(50)) for row in short)
+
+
+@pytest.mark.parametrize("k", [1, 64, 5000, 20000])
+def test_select_rows_sampled_threshold_and_fallbacks(k):
+    """Long rows (the sampled-threshold path, its radix fallback for large k),
+    a row whose k-th value repeats more often than the tie buffer holds, a row
+    of one value, negative values, +-inf and NaN: always the stable argsort's
+    first-k set."""
+    from trajsimimeasures_b200.knn import select_rows
+    rng = np.random.default_rng(100 + k)
+    n = 300_000
+    a = rng.standard_normal((6, n)).astype(np.float32)
+    a[1] = np.abs(a[1])
+    a[2, rng.choice(n, 5000, replace=False)] = np.nan
+    a[2, :3] = -np.inf
+    a[2, 3:6] = np.inf
+    srt = np.sort(a[3])
+    a[3, rng.choice(n, 3000, replace=False)] = srt[min(k, n - 1)]  # > 1024 ties at the cut
+    a[4] = 0.5
+    a[5] = np.round(a[5], 2)  # heavy ties everywhere
+    i = select_rows(torch.from_numpy(a).cuda(), k).cpu().numpy()
+    want = np.argsort(a, axis=1, kind="stable")[:, :k]
+    for r in range(a.shape[0]):
+        assert set(i[r].tolist()) == set(want[r].tolist()), r
+    # rows that fit the shared-memory buffer whole
+    b = np.round(rng.random((3, 10_000)), 3).astype(np.float32)
+    j = select_rows(torch.from_numpy(b).cuda(), min(k, 10_000)).cpu().numpy()
+    wb = np.argsort(b, axis=1, kind="stable")[:, :min(k, 10_000)]
+    for r in range(b.shape[0]):
+        assert set(j[r].tolist()) == set(wb[r].tolist()), r

@@ -335,9 +335,11 @@ int tsm_select_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, 
     if (n_rows > 0x7fffffffLL || n_cols > 0x7fffffffLL) return fail(TSM_EINVAL, "tsm_select_rows: too large");
     if (!d || !out_idx) return fail(TSM_EINVAL, "tsm_select_rows: null pointer");
     if (ld < n_cols) return fail(TSM_EINVAL, "tsm_select_rows: ld < n_cols");
-    tsm::select_rows_kernel<<<(unsigned)n_rows, tsm::kTopkThreads, 0, (cudaStream_t)stream>>>(d, n_cols, ld, k,
-                                                                                                out_idx);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = set_smem((const void*)&tsm::select_rows_kernel, (int)tsm::kSelSmemBytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    tsm::select_rows_kernel<<<(unsigned)n_rows, tsm::kTopkThreads, tsm::kSelSmemBytes, (cudaStream_t)stream>>>(
+        d, n_cols, ld, k, out_idx);
+    e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "select_rows_kernel launch");
     return TSM_OK;
 }

@@ -10,8 +10,9 @@ its GPU refinement bridge Traj::TrajSimiGPU is broken as shipped).  Here:
   and selecting with the top-k kernel (tsm_topk_rows); per chunk the k best
   are kept, then merged.
 * ``knn_rerank``: exact top-k among given candidates (e.g. a learned filter's
-  top-200): the candidate pairs are evaluated with the paired kernel and the
-  best k selected.  ``recall_at_k`` compares two answers.
+  top-200): the candidate pairs are evaluated with the paired kernel, in an
+  order of equal loop shapes computed on the device, and the best k
+  selected.  ``recall_at_k`` compares two answers.
 """
 from __future__ import annotations
 
@@ -21,7 +22,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .engine import TrajSet, _ptr, _stream_ptr, matrix_raw, measure_id, pairs_raw
+from .engine import DEFAULT_ROWS, TrajSet, _ptr, _stream_ptr, matrix_raw, measure_id, pairs_raw
 
 
 def topk_rows(d: torch.Tensor, k: int, stream=None):
@@ -89,13 +90,23 @@ def knn_rerank(Q: TrajSet, D: TrajSet, cand: torch.Tensor, k=10, measure="dtw", 
     off_b, len_b = D.off[di], D.lens[di]
     out = torch.empty(nq * c, dtype=torch.float32, device=Q.device)
     pairs_raw(m, pool, off_a, len_a, off_b, len_b, max(Q.max_len, D.max_len), out=out, eps=eps, gpoint=gpoint,
-              exact=exact, stream=stream)
+              exact=exact, stream=stream, order=shape_order(len_a, len_b))
     # ties to the smaller database index, as in knn_exhaustive
     o = torch.argsort(cand, dim=1)
     dd = torch.gather(out.view(nq, c), 1, o).contiguous()
     ci = torch.gather(cand, 1, o)
     v, j = topk_rows(dd, k, stream=stream)
     return v, torch.gather(ci, 1, j.long())
+
+
+def shape_order(len_a: torch.Tensor, len_b: torch.Tensor, rows=DEFAULT_ROWS) -> torch.Tensor:
+    """engine.pair_order on the device: the pairs ordered by (row blocks,
+    columns) of their DP, so a warp's 32 lanes run loops of equal trip counts
+    (int32 processing order for tsm_pairs)."""
+    la, lb = len_a.long(), len_b.long()
+    nr, nc = torch.maximum(la, lb), torch.minimum(la, lb)
+    key = ((nr + rows - 1) // rows) * 65536 + nc
+    return torch.argsort(key, stable=True).to(torch.int32)
 
 
 def recall_at_k(approx_idx, exact_idx) -> float:
@@ -121,7 +132,8 @@ def select_rows(d: torch.Tensor, k: int, stream=None) -> torch.Tensor:
 class SurrogateIndex:
     """Database embeddings of a trained encoder, used to pick kNN candidates:
     the c database trajectories nearest to a query in embedding space
-    (squared L2 via one matrix product), then reranked by exact DP.
+    (squared L2 via one TF32 matrix product with the squared norms folded in,
+    then the sampled-threshold selection kernel), then reranked by exact DP.
 
     The candidate count is calibrated, not guessed: ``calibrate`` runs the
     exhaustive search on a sample of queries and takes the smallest count of
@@ -130,20 +142,50 @@ class SurrogateIndex:
 
     LADDER = (200, 500, 1000, 2000, 5000, 10000, 20000, 50000)
 
+    # embedding width + 1 (the squared norm), padded to a multiple of 4 floats
+    AUG = 132
+
     def __init__(self, encoder, D: TrajSet, batch=4096):
         self.enc = encoder
         self.D = D
-        self.emb = encoder.embed(D, batch=batch)
-        self.sqn = (self.emb * self.emb).sum(1)
+        emb = encoder.embed(D, batch=batch)
+        w = emb.shape[1]
+        # augmented rows [e_j, |e_j|^2, 0...]: one product with [-2 e_q, 1, 0...]
+        # gives |e_j|^2 - 2 e_q.e_j, the squared distance less the query's own
+        # |e_q|^2, which does not change a query's ranking
+        self.aug = torch.zeros((emb.shape[0], max(self.AUG, (w + 4) // 4 * 4)), dtype=torch.float32,
+                               device=emb.device)
+        self.aug[:, :w] = emb
+        self.aug[:, w] = (emb * emb).sum(1)
+        self.width = w
         self.c = None
+
+    @property
+    def emb(self) -> torch.Tensor:
+        """Database embeddings [n, width] (a view of the augmented rows)."""
+        return self.aug[:, :self.width]
+
+    def scan(self, e: torch.Tensor) -> torch.Tensor:
+        """Embedding-space distances (less |e_q|^2) of queries e [b, width] to
+        every database trajectory: one TF32 tensor-core product, FP32
+        accumulation and output ([b, n] float32)."""
+        q = torch.zeros((e.shape[0], self.aug.shape[1]), dtype=torch.float32, device=e.device)
+        q[:, :self.width] = -2.0 * e
+        q[:, self.width] = 1.0
+        mm = torch.backends.cuda.matmul
+        prev = mm.allow_tf32
+        mm.allow_tf32 = True
+        try:
+            return q @ self.aug.T
+        finally:
+            mm.allow_tf32 = prev
 
     def candidates(self, Q: TrajSet, c: int, chunk=256) -> torch.Tensor:
         eq = self.enc.embed(Q)
         out = torch.empty((Q.n, c), dtype=torch.int64, device=Q.device)
         for q0 in range(0, Q.n, chunk):
-            e = eq[q0:q0 + chunk]
-            d = (e * e).sum(1, keepdim=True) + self.sqn[None, :] - 2.0 * (e @ self.emb.T)
-            out[q0:q0 + e.shape[0]] = select_rows(d.contiguous(), c).long()
+            d = self.scan(eq[q0:q0 + chunk])
+            out[q0:q0 + d.shape[0]] = select_rows(d, c).long()
         return out
 
     def query(self, Q: TrajSet, k=10, c=None, measure="dtw", **kw):
