@@ -98,6 +98,23 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
               void* stream);
 
 /*
+ * Per-query candidate lists (the refinement step of a kNN query):
+ *   out[i*ld_out + s] = measure(Q_i, D_{cand[i*ncand + s]}),  i < nq, s < ncand.
+ * Replaces the exact refinement of filtered candidates in the reference's kNN
+ * queries (query/cpp/DITA.cpp:276-431, DFT.cpp:89-230, which evaluate the
+ * measure on each surviving candidate; and its GPU bridge Traj::TrajSimiGPU,
+ * query/cpp/spatial/traj.cpp:242-360, which was meant to batch them).
+ *   cand int32 [nq][ncand]: database indices; a query's row is best sorted by
+ *        database length (neighbouring threads then get equal loop shapes);
+ *        an index outside 0..nd-1 gives NaN (count -1) for that entry
+ *   ld_out >= ncand; the other arguments as in tsm_matrix
+ */
+int tsm_matrix_gather(int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len, int64_t nq,
+                      int32_t q_max_len, const float* d_pts, const int64_t* d_off, const int32_t* d_len, int64_t nd,
+                      int32_t d_max_len, const int32_t* cand, int64_t ncand, const tsm_params* params, float* out,
+                      int64_t ld_out, int32_t* out_counts, void* stream);
+
+/*
  * All pairs of a query set Q and a database set D:
  *   out[i*ld_out + j] = measure(Q_i, D_j),  i < nq, j < nd.
  * Replaces the host-side Q x D pair expansion + batched core.<measure> calls of
@@ -138,12 +155,13 @@ int tsm_allpairs_sym(int measure, const float* pts, const int64_t* off, const in
  * for batches of very uneven lengths and several measures at once.
  *   tasks      device int32 [n_tasks][4] = {kind, measure, first, count}:
  *              pairs order[first .. first+count) as one warp task; kind 0 =
- *              one pair per lane, 1 = one pair per 8 lanes, 2 = one pair per
- *              warp, 3 = Hausdorff one pair per lane, 4 = Hausdorff one pair
- *              per warp.  Sorted by the caller, largest first.
- *   warp_smem_floats  shared memory per warp (floats): the tile capacity is
- *              warp_smem_floats/32 columns, the 8-lane capacity /4, the
- *              one-warp capacity warp_smem_floats; tasks must respect them
+ *              one pair per lane, 5 / 1 / 6 / 2 = one pair per 4 / 8 / 16 /
+ *              32 lanes, 3 = Hausdorff one pair per lane, 4 = Hausdorff one
+ *              pair per warp.  Warps take the tasks in this order.
+ *   warp_smem_floats  shared memory per warp (floats), a multiple of 32: a
+ *              pair's shorter side may be up to warp_smem_floats/32 columns
+ *              in kind 0 and warp_smem_floats*G/32 in a G-lane kind; a pair
+ *              beyond its kind's capacity gets NaN (count -1)
  *   out        float32 [n_measures_used][out_stride]: out[measure*out_stride + pair]
  *   out_counts int32, same layout (EDR/LCSS), or NULL
  *   workspace  device memory of tsm_sched_workspace_bytes() bytes, zeroed

@@ -103,3 +103,35 @@ def test_select_rows_sampled_threshold_and_fallbacks(k):
     wb = np.argsort(b, axis=1, kind="stable")[:, :min(k, 10_000)]
     for r in range(b.shape[0]):
         assert set(j[r].tolist()) == set(wb[r].tolist()), r
+
+
+@pytest.mark.parametrize("measure", ["dtw", "edr", "lcss", "erp", "dfrechet", "hausdorff"])
+def test_matrix_gather_equals_matrix_entries(measure):
+    """tsm_matrix_gather (per-query candidate rows) is bit-identical to the
+    full matrix at the gathered entries, counts included; indices outside the
+    database give NaN and count -1."""
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.engine import TrajSet, matrix, matrix_gather_raw, measure_id
+    dev = torch.device("cuda", 0)
+    Q = TrajSet.from_packed(*D.trajectory_set(37, seed=5), device=dev)
+    Dset = TrajSet.from_packed(*D.trajectory_set(500, 1, 230, seed=6), device=dev)
+    kw = dict(eps=D.EPS_DEG, gpoint=D.BOX_CENTRE, exact=True)
+    full, fcnt = matrix(measure, Q, Dset, with_counts=True, **kw)
+    rng = np.random.default_rng(7)
+    cand = rng.integers(0, 500, (37, 301)).astype(np.int32)
+    cand[3, 5] = -1
+    cand[4, 7] = 500
+    c = torch.from_numpy(cand).to(dev)
+    out = torch.full((37, 320), -5.0, device=dev)
+    cnt = torch.full((37, 320), -5, dtype=torch.int32, device=dev)
+    matrix_gather_raw(measure, Q, Dset, c, out=out, counts=cnt, **kw)
+    o, k = out.cpu().numpy(), cnt.cpu().numpy()
+    f, fc = full.cpu().numpy(), fcnt.cpu().numpy()
+    ok = (cand >= 0) & (cand < 500)
+    qi = np.broadcast_to(np.arange(37)[:, None], cand.shape)
+    np.testing.assert_array_equal(o[:, :301][ok], f[qi[ok], cand[ok]])
+    assert np.isnan(o[3, 5]) and np.isnan(o[4, 7])
+    assert (o[:, 301:] == -5.0).all()  # nothing past ncand is written
+    if measure_id(measure) in (1, 2):
+        np.testing.assert_array_equal(k[:, :301][ok], fc[qi[ok], cand[ok]])
+        assert k[3, 5] == -1 and k[4, 7] == -1

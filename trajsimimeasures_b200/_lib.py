@@ -22,7 +22,7 @@ FLAG_EXACT = 1
 EXPORTS = ("tsm_version", "tsm_last_error", "tsm_max_supported_len", "tsm_pairs", "tsm_matrix",
            "tsm_sched_workspace_bytes", "tsm_pairs_sched", "tsm_topk_rows", "tsm_pairs_sched_noalloc",
            "tsm_enc_param_count", "tsm_enc_workspace_bytes", "tsm_enc_forward", "tsm_enc_loss_grad", "tsm_enc_adam",
-           "tsm_select_rows", "tsm_allpairs_sym")
+           "tsm_select_rows", "tsm_allpairs_sym", "tsm_matrix_gather")
 
 
 class TsmParams(ctypes.Structure):
@@ -61,6 +61,9 @@ def load():
         lib.tsm_matrix.restype = ctypes.c_int
         lib.tsm_matrix.argtypes = [ctypes.c_int, _vp, _vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _i64, _i32,
                                    ctypes.POINTER(TsmParams), _vp, _i64, _vp, _vp]
+        lib.tsm_matrix_gather.restype = ctypes.c_int
+        lib.tsm_matrix_gather.argtypes = [ctypes.c_int, _vp, _vp, _vp, _i64, _i32, _vp, _vp, _vp, _i64, _i32, _vp, _i64,
+                                          ctypes.POINTER(TsmParams), _vp, _i64, _vp, _vp]
         lib.tsm_allpairs_sym.restype = ctypes.c_int
         lib.tsm_allpairs_sym.argtypes = [ctypes.c_int, _vp, _vp, _vp, _vp, _i64, _i32, ctypes.POINTER(TsmParams), _vp,
                                          _i64, _vp, _vp]

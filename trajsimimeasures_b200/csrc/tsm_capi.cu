@@ -233,12 +233,14 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
 
 namespace {
 
-// One matrix launch: Q x D (q_order == nullptr, sym == 0), or the symmetric
-// upper triangle of one set in its length order (q_order == d_order, sym == 1).
+// One matrix launch: Q x D (q_order == nullptr, sym == 0), the symmetric
+// upper triangle of one set in its length order (q_order == d_order, sym ==
+// 1), or per-query candidate rows (d_order [nq][nd], sym == 2).  d_total: the
+// number of database trajectories (indices from d_order are checked against it).
 int matrix_launch(const char* who, int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len,
                   const int32_t* q_order, int64_t nq, int32_t q_max_len, const float* d_pts, const int64_t* d_off,
-                  const int32_t* d_len, const int32_t* d_order, int64_t nd, int32_t d_max_len, int sym,
-                  const tsm_params* params, float* out, int64_t ld_out, int32_t* out_counts, void* stream) {
+                  const int32_t* d_len, const int32_t* d_order, int64_t nd, int64_t d_total, int32_t d_max_len,
+                  int sym, const tsm_params* params, float* out, int64_t ld_out, int32_t* out_counts, void* stream) {
     const int R = rows_of(params, measure);
     const bool exact = exact_of(params);
     cudaStream_t s = (cudaStream_t)stream;
@@ -247,7 +249,7 @@ int matrix_launch(const char* who, int measure, const float* q_pts, const int64_
     const float2* d2 = reinterpret_cast<const float2*>(d_pts);
     int qcap = q_max_len < 1 ? 1 : q_max_len;
     int dml = d_max_len;
-    int64_t ndd = nd, ld = ld_out;
+    int64_t ndd = nd, ld = ld_out, dtot = d_total;
     if (measure == TSM_HAUSDORFF) {
         const void* fn = pick_haus(true, R, exact);
         if (!fn) return fail(TSM_EINVAL, "%s: rows_per_thread must be 4, 8 or 16", who);
@@ -257,8 +259,8 @@ int matrix_launch(const char* who, int measure, const float* q_pts, const int64_
         int chunks = (int)((nd + threads - 1) / threads);
         if ((int64_t)chunks * nq > 0x7fffffffLL) return fail(TSM_EINVAL, "%s: grid too large", who);
         dim3 grid((unsigned)(chunks * nq));
-        void* args[] = {&q2,  &q_off, &q_len, &q_order, &d2,  &d_off, &d_len, &d_order,
-                        &ndd, &chunks, &sym,  &qcap,    &dml, &out,   &ld};
+        void* args[] = {&q2,   &q_off,  &q_len, &q_order, &d2,  &d_off, &d_len, &d_order,
+                        &ndd,  &dtot,   &chunks, &sym,    &qcap, &dml,  &out,   &ld};
         return launch(fn, grid, dim3(threads), smem, args, s);
     }
     if (q_max_len > kMatrixQueryMax)
@@ -272,8 +274,8 @@ int matrix_launch(const char* who, int measure, const float* q_pts, const int64_
     int chunks = (int)((nd + threads - 1) / threads);
     if ((int64_t)chunks * nq > 0x7fffffffLL) return fail(TSM_EINVAL, "%s: grid too large", who);
     dim3 grid((unsigned)(chunks * nq));
-    void* args[] = {&q2,   &q_off, &q_len, &q_order,   &d2,  &d_off, &d_len, &d_order, &ndd,
-                    &chunks, &sym, &qcap,  &dml, (void*)&kp, &out, &ld,   &out_counts};
+    void* args[] = {&q2,     &q_off, &q_len, &q_order, &d2,        &d_off, &d_len, &d_order, &ndd,
+                    &dtot,   &chunks, &sym,  &qcap,    &dml,       (void*)&kp, &out, &ld,     &out_counts};
     return launch(fn, grid, dim3(threads), smem, args, s);
 }
 
@@ -292,7 +294,24 @@ int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int3
     if (ld_out < nd) return fail(TSM_EINVAL, "tsm_matrix: ld_out < nd");
     if (q_max_len < 0 || d_max_len < 0) return fail(TSM_EINVAL, "tsm_matrix: max_len < 0");
     return matrix_launch("tsm_matrix", measure, q_pts, q_off, q_len, nullptr, nq, q_max_len, d_pts, d_off, d_len,
-                         d_order, nd, d_max_len, 0, params, out, ld_out, out_counts, stream);
+                         d_order, nd, nd, d_max_len, 0, params, out, ld_out, out_counts, stream);
+}
+
+int tsm_matrix_gather(int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len, int64_t nq,
+                      int32_t q_max_len, const float* d_pts, const int64_t* d_off, const int32_t* d_len, int64_t nd,
+                      int32_t d_max_len, const int32_t* cand, int64_t ncand, const tsm_params* params, float* out,
+                      int64_t ld_out, int32_t* out_counts, void* stream) {
+    g_err.clear();
+    if (measure < TSM_DTW || measure > TSM_HAUSDORFF)
+        return fail(TSM_EINVAL, "tsm_matrix_gather: unknown measure %d", measure);
+    if (nq < 0 || nd < 0 || ncand < 0) return fail(TSM_EINVAL, "tsm_matrix_gather: negative size");
+    if (nq == 0 || ncand == 0) return TSM_OK;
+    if (!q_pts || !q_off || !q_len || !d_pts || !d_off || !d_len || !cand || !out)
+        return fail(TSM_EINVAL, "tsm_matrix_gather: null pointer");
+    if (ld_out < ncand) return fail(TSM_EINVAL, "tsm_matrix_gather: ld_out < ncand");
+    if (q_max_len < 0 || d_max_len < 0) return fail(TSM_EINVAL, "tsm_matrix_gather: max_len < 0");
+    return matrix_launch("tsm_matrix_gather", measure, q_pts, q_off, q_len, nullptr, nq, q_max_len, d_pts, d_off,
+                         d_len, cand, ncand, nd, d_max_len, 2, params, out, ld_out, out_counts, stream);
 }
 
 int tsm_allpairs_sym(int measure, const float* pts, const int64_t* off, const int32_t* len, const int32_t* order,
@@ -307,7 +326,7 @@ int tsm_allpairs_sym(int measure, const float* pts, const int64_t* off, const in
     if (ld_out < n) return fail(TSM_EINVAL, "tsm_allpairs_sym: ld_out < n");
     if (max_len < 0) return fail(TSM_EINVAL, "tsm_allpairs_sym: max_len < 0");
     return matrix_launch("tsm_allpairs_sym", measure, pts, off, len, order, n, max_len, pts, off, len, order, n,
-                         max_len, 1, params, out, ld_out, out_counts, stream);
+                         n, max_len, 1, params, out, ld_out, out_counts, stream);
 }
 
 int tsm_topk_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, int32_t k, float* out_d,

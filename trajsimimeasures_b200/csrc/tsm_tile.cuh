@@ -395,25 +395,28 @@ __global__ void __launch_bounds__(128) dp_pairs_kernel(
 // Matrix mode -----------------------------------------------------------------
 // grid.x = nq * chunks; CTA (s, chunk) computes out[i, d_order[chunk*blockDim + t]]
 // for the query i = q_order[s] (i = s without an order).
-// Symmetric mode (sym != 0; the query set is the database set and q_order ==
+// Symmetric mode (sym == 1; the query set is the database set and q_order ==
 // d_order): only the slots at or after the query's own sorted position s are
 // computed (the upper triangle in sorted order), and each value is written to
 // out[i, j] and out[j, i]; CTAs wholly below the diagonal exit at once.
+// Gather mode (sym == 2): d_order holds one row of nd database indices per
+// query, and slot t of query i goes to out[i, t].  A database index outside
+// 0..d_total-1 gives NaN (count -1).
 // Dynamic shared memory = cap float4 columns + W*32*cap floats.
 
 template <int M, int R, bool EXACT>
 __global__ void __launch_bounds__(128) dp_matrix_kernel(
     const float2* __restrict__ q_pts, const int64_t* __restrict__ q_off, const int32_t* __restrict__ q_len,
     const int32_t* __restrict__ q_order, const float2* __restrict__ d_pts, const int64_t* __restrict__ d_off,
-    const int32_t* __restrict__ d_len, const int32_t* __restrict__ d_order, int64_t nd, int chunks, int sym,
-    int cap, int d_max_len, KParams p, float* __restrict__ out, int64_t ld, int32_t* __restrict__ counts) {
+    const int32_t* __restrict__ d_len, const int32_t* __restrict__ d_order, int64_t nd, int64_t d_total, int chunks,
+    int sym, int cap, int d_max_len, KParams p, float* __restrict__ out, int64_t ld, int32_t* __restrict__ counts) {
     extern __shared__ float smem[];
     __shared__ float s_scol;
     float4* cols = reinterpret_cast<float4*>(smem);
     float* buf = smem + 4 * cap + (threadIdx.x >> 5) * (32 * cap) + (threadIdx.x & 31);
     const int64_t qs = blockIdx.x / chunks;
     const int chunk = blockIdx.x % chunks;
-    if (sym && (int64_t)(chunk + 1) * blockDim.x <= qs) return;  // below the diagonal (uniform per CTA)
+    if (sym == 1 && (int64_t)(chunk + 1) * blockDim.x <= qs) return;  // below the diagonal (uniform per CTA)
     const int64_t qi = q_order ? (int64_t)q_order[qs] : qs;
     const int nq = q_len[qi];
     const bool qbad = nq < 0 || nq > cap;
@@ -434,13 +437,14 @@ __global__ void __launch_bounds__(128) dp_matrix_kernel(
         __syncthreads();
     }
     const int64_t slot = (int64_t)chunk * blockDim.x + threadIdx.x;
-    if (slot >= nd || (sym && slot < qs)) return;
-    const int64_t dj = d_order ? (int64_t)d_order[slot] : slot;
-    const int ndl = d_len[dj];
+    if (slot >= nd || (sym == 1 && slot < qs)) return;
+    const int64_t dj = d_order ? (int64_t)d_order[(sym == 2 ? qs * nd : 0) + slot] : slot;
+    const bool dbad = dj < 0 || dj >= d_total;
+    const int ndl = dbad ? -1 : d_len[dj];
     const bool count = (M == EDR || M == LCSS) && counts != nullptr;
-    const int64_t o_idx = qi * ld + dj, t_idx = dj * ld + qi;
-    const bool mirror = sym && dj != qi;
-    if (qbad || ndl < 0 || ndl > d_max_len) {
+    const int64_t o_idx = qi * ld + (sym == 2 ? slot : dj), t_idx = dj * ld + qi;
+    const bool mirror = sym == 1 && dj != qi;
+    if (qbad || dbad || ndl < 0 || ndl > d_max_len) {
         out[o_idx] = CUDART_NAN_F;
         if (count) counts[o_idx] = -1;
         if (mirror) {
@@ -630,15 +634,15 @@ struct StagedNegPts {
 };
 
 // Matrix kernel: CTA (s, chunk) stages query i's segment pairs in shared
-// memory once; each thread takes one database trajectory.  Query order and
-// symmetric mode as in dp_matrix_kernel.  Dynamic shared memory =
+// memory once; each thread takes one database trajectory.  Query order,
+// symmetric and gather modes as in dp_matrix_kernel.  Dynamic shared memory =
 // ceil(q_max_len/2) * 40 bytes.
 template <int R, bool EXACT>
 __global__ void __launch_bounds__(128) hausdorff_matrix_kernel(
     const float2* __restrict__ q_pts, const int64_t* __restrict__ q_off, const int32_t* __restrict__ q_len,
     const int32_t* __restrict__ q_order, const float2* __restrict__ d_pts, const int64_t* __restrict__ d_off,
-    const int32_t* __restrict__ d_len, const int32_t* __restrict__ d_order, int64_t nd, int chunks, int sym,
-    int q_max_len, int d_max_len, float* __restrict__ out, int64_t ld) {
+    const int32_t* __restrict__ d_len, const int32_t* __restrict__ d_order, int64_t nd, int64_t d_total, int chunks,
+    int sym, int q_max_len, int d_max_len, float* __restrict__ out, int64_t ld) {
     extern __shared__ float4 smem4[];
     const int cap_pairs = (q_max_len + 1) >> 1;
     float4* A = smem4;
@@ -646,7 +650,7 @@ __global__ void __launch_bounds__(128) hausdorff_matrix_kernel(
     float2* C = reinterpret_cast<float2*>(smem4 + 2 * cap_pairs);
     const int64_t qs = blockIdx.x / chunks;
     const int chunk = blockIdx.x % chunks;
-    if (sym && (int64_t)(chunk + 1) * blockDim.x <= qs) return;
+    if (sym == 1 && (int64_t)(chunk + 1) * blockDim.x <= qs) return;
     const int64_t qi = q_order ? (int64_t)q_order[qs] : qs;
     const int nq = q_len[qi];
     const bool qbad = nq < 0 || nq > q_max_len;
@@ -665,13 +669,14 @@ __global__ void __launch_bounds__(128) hausdorff_matrix_kernel(
     }
     __syncthreads();
     const int64_t slot = (int64_t)chunk * blockDim.x + threadIdx.x;
-    if (slot >= nd || (sym && slot < qs)) return;
-    const int64_t dj = d_order ? (int64_t)d_order[slot] : slot;
-    const int ndl = d_len[dj];
-    const int64_t o_idx = qi * ld + dj;
-    const bool mirror = sym && dj != qi;
+    if (slot >= nd || (sym == 1 && slot < qs)) return;
+    const int64_t dj = d_order ? (int64_t)d_order[(sym == 2 ? qs * nd : 0) + slot] : slot;
+    const bool dbad = dj < 0 || dj >= d_total;
+    const int ndl = dbad ? -1 : d_len[dj];
+    const int64_t o_idx = qi * ld + (sym == 2 ? slot : dj);
+    const bool mirror = sym == 1 && dj != qi;
     float v = CUDART_NAN_F;
-    if (!(qbad || ndl < 0 || ndl > d_max_len)) {
+    if (!(qbad || dbad || ndl < 0 || ndl > d_max_len)) {
         const float2* dp = d_pts + d_off[dj];
         const float m1 = directed_max_staged2<R>(dp, ndl, A, B, C, nq);
         const float m2 = directed_max2<R, EXACT>(StagedNegPts{A}, nq, dp, ndl);

@@ -170,6 +170,25 @@ def matrix_raw(measure, q: TrajSet, d: TrajSet, *, out, counts=None, d_order=Non
     return out
 
 
+MATRIX_QUERY_MAX = 1400  # longest query of the matrix forms (kMatrixQueryMax in the library)
+
+
+def matrix_gather_raw(measure, q: TrajSet, d: TrajSet, cand: torch.Tensor, *, out, counts=None, eps=0.0,
+                      gpoint=(0.0, 0.0), exact=False, rows=0, stream=None):
+    """tsm_matrix_gather: out[i, s] = measure(Q_i, D_cand[i, s]) for an int32
+    candidate matrix cand [nq, c] on the device (no copies, no sync)."""
+    m = measure_id(measure)
+    lib = _lib.load()
+    p = _lib.params(eps, gpoint, exact, rows)
+    if cand.dtype != torch.int32 or cand.dim() != 2 or not cand.is_contiguous():
+        raise ValueError("cand must be a contiguous int32 [nq, c] tensor")
+    rc = lib.tsm_matrix_gather(m, _ptr(q.pts), _ptr(q.off), _ptr(q.lens), q.n, q.max_len, _ptr(d.pts), _ptr(d.off),
+                               _ptr(d.lens), d.n, d.max_len, _ptr(cand), int(cand.shape[1]), ctypes.byref(p),
+                               _ptr(out), int(out.stride(0)), _ptr(counts), _stream_ptr(stream))
+    _lib.check(rc, "tsm_matrix_gather")
+    return out
+
+
 def allpairs_sym_raw(measure, s: TrajSet, *, out, counts=None, eps=0.0, gpoint=(0.0, 0.0), exact=False, rows=0,
                      stream=None):
     """tsm_allpairs_sym on a device-resident set: the full symmetric n x n
