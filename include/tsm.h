@@ -235,6 +235,17 @@ int64_t tsm_enc_workspace_bytes(int32_t B, int32_t T, int32_t P);
 /* emb float32 [B][128] (device) */
 int tsm_enc_forward(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
                     int32_t T, const float* nrm, void* workspace, float* emb, void* stream);
+/* Inference-only forward on the tensor cores (tcgen05): 128 trajectories per
+ * CTA, each GRU step one set of BF16 x BF16 -> FP32 MMAs into tensor memory,
+ * with a_t and h_t entering the products as BF16 (the training forward above
+ * keeps them FP32), and no training caches.  Used to embed the kNN database
+ * and the queries: the test-time embedding of the reference's learned
+ * measures (nn/MLP_trajsimi_train.py).  emb float32 [B][128] (device);
+ * workspace of tsm_enc_embed_workspace_bytes(B, T) bytes.  Batches of similar
+ * lengths waste fewer steps (a CTA runs its longest trajectory's length). */
+int64_t tsm_enc_embed_workspace_bytes(int32_t B, int32_t T);
+int tsm_enc_embed(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
+                  int32_t T, const float* nrm, void* workspace, float* emb, void* stream);
 /* Forward + pair loss + backward.  Pairs (ia[p], ib[p]) index the batch,
  * y[p] the target distances; loss = mean_p (||e_ia - e_ib|| - y)^2.
  * grad float32 [param_count] (overwritten), loss float32 [1], pred [P]

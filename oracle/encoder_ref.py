@@ -37,7 +37,13 @@ def unpack(params: np.ndarray):
     return out
 
 
-def embed(W, trajs, nrm):
+def _bf16(x):
+    return x.to(torch.float32).to(torch.bfloat16).to(torch.float64)
+
+
+def embed(W, trajs, nrm, bf16_operands=False):
+    """bf16_operands: a_t and h_t enter the gate products rounded to BF16, as
+    in the tensor-core inference kernel (tsm_enc_embed)."""
     embs = []
     mean = torch.tensor([nrm[0], nrm[1]], dtype=torch.float64)
     inv = torch.tensor([nrm[2], nrm[3]], dtype=torch.float64)
@@ -48,8 +54,9 @@ def embed(W, trajs, nrm):
         if n > 0:
             a = torch.relu(torch.nn.functional.conv1d(x.T[None], W["conv_w"], W["conv_b"], padding=2))[0].T  # [n, 64]
             for s in range(n):
-                gi = W["w_ih"] @ a[s] + W["b_ih"]
-                gh = W["w_hh"] @ h + W["b_hh"]
+                ai, hi = (_bf16(a[s]), _bf16(h)) if bf16_operands else (a[s], h)
+                gi = W["w_ih"] @ ai + W["b_ih"]
+                gh = W["w_hh"] @ hi + W["b_hh"]
                 r = torch.sigmoid(gi[:128] + gh[:128])
                 z = torch.sigmoid(gi[128:256] + gh[128:256])
                 nn_ = torch.tanh(gi[256:] + r * gh[256:])

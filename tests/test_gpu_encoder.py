@@ -51,10 +51,38 @@ def test_encoder_forward_long_batch():
     trajs = D.unpack(pts, off, lens)
     s = _set(trajs)
     enc = Encoder.init(s, seed=6)
-    e = enc.embed(s, batch=24).cpu().numpy()  # two batches (16 + 24 trajectories per GRU CTA tiles)
+    e = enc.embed(s, batch=24, tensor_cores=False).cpu().numpy()  # two batches (16 trajectories per GRU CTA)
     W = R.unpack(enc.params.cpu().numpy())
     e_ref = R.embed(W, trajs[:6], enc.nrm).detach().numpy()
     np.testing.assert_allclose(e[:6], e_ref, rtol=1e-4, atol=1e-5)
+
+
+def test_tensor_core_embedding_matches_bf16_operand_reference():
+    """The tcgen05 inference kernel (tsm_enc_embed): against the FP64
+    reference with a_t and h_t rounded to BF16 before the gate products, and
+    against the FP32-activation training forward, over three 128-trajectory
+    CTAs of lengths 1..230 (the last one partly filled)."""
+    from oracle import encoder_ref as R
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.surrogate import Encoder
+    rng = np.random.default_rng(11)
+    L = np.concatenate([[1, 2, 230], rng.integers(1, 231, 297)])
+    pts, off, lens = D._walks(rng, L, D.STEP_SIGMA)
+    trajs = D.unpack(pts, off, lens)
+    s = _set(trajs)
+    enc = Encoder.init(s, seed=12)
+    enc.params.mul_(2.0)  # gates away from their linear range
+    e_tc = enc.embed(s, batch=300).cpu().numpy()
+    e_fp = enc.embed(s, batch=300, tensor_cores=False).cpu().numpy()
+    assert np.isfinite(e_tc).all()
+    pick = [0, 1, 2, 3, 150, 299]
+    W = R.unpack(enc.params.cpu().numpy())
+    e_ref = R.embed(W, [trajs[i] for i in pick], enc.nrm, bf16_operands=True).detach().numpy()
+    scale = np.abs(e_ref).max()
+    err = np.abs(e_tc[pick] - e_ref).max() / scale
+    assert err <= 2e-3, err
+    # BF16 activations against FP32 ones: the same network to BF16 rounding
+    assert np.abs(e_tc - e_fp).max() <= 3e-2 * np.abs(e_fp).max()
 
 
 def test_training_learns_dtw_order():

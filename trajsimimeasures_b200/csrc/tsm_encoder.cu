@@ -11,11 +11,13 @@
 // The reference trains its learned measures the same way (MSE on
 // distance / max distance, nn/MLP_trajsimi_train.py:74-84,197-200).
 //
-// Kernels (all hand-written, SIMT FP32 FMA): at 16 trajectories per CTA the
-// GRU's per-step products are 16 x 384 x 192 multiply-adds, too small and too
-// serial (one step depends on the last) to fill tensor-core tiles; the GRU
-// kernels keep the BF16 weights resident in shared memory for all time steps
-// and step time inside the kernel.
+// Training kernels (hand-written, SIMT FP32 FMA): 16 trajectories per CTA,
+// the BF16 weights resident in shared memory for all time steps, time stepped
+// inside the kernel, FP32 activations, and the caches BPTT needs.  Inference
+// (embedding a database or a query batch) runs on the tensor cores instead:
+// enc_gru_embed_tc takes 128 trajectories per CTA, so each step's products
+// (128 x 384 x 192) are tcgen05 MMA tiles with the accumulators in tensor
+// memory.
 //
 //   enc_round_bf16    FP32 master -> BF16 weights
 //   enc_conv_fwd      conv + relu -> A [B][T][64]
@@ -27,12 +29,14 @@
 //   enc_gemm_tn       split-K reduction dW[m][n] += sum_k A[k][m] B[k][n]  (weight gradients)
 //   enc_conv_bwd      dW1, db1
 //   enc_adam          Adam step on the FP32 master weights
+//   enc_gru_embed_tc  inference GRU on the tensor cores -> last hidden state
 #include <cuda_bf16.h>
 #include <cstdio>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "tsm.h"
+#include "tsm_umma.cuh"
 
 int tsm_internal_fail(int code, const char* msg);
 
@@ -472,6 +476,213 @@ __global__ void enc_adam(float* __restrict__ p, const float* __restrict__ g, flo
     p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core GRU forward for inference (tcgen05).  CTA = 128 trajectories
+// (the MMA's M), 256 threads.  Per time step the operand X = [a_t | h_t]
+// (128 x 192 BF16, shared memory) is multiplied by the BF16 gate weights,
+// resident in shared memory for all steps, into three FP32 accumulators in
+// tensor memory (512 columns):
+//   columns   0..255  r and z pre-activations  X [Wih_rz | Whh_rz]^T  (K = 192)
+//   columns 256..383  Win a_t                   a_t Wih_n^T            (K = 64)
+//   columns 384..511  Whn h_t                   h_t Whh_n^T            (K = 128)
+// (n needs Whn h apart from Win a: r multiplies only the hidden part.)  One
+// thread issues the 24 MMAs and commits them to an mbarrier; then warp w reads
+// lanes 32 (w % 4) .. +31 (its 32 trajectories) and hidden units
+// 64 (w / 4) .. +63, applies the gates with the biases in FP32, keeps h in FP32
+// registers and writes it back to X as BF16 for the next step.  a_t and h_t
+// enter the products as BF16 (the SIMT training kernel multiplies FP32 a and
+// h by the BF16 weights), so the embeddings agree with it to BF16 rounding of
+// the activations.
+constexpr int TC_M = 128;
+constexpr int TC_THREADS = 256;
+constexpr int TC_K = C1 + HD;                               // 192
+constexpr int TC_OFF_X = 0;                                 // X     [128][192] BF16
+constexpr int TC_OFF_WRZ = TC_OFF_X + TC_M * TC_K * 2;      // W_rz  [256][192] BF16
+constexpr int TC_OFF_WIN = TC_OFF_WRZ + 2 * HD * TC_K * 2;  // W_in  [128][64]
+constexpr int TC_OFF_WHN = TC_OFF_WIN + HD * C1 * 2;        // W_hn  [128][128]
+constexpr int TC_OFF_BIAS = TC_OFF_WHN + HD * HD * 2;       // float b_ih[384], b_hh[384]
+constexpr int TC_OFF_BAR = TC_OFF_BIAS + 2 * G3 * 4;        // mbarrier (8 B), TMEM address (4 B)
+constexpr int TC_SMEM = TC_OFF_BAR + 16;
+constexpr uint32_t TC_TMEM_COLS = 512;
+// a wait for the tensor cores longer than this many SM clocks (~1 s) is an error
+constexpr long long TC_WAIT_CYCLES = 2000000000LL;
+
+// Eight BF16 values as one 16-byte store.
+__device__ __forceinline__ uint4 pack8_bf16(const float* v) {
+    uint4 u;
+    u.x = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[0])) |
+          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[1])) << 16);
+    u.y = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[2])) |
+          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[3])) << 16);
+    u.z = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[4])) |
+          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[5])) << 16);
+    u.w = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[6])) |
+          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[7])) << 16);
+    return u;
+}
+
+// This thread's 32 conv channels (half `hc` of 64) of trajectory b at step t
+// (zeros past the batch or the time range; the conv output is already zero
+// past the trajectory's length).
+__device__ __forceinline__ void load_a32(const float* __restrict__ A, int b, int B, int t, int T, int hc,
+                                         float4 (&v)[8]) {
+    const bool ok = b < B && t < T;
+    const float4* src = reinterpret_cast<const float4*>(A + ((int64_t)(ok ? b : 0) * T + (ok ? t : 0)) * C1 + 32 * hc);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = ok ? __ldg(src + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+__device__ __forceinline__ void store_a32(unsigned char* X, int row, int hc, const float4 (&v)[8]) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float f[8] = {v[2 * c].x,     v[2 * c].y,     v[2 * c].z,     v[2 * c].w,
+                            v[2 * c + 1].x, v[2 * c + 1].y, v[2 * c + 1].z, v[2 * c + 1].w};
+        *reinterpret_cast<uint4*>(X + tsm::umma::core_offset(row, 32 * hc + 8 * c, TC_M)) = pack8_bf16(f);
+    }
+}
+
+// hl[b][128] = h after the last valid step of trajectory b.  A [B][T][64]:
+// conv output.  wq: BF16 weights; p: FP32 parameters (biases).  If the tensor
+// cores do not complete a step within TC_WAIT_CYCLES, the CTA writes NaN to
+// its rows of hl and stops.
+__global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const float* __restrict__ A,
+                                                                   const int32_t* __restrict__ len, int B, int T,
+                                                                   const __nv_bfloat16* __restrict__ wq,
+                                                                   const float* __restrict__ p,
+                                                                   float* __restrict__ hl) {
+    namespace U = tsm::umma;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char* X = sm + TC_OFF_X;
+    float* bias = reinterpret_cast<float*>(sm + TC_OFF_BIAS);
+    const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
+    const uint32_t bar = sbase + TC_OFF_BAR;
+    volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(sm + TC_OFF_BAR + 8);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int row = 32 * (warp & 3) + lane;  // this thread's trajectory (TMEM lane)
+    const int hc = warp >> 2;                // hidden units 64 hc .. +63, conv channels 32 hc .. +31
+    const int b = blockIdx.x * TC_M + row;
+    const int n = b < B ? len[b] : 0;
+
+    // weights -> core-matrix layout (16-byte chunks of 8 consecutive k)
+    for (int e = tid; e < 2 * HD * (TC_K / 8); e += TC_THREADS) {  // W_rz: gate rows 0..255, k < 192
+        const int r = e / (TC_K / 8), c = e % (TC_K / 8);
+        const __nv_bfloat16* src = c < C1 / 8 ? wq + OFF_WIH + r * C1 + 8 * c : wq + OFF_WHH + r * HD + 8 * (c - C1 / 8);
+        *reinterpret_cast<uint4*>(sm + TC_OFF_WRZ + U::core_offset(r, 8 * c, 2 * HD)) =
+            *reinterpret_cast<const uint4*>(src);
+    }
+    for (int e = tid; e < HD * (C1 / 8); e += TC_THREADS) {  // W_in: gate rows 256..383, k < 64
+        const int r = e / (C1 / 8), c = e % (C1 / 8);
+        *reinterpret_cast<uint4*>(sm + TC_OFF_WIN + U::core_offset(r, 8 * c, HD)) =
+            *reinterpret_cast<const uint4*>(wq + OFF_WIH + (2 * HD + r) * C1 + 8 * c);
+    }
+    for (int e = tid; e < HD * (HD / 8); e += TC_THREADS) {  // W_hn: gate rows 256..383, k < 128
+        const int r = e / (HD / 8), c = e % (HD / 8);
+        *reinterpret_cast<uint4*>(sm + TC_OFF_WHN + U::core_offset(r, 8 * c, HD)) =
+            *reinterpret_cast<const uint4*>(wq + OFF_WHH + (2 * HD + r) * HD + 8 * c);
+    }
+    for (int e = tid; e < 2 * G3; e += TC_THREADS) bias[e] = e < G3 ? p[OFF_BIH + e] : p[OFF_BHH + e - G3];
+    {  // X = [a_0 | h_0 = 0]
+        const float z8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int c = 0; c < 8; ++c)  // this thread's 64 hidden units
+            *reinterpret_cast<uint4*>(X + U::core_offset(row, C1 + 64 * hc + 8 * c, TC_M)) = pack8_bf16(z8);
+        float4 a[8];
+        load_a32(A, b, B, 0, T, hc, a);
+        store_a32(X, row, hc, a);
+    }
+    if (tid == 0) {
+        U::mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) U::tmem_alloc(sbase + TC_OFF_BAR + 8, TC_TMEM_COLS);
+    U::fence_smem_async();
+    U::fence_before_sync();
+    __syncthreads();
+    U::fence_after_sync();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t tl = tmem + ((uint32_t)(32 * (warp & 3)) << 16);  // this warp's lane quarter
+
+    int tmax = 0;
+    for (int i = 0; i < TC_M; ++i) {
+        const int bi = blockIdx.x * TC_M + i;
+        if (bi < B) tmax = max(tmax, len[bi]);
+    }
+    float h[64];
+#pragma unroll
+    for (int i = 0; i < 64; ++i) h[i] = 0.f;
+    bool failed = false;
+    for (int t = 0; t < tmax; ++t) {
+        if (tid == 0) {
+            U::fence_after_sync();
+            constexpr uint32_t kRZ = U::idesc_bf16_f32(TC_M, 2 * HD), kN = U::idesc_bf16_f32(TC_M, HD);
+            for (int ks = 0; ks < TC_K / 16; ++ks)  // r, z: X [W_ih | W_hh]^T, K = 192
+                U::mma_bf16(tmem, U::smem_desc(sbase + TC_OFF_X + ks * 2 * (TC_M * 16), TC_M * 16, 128),
+                            U::smem_desc(sbase + TC_OFF_WRZ + ks * 2 * (2 * HD * 16), 2 * HD * 16, 128), kRZ, ks);
+            for (int ks = 0; ks < C1 / 16; ++ks)  // Win a: the first 64 columns of X
+                U::mma_bf16(tmem + 2 * HD, U::smem_desc(sbase + TC_OFF_X + ks * 2 * (TC_M * 16), TC_M * 16, 128),
+                            U::smem_desc(sbase + TC_OFF_WIN + ks * 2 * (HD * 16), HD * 16, 128), kN, ks);
+            for (int ks = 0; ks < HD / 16; ++ks)  // Whn h: columns 64..191 of X
+                U::mma_bf16(tmem + 3 * HD,
+                            U::smem_desc(sbase + TC_OFF_X + (C1 / 8 + ks * 2) * (TC_M * 16), TC_M * 16, 128),
+                            U::smem_desc(sbase + TC_OFF_WHN + ks * 2 * (HD * 16), HD * 16, 128), kN, ks);
+            U::commit(bar);
+        }
+        float4 an[8];  // a_{t+1}, loaded while the tensor cores run
+        load_a32(A, b, B, t + 1, T, hc, an);
+        const bool ok = U::mbar_wait(bar, (uint32_t)(t & 1), TC_WAIT_CYCLES);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        U::fence_after_sync();
+        const bool live = t < n;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {  // 16 hidden units at a time
+            const int k0 = 64 * hc + 16 * c;
+            uint32_t rr[16], zz[16], ii[16], hh[16];
+            U::ld16(tl + k0, rr);
+            U::ld16(tl + HD + k0, zz);
+            U::ld16(tl + 2 * HD + k0, ii);
+            U::ld16(tl + 3 * HD + k0, hh);
+            U::wait_ld(rr);
+            U::wait_ld(zz);
+            U::wait_ld(ii);
+            U::wait_ld(hh);
+            float hv[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int k = k0 + j;
+                const float r = sigm(__uint_as_float(rr[j]) + bias[k] + bias[G3 + k]);
+                const float z = sigm(__uint_as_float(zz[j]) + bias[HD + k] + bias[G3 + HD + k]);
+                const float nn = tanhf(__uint_as_float(ii[j]) + bias[2 * HD + k] +
+                                       r * (__uint_as_float(hh[j]) + bias[G3 + 2 * HD + k]));
+                const float hp = h[16 * c + j];
+                hv[j] = live ? (1.f - z) * nn + z * hp : hp;
+                h[16 * c + j] = hv[j];
+            }
+            if (live) {
+                *reinterpret_cast<uint4*>(X + U::core_offset(row, C1 + k0, TC_M)) = pack8_bf16(hv);
+                *reinterpret_cast<uint4*>(X + U::core_offset(row, C1 + k0 + 8, TC_M)) = pack8_bf16(hv + 8);
+            }
+        }
+        store_a32(X, row, hc, an);
+        U::fence_smem_async();
+        U::fence_before_sync();
+        __syncthreads();
+    }
+    if (b < B) {
+        float* dst = hl + (int64_t)b * HD + 64 * hc;
+#pragma unroll
+        for (int i = 0; i < 64; ++i) dst[i] = failed ? __int_as_float(0x7fc00000) : h[i];
+    }
+    U::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        U::fence_after_sync();
+        U::tmem_dealloc(tmem, TC_TMEM_COLS);
+    }
+}
+
 }  // namespace enc
 
 // ---------------------------------------------------------------------------
@@ -581,6 +792,32 @@ int enc_backward(const float* params, const float* pts, const int64_t* off, cons
     return enc_check(cudaGetLastError(), "encoder backward launch");
 }
 
+// Inference workspace: conv output, last hidden states, embeddings, BF16 weights.
+struct EmbWs {
+    float *A, *hl, *E;
+    __nv_bfloat16* wq;
+};
+
+int64_t emb_layout(int B, int T, float* base, EmbWs* w) {
+    int64_t o = 0;
+    auto take = [&](int64_t n) {
+        float* q = base ? base + o : nullptr;
+        o += align64(n);
+        return q;
+    };
+    float* A = take((int64_t)B * T * enc::C1);
+    float* hl = take((int64_t)B * enc::HD);
+    float* E = take((int64_t)B * enc::ED);
+    float* wqf = take((enc::N_PARAMS + 1) / 2);
+    if (w) {
+        w->A = A;
+        w->hl = hl;
+        w->E = E;
+        w->wq = reinterpret_cast<__nv_bfloat16*>(wqf);
+    }
+    return o;
+}
+
 }  // namespace
 
 extern "C" {
@@ -635,6 +872,33 @@ int tsm_enc_adam(float* params, const float* grad, float* m, float* v, int32_t s
     enc::enc_adam<<<(enc::N_PARAMS + 255) / 256, 256, 0, (cudaStream_t)stream>>>(params, grad, m, v, enc::N_PARAMS, lr,
                                                                                  beta1, beta2, eps, bc1, bc2);
     return enc_check(cudaGetLastError(), "enc_adam launch");
+}
+
+int64_t tsm_enc_embed_workspace_bytes(int32_t B, int32_t T) {
+    if (B < 1 || T < 1) return 0;
+    return emb_layout(B, T, nullptr, nullptr) * 4;
+}
+
+int tsm_enc_embed(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
+                  int32_t T, const float* nrm, void* workspace, float* emb, void* stream) {
+    int rc = enc_args(params, pts, off, len, B, T, nrm, workspace);
+    if (rc) return rc;
+    if (!emb) return tsm_internal_fail(TSM_EINVAL, "tsm_enc_embed: null output");
+    using namespace enc;
+    EmbWs w;
+    emb_layout(B, T, static_cast<float*>(workspace), &w);
+    cudaStream_t s = (cudaStream_t)stream;
+    const float4 n4 = make_float4(nrm[0], nrm[1], nrm[2], nrm[3]);
+    enc_round_bf16<<<(OFF_WO + 255) / 256, 256, 0, s>>>(params, w.wq);
+    const int64_t tot = (int64_t)B * T * C1;
+    enc_conv_fwd<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(reinterpret_cast<const float2*>(pts), off, len, B, T,
+                                                                n4, w.wq, params, w.A);
+    rc = enc_check(cudaFuncSetAttribute(enc_gru_embed_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM),
+                   "cudaFuncSetAttribute(enc_gru_embed_tc)");
+    if (rc) return rc;
+    enc_gru_embed_tc<<<(B + TC_M - 1) / TC_M, TC_THREADS, TC_SMEM, s>>>(w.A, len, B, T, w.wq, params, w.hl);
+    enc_head_fwd<<<(unsigned)(((int64_t)B * ED + 255) / 256), 256, 0, s>>>(w.hl, B, params, emb);
+    return enc_check(cudaGetLastError(), "tsm_enc_embed launch");
 }
 
 }  // extern "C"

@@ -56,6 +56,7 @@ class Encoder:
     step: int = 0
     _ws: torch.Tensor = field(default=None, repr=False)
     _ws_key: tuple = field(default=(0, 0, 0), repr=False)
+    _ews: torch.Tensor = field(default=None, repr=False)  # inference workspace (tsm_enc_embed)
 
     @staticmethod
     def n_params() -> int:
@@ -90,23 +91,47 @@ class Encoder:
         return (ctypes.c_float * 4)(*[float(x) for x in self.nrm])
 
     # -- inference ----------------------------------------------------------------
-    def embed(self, s: TrajSet, idx=None, batch=2048, stream=None) -> torch.Tensor:
-        """Embeddings [n, 128] of trajectories idx (default all) of s."""
+    def embed(self, s: TrajSet, idx=None, batch=4096, stream=None, tensor_cores=True) -> torch.Tensor:
+        """Embeddings [n, 128] of trajectories idx (default all) of s.
+
+        tensor_cores=True: the tcgen05 inference kernel (tsm_enc_embed; a_t
+        and h_t enter the gate products as BF16), over batches of similar
+        lengths.  False: the training forward (tsm_enc_forward, FP32 a_t and h_t)."""
         lib = _lib.load()
         idx = torch.arange(s.n, device=s.device) if idx is None else torch.as_tensor(idx, device=s.device).long()
         out = torch.empty((idx.shape[0], EMB), dtype=torch.float32, device=s.device)
         lens_h = s.lens_host if s.lens_host is not None else s.lens.cpu().numpy()
         idx_h = idx.cpu().numpy()
+        # length order: a kernel CTA runs as many steps as its longest trajectory
+        perm_h = np.argsort(lens_h[idx_h], kind="stable") if tensor_cores else np.arange(idx_h.shape[0])
+        perm = torch.from_numpy(perm_h).to(s.device)
         for b0 in range(0, idx.shape[0], batch):
-            sel = idx[b0:b0 + batch]
+            pos = perm[b0:b0 + batch]
+            sel = idx[pos]
             B = int(sel.shape[0])
-            T = max(int(lens_h[idx_h[b0:b0 + batch]].max()), 1)
+            T = max(int(lens_h[idx_h[perm_h[b0:b0 + batch]]].max()), 1)
             off, ln = s.off[sel].contiguous(), s.lens[sel].contiguous()
-            ws = self._workspace(B, T, 1)
-            rc = lib.tsm_enc_forward(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T, self._nrm_ptr(),
-                                     _ptr(ws), _ptr(out[b0:b0 + B]), _stream_ptr(stream))
-            _lib.check(rc, "tsm_enc_forward")
+            res = torch.empty((B, EMB), dtype=torch.float32, device=s.device)
+            if tensor_cores:
+                ws = self._embed_workspace(B, T)
+                rc = lib.tsm_enc_embed(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T, self._nrm_ptr(),
+                                       _ptr(ws), _ptr(res), _stream_ptr(stream))
+                _lib.check(rc, "tsm_enc_embed")
+            else:
+                ws = self._workspace(B, T, 1)
+                rc = lib.tsm_enc_forward(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T,
+                                         self._nrm_ptr(), _ptr(ws), _ptr(res), _stream_ptr(stream))
+                _lib.check(rc, "tsm_enc_forward")
+            out[pos] = res
         return out
+
+    def _embed_workspace(self, B, T):
+        nb = _lib.load().tsm_enc_embed_workspace_bytes(B, T)
+        if nb <= 0:
+            raise ValueError("bad encoder batch shape")
+        if self._ews is None or self._ews.numel() * 4 < nb:
+            self._ews = torch.empty(nb // 4 + 64, dtype=torch.float32, device=self.params.device)
+        return self._ews
 
     # -- training -----------------------------------------------------------------
     def loss_grad(self, s: TrajSet, tidx, ia, ib, y, stream=None):
