@@ -491,8 +491,9 @@ __global__ void enc_adam(float* __restrict__ p, const float* __restrict__ g, flo
 // 64 (w / 4) .. +63, applies the gates with the biases in FP32, keeps h in FP32
 // registers and writes it back to X as BF16 for the next step.  a_t and h_t
 // enter the products as BF16 (the SIMT training kernel multiplies FP32 a and
-// h by the BF16 weights), so the embeddings agree with it to BF16 rounding of
-// the activations.
+// h by the BF16 weights) and the gates use the hardware tanh, so the
+// embeddings agree with the training forward to BF16 rounding of the
+// activations.
 constexpr int TC_M = 128;
 constexpr int TC_THREADS = 256;
 constexpr int TC_K = C1 + HD;                               // 192
@@ -506,6 +507,16 @@ constexpr int TC_SMEM = TC_OFF_BAR + 16;
 constexpr uint32_t TC_TMEM_COLS = 512;
 // a wait for the tensor cores longer than this many SM clocks (~1 s) is an error
 constexpr long long TC_WAIT_CYCLES = 2000000000LL;
+
+// Gate nonlinearities of the inference kernel: the hardware tanh (MUFU,
+// about 2^-11 relative error, the size of the BF16 rounding the operands
+// already carry) and sigma(x) = (1 + tanh(x / 2)) / 2, one MUFU operation each.
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sigm_hw(float x) { return fmaf(0.5f, tanh_hw(0.5f * x), 0.5f); }
 
 // Eight BF16 values as one 16-byte store.
 __device__ __forceinline__ uint4 pack8_bf16(const float* v) {
@@ -652,10 +663,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const float* _
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
                 const int k = k0 + j;
-                const float r = sigm(__uint_as_float(rr[j]) + bias[k] + bias[G3 + k]);
-                const float z = sigm(__uint_as_float(zz[j]) + bias[HD + k] + bias[G3 + HD + k]);
-                const float nn = tanhf(__uint_as_float(ii[j]) + bias[2 * HD + k] +
-                                       r * (__uint_as_float(hh[j]) + bias[G3 + 2 * HD + k]));
+                const float r = sigm_hw(__uint_as_float(rr[j]) + bias[k] + bias[G3 + k]);
+                const float z = sigm_hw(__uint_as_float(zz[j]) + bias[HD + k] + bias[G3 + HD + k]);
+                const float nn = tanh_hw(__uint_as_float(ii[j]) + bias[2 * HD + k] +
+                                         r * (__uint_as_float(hh[j]) + bias[G3 + 2 * HD + k]));
                 const float hp = h[16 * c + j];
                 hv[j] = live ? (1.f - z) * nn + z * hp : hp;
                 h[16 * c + j] = hv[j];

@@ -158,7 +158,7 @@ class SurrogateIndex:
     # embedding width + 1 (the squared norm), padded to a multiple of 4 floats
     AUG = 132
 
-    def __init__(self, encoder, D: TrajSet, batch=4096):
+    def __init__(self, encoder, D: TrajSet, batch=None):
         self.enc = encoder
         self.D = D
         emb = encoder.embed(D, batch=batch)

@@ -91,13 +91,17 @@ class Encoder:
         return (ctypes.c_float * 4)(*[float(x) for x in self.nrm])
 
     # -- inference ----------------------------------------------------------------
-    def embed(self, s: TrajSet, idx=None, batch=4096, stream=None, tensor_cores=True) -> torch.Tensor:
+    # trajectories per tensor-core embedding launch: 296 CTAs of 128, two per SM of a B200
+    TC_BATCH = 296 * 128
+
+    def embed(self, s: TrajSet, idx=None, batch=None, stream=None, tensor_cores=True) -> torch.Tensor:
         """Embeddings [n, 128] of trajectories idx (default all) of s.
 
         tensor_cores=True: the tcgen05 inference kernel (tsm_enc_embed; a_t
         and h_t enter the gate products as BF16), over batches of similar
         lengths.  False: the training forward (tsm_enc_forward, FP32 a_t and h_t)."""
         lib = _lib.load()
+        batch = batch or (self.TC_BATCH if tensor_cores else 4096)
         idx = torch.arange(s.n, device=s.device) if idx is None else torch.as_tensor(idx, device=s.device).long()
         out = torch.empty((idx.shape[0], EMB), dtype=torch.float32, device=s.device)
         lens_h = s.lens_host if s.lens_host is not None else s.lens.cpu().numpy()
@@ -186,7 +190,7 @@ class Encoder:
                 log(f"epoch {ep}: mse {hist[-1]:.3e}")
         return hist
 
-    def predict_pairs(self, s: TrajSet, pa, pb, batch=4096) -> np.ndarray:
+    def predict_pairs(self, s: TrajSet, pa, pb, batch=None) -> np.ndarray:
         """||e_a - e_b|| for pairs of s (normalised-distance units)."""
         pa = np.asarray(pa)
         pb = np.asarray(pb)
