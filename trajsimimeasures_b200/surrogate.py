@@ -91,7 +91,7 @@ class Encoder:
         return (ctypes.c_float * 4)(*[float(x) for x in self.nrm])
 
     # -- inference ----------------------------------------------------------------
-    # trajectories per tensor-core embedding launch: 296 CTAs of 128, two per SM of a B200
+    # trajectories per tensor-core embedding launch: 296 CTAs of 128, two waves over a B200's 148 SMs
     TC_BATCH = 296 * 128
 
     def embed(self, s: TrajSet, idx=None, batch=None, stream=None, tensor_cores=True) -> torch.Tensor:
