@@ -29,6 +29,7 @@
 //   enc_gemm_tn       split-K reduction dW[m][n] += sum_k A[k][m] B[k][n]  (weight gradients)
 //   enc_conv_bwd      dW1, db1
 //   enc_adam          Adam step on the FP32 master weights
+//   enc_conv_fwd_tc   conv + relu -> BF16 a_t operand images for the tensor-core GRU
 //   enc_gru_embed_tc  inference GRU on the tensor cores -> last hidden state
 #include <cuda_bf16.h>
 #include <cstdio>
@@ -206,17 +207,36 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
     }
 }
 
-// E[b][o] = bo[o] + sum_k Wo[o][k] hl[b][k].  One thread per (b, o).
-__global__ void enc_head_fwd(const float* __restrict__ hl, int B, const float* __restrict__ p, float* __restrict__ E) {
-    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= (int64_t)B * ED) return;
-    const int o = gid % ED;
-    const int64_t b = gid / ED;
-    float acc = p[OFF_BO + o];
-    const float* w = p + OFF_WO + o * HD;
-    const float* h = hl + b * HD;
-    for (int k = 0; k < HD; ++k) acc = fmaf(w[k], h[k], acc);
-    E[gid] = acc;
+// E[b][o] = bo[o] + sum_k Wo[o][k] hl[b][k] (bias first, k ascending).  One
+// thread per output o, HEAD_B trajectories per CTA, their hidden states
+// staged in shared memory; each W_o row is read once per CTA.
+constexpr int HEAD_B = 32;
+__global__ void __launch_bounds__(ED) enc_head_fwd(const float* __restrict__ hl, int B, const float* __restrict__ p,
+                                                   float* __restrict__ E) {
+    __shared__ __align__(16) float hs[HEAD_B][HD];
+    const int o = threadIdx.x;
+    const int64_t b0 = (int64_t)blockIdx.x * HEAD_B;
+    for (int e = o; e < HEAD_B * HD; e += ED) {
+        const int64_t b = b0 + e / HD;
+        hs[e / HD][e % HD] = b < B ? hl[b * HD + e % HD] : 0.f;
+    }
+    __syncthreads();
+    float acc[HEAD_B];
+    const float bo = p[OFF_BO + o];
+#pragma unroll
+    for (int j = 0; j < HEAD_B; ++j) acc[j] = bo;
+    const float* w = p + OFF_WO + o * HD;  // the caller's buffer: 4-byte alignment only
+    for (int k = 0; k < HD; k += 4) {
+        const float w0 = __ldg(w + k), w1 = __ldg(w + k + 1), w2 = __ldg(w + k + 2), w3 = __ldg(w + k + 3);
+#pragma unroll
+        for (int j = 0; j < HEAD_B; ++j) {
+            const float4 h = *reinterpret_cast<const float4*>(&hs[j][k]);
+            acc[j] = fmaf(w3, h.w, fmaf(w2, h.z, fmaf(w1, h.y, fmaf(w0, h.x, acc[j]))));
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < HEAD_B; ++j)
+        if (b0 + j < B) E[(b0 + j) * ED + o] = acc[j];
 }
 
 // One warp per pair: pred = ||E[ia]-E[ib]||, loss += (pred-y)^2 / P,
@@ -478,34 +498,40 @@ __global__ void enc_adam(float* __restrict__ p, const float* __restrict__ g, flo
 
 // ---------------------------------------------------------------------------
 // Tensor-core GRU forward for inference (tcgen05).  CTA = 128 trajectories
-// (the MMA's M), 256 threads.  Per time step the operand X = [a_t | h_t]
+// (the MMA's M), 256 threads.  Per time step the operand [a_t | h_t]
 // (128 x 192 BF16, shared memory) is multiplied by the BF16 gate weights,
 // resident in shared memory for all steps, into three FP32 accumulators in
 // tensor memory (512 columns):
-//   columns   0..255  r and z pre-activations  X [Wih_rz | Whh_rz]^T  (K = 192)
-//   columns 256..383  Win a_t                   a_t Wih_n^T            (K = 64)
-//   columns 384..511  Whn h_t                   h_t Whh_n^T            (K = 128)
+//   columns   0..255  r and z pre-activations  [a_t | h_t] [Wih_rz | Whh_rz]^T  (K = 192)
+//   columns 256..383  Win a_t                   a_t Wih_n^T                      (K = 64)
+//   columns 384..511  Whn h_t                   h_t Whh_n^T                      (K = 128)
 // (n needs Whn h apart from Win a: r multiplies only the hidden part.)  One
 // thread issues the 24 MMAs and commits them to an mbarrier; then warp w reads
 // lanes 32 (w % 4) .. +31 (its 32 trajectories) and hidden units
 // 64 (w / 4) .. +63, applies the gates with the biases in FP32, keeps h in FP32
-// registers and writes it back to X as BF16 for the next step.  a_t and h_t
-// enter the products as BF16 (the SIMT training kernel multiplies FP32 a and
-// h by the BF16 weights) and the gates use the hardware tanh, so the
-// embeddings agree with the training forward to BF16 rounding of the
-// activations.
+// registers and writes it back to shared memory as BF16 for the next step.
+// The a_t part comes from enc_conv_fwd_tc as one 16 KB BF16 image per step
+// already in the operand layout; thread 0 bulk-copies step t+1's image into
+// the second of two a-buffers while step t computes (per-buffer mbarriers
+// count the bytes).  a_t and h_t enter the products as BF16 (the SIMT training
+// kernel multiplies FP32 a and h by the BF16 weights) and the gates use the
+// hardware tanh, so the embeddings agree with the training forward to BF16
+// rounding of the activations.
 constexpr int TC_M = 128;
 constexpr int TC_THREADS = 256;
 constexpr int TC_K = C1 + HD;                               // 192
-constexpr int TC_OFF_X = 0;                                 // X     [128][192] BF16
-constexpr int TC_OFF_WRZ = TC_OFF_X + TC_M * TC_K * 2;      // W_rz  [256][192] BF16
-constexpr int TC_OFF_WIN = TC_OFF_WRZ + 2 * HD * TC_K * 2;  // W_in  [128][64]
-constexpr int TC_OFF_WHN = TC_OFF_WIN + HD * C1 * 2;        // W_hn  [128][128]
+constexpr int TC_A_BYTES = TC_M * C1 * 2;                   // one a_t image: 16 KB
+constexpr int TC_OFF_A0 = 0;                                // a-buffers [128][64] BF16
+constexpr int TC_OFF_A1 = TC_OFF_A0 + TC_A_BYTES;
+constexpr int TC_OFF_XH = TC_OFF_A1 + TC_A_BYTES;           // h [128][128] BF16
+constexpr int TC_OFF_WRZ = TC_OFF_XH + TC_M * HD * 2;       // W_rz [256][192] BF16
+constexpr int TC_OFF_WIN = TC_OFF_WRZ + 2 * HD * TC_K * 2;  // W_in [128][64]
+constexpr int TC_OFF_WHN = TC_OFF_WIN + HD * C1 * 2;        // W_hn [128][128]
 constexpr int TC_OFF_BIAS = TC_OFF_WHN + HD * HD * 2;       // float b_ih[384], b_hh[384]
-constexpr int TC_OFF_BAR = TC_OFF_BIAS + 2 * G3 * 4;        // mbarrier (8 B), TMEM address (4 B)
-constexpr int TC_SMEM = TC_OFF_BAR + 16;
+constexpr int TC_OFF_BAR = TC_OFF_BIAS + 2 * G3 * 4;        // mbarriers: MMA, a0, a1 (8 B each); TMEM address
+constexpr int TC_SMEM = TC_OFF_BAR + 32;
 constexpr uint32_t TC_TMEM_COLS = 512;
-// a wait for the tensor cores longer than this many SM clocks (~1 s) is an error
+// a wait for the tensor cores or a copy longer than this many SM clocks (~1 s) is an error
 constexpr long long TC_WAIT_CYCLES = 2000000000LL;
 
 // Gate nonlinearities of the inference kernel: the hardware tanh (MUFU,
@@ -532,47 +558,81 @@ __device__ __forceinline__ uint4 pack8_bf16(const float* v) {
     return u;
 }
 
-// This thread's 32 conv channels (half `hc` of 64) of trajectory b at step t
-// (zeros past the batch or the time range; the conv output is already zero
-// past the trajectory's length).
-__device__ __forceinline__ void load_a32(const float* __restrict__ A, int b, int B, int t, int T, int hc,
-                                         float4 (&v)[8]) {
-    const bool ok = b < B && t < T;
-    const float4* src = reinterpret_cast<const float4*>(A + ((int64_t)(ok ? b : 0) * T + (ok ? t : 0)) * C1 + 32 * hc);
+// Conv output for the tensor-core GRU (same arithmetic as enc_conv_fwd, then
+// rounded to BF16): for block g of 128 trajectories and step t, the 16 KB
+// image of the a_t operand (rows = trajectories, k = channels, core-matrix
+// layout) at Ab + (g * T + t) * 128 * 64.  Rows past B and steps past a
+// trajectory's length are zero.  One thread per (trajectory, step), all 64
+// channels, with the conv weights in shared memory; consecutive threads take
+// consecutive rows of one image, so a warp's 16-byte stores are contiguous.
+// Bp = B rounded up to a multiple of 128; blockDim = 256.
+__global__ void __launch_bounds__(256) enc_conv_fwd_tc(const float2* __restrict__ pts, const int64_t* __restrict__ off,
+                                                       const int32_t* __restrict__ len, int B, int Bp, int T,
+                                                       float4 nrm, const __nv_bfloat16* __restrict__ wq,
+                                                       const float* __restrict__ p, __nv_bfloat16* __restrict__ Ab) {
+    __shared__ float w1[C1 * 2 * KW], b1[C1];
+    for (int e = threadIdx.x; e < C1 * 2 * KW; e += blockDim.x) w1[e] = __bfloat162float(wq[OFF_W1 + e]);
+    for (int e = threadIdx.x; e < C1; e += blockDim.x) b1[e] = p[OFF_B1 + e];
+    __syncthreads();
+    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (int64_t)Bp * T) return;
+    const int row = gid % TC_M;
+    const int t = (gid / TC_M) % T;
+    const int g = gid / ((int64_t)TC_M * T);
+    const int b = g * TC_M + row;
+    const int n = b < B ? len[b] : 0;
+    float x[KW][2];  // the window's normalised points
+    if (t < n) {
+        const int64_t o = off[b];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) v[i] = ok ? __ldg(src + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-}
-
-__device__ __forceinline__ void store_a32(unsigned char* X, int row, int hc, const float4 (&v)[8]) {
+        for (int k = 0; k < KW; ++k)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        const float f[8] = {v[2 * c].x,     v[2 * c].y,     v[2 * c].z,     v[2 * c].w,
-                            v[2 * c + 1].x, v[2 * c + 1].y, v[2 * c + 1].z, v[2 * c + 1].w};
-        *reinterpret_cast<uint4*>(X + tsm::umma::core_offset(row, 32 * hc + 8 * c, TC_M)) = pack8_bf16(f);
+            for (int i = 0; i < 2; ++i) x[k][i] = xin(pts, o, n, t + k - 2, i, nrm);
+    }
+    unsigned char* img = reinterpret_cast<unsigned char*>(Ab + ((int64_t)g * T + t) * (TC_M * C1));
+#pragma unroll 1
+    for (int c8 = 0; c8 < C1 / 8; ++c8) {
+        float a[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int c = 8 * c8 + q;
+            float v = 0.f;
+            if (t < n) {
+                float acc = b1[c];
+#pragma unroll
+                for (int k = 0; k < KW; ++k)
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) acc = fmaf(w1[(c * 2 + i) * KW + k], x[k][i], acc);
+                v = fmaxf(acc, 0.f);
+            }
+            a[q] = v;
+        }
+        *reinterpret_cast<uint4*>(img + tsm::umma::core_offset(row, 8 * c8, TC_M)) = pack8_bf16(a);
     }
 }
 
-// hl[b][128] = h after the last valid step of trajectory b.  A [B][T][64]:
-// conv output.  wq: BF16 weights; p: FP32 parameters (biases).  If the tensor
-// cores do not complete a step within TC_WAIT_CYCLES, the CTA writes NaN to
-// its rows of hl and stops.
-__global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const float* __restrict__ A,
+// hl[b][128] = h after the last valid step of trajectory b.  Ab: the a_t
+// images of enc_conv_fwd_tc (T steps per block of 128).  wq: BF16 weights; p:
+// FP32 parameters (biases).  If the tensor cores or a copy do not complete
+// within TC_WAIT_CYCLES, the CTA writes NaN to its rows of hl and stops.
+__global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfloat16* __restrict__ Ab,
                                                                    const int32_t* __restrict__ len, int B, int T,
                                                                    const __nv_bfloat16* __restrict__ wq,
                                                                    const float* __restrict__ p,
                                                                    float* __restrict__ hl) {
     namespace U = tsm::umma;
     extern __shared__ __align__(1024) unsigned char sm[];
-    unsigned char* X = sm + TC_OFF_X;
+    unsigned char* XH = sm + TC_OFF_XH;
     float* bias = reinterpret_cast<float*>(sm + TC_OFF_BIAS);
     const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
-    const uint32_t bar = sbase + TC_OFF_BAR;
-    volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(sm + TC_OFF_BAR + 8);
+    const uint32_t mbar = sbase + TC_OFF_BAR, abar0 = mbar + 8, abar1 = mbar + 16;
+    volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(sm + TC_OFF_BAR + 24);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int row = 32 * (warp & 3) + lane;  // this thread's trajectory (TMEM lane)
-    const int hc = warp >> 2;                // hidden units 64 hc .. +63, conv channels 32 hc .. +31
+    const int hc = warp >> 2;                // hidden units 64 hc .. +63
     const int b = blockIdx.x * TC_M + row;
     const int n = b < B ? len[b] : 0;
+    const __nv_bfloat16* img = Ab + (int64_t)blockIdx.x * T * (TC_M * C1);  // this block's a_t images
 
     // weights -> core-matrix layout (16-byte chunks of 8 consecutive k)
     for (int e = tid; e < 2 * HD * (TC_K / 8); e += TC_THREADS) {  // W_rz: gate rows 0..255, k < 192
@@ -592,20 +652,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const float* _
             *reinterpret_cast<const uint4*>(wq + OFF_WHH + (2 * HD + r) * HD + 8 * c);
     }
     for (int e = tid; e < 2 * G3; e += TC_THREADS) bias[e] = e < G3 ? p[OFF_BIH + e] : p[OFF_BHH + e - G3];
-    {  // X = [a_0 | h_0 = 0]
+    {  // h_0 = 0: this thread's 64 hidden units
         const float z8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-        for (int c = 0; c < 8; ++c)  // this thread's 64 hidden units
-            *reinterpret_cast<uint4*>(X + U::core_offset(row, C1 + 64 * hc + 8 * c, TC_M)) = pack8_bf16(z8);
-        float4 a[8];
-        load_a32(A, b, B, 0, T, hc, a);
-        store_a32(X, row, hc, a);
+        for (int c = 0; c < 8; ++c) *reinterpret_cast<uint4*>(XH + U::core_offset(row, 64 * hc + 8 * c, TC_M)) = pack8_bf16(z8);
     }
     if (tid == 0) {
-        U::mbar_init(bar, 1);
+        U::mbar_init(mbar, 1);
+        U::mbar_init(abar0, 1);
+        U::mbar_init(abar1, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) U::tmem_alloc(sbase + TC_OFF_BAR + 8, TC_TMEM_COLS);
+    if (warp == 0) U::tmem_alloc(sbase + TC_OFF_BAR + 24, TC_TMEM_COLS);
     U::fence_smem_async();
     U::fence_before_sync();
     __syncthreads();
@@ -618,29 +676,48 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const float* _
         const int bi = blockIdx.x * TC_M + i;
         if (bi < B) tmax = max(tmax, len[bi]);
     }
+    tmax = min(tmax, T);
+    int pend = -1;  // thread 0: the step whose a_t copy is issued and not yet waited for
+    if (tid == 0 && tmax > 0) {  // a_0 into buffer 0
+        U::mbar_arrive_expect_tx(abar0, TC_A_BYTES);
+        U::bulk_load(sbase + TC_OFF_A0, img, TC_A_BYTES, abar0);
+        pend = 0;
+    }
     float h[64];
 #pragma unroll
     for (int i = 0; i < 64; ++i) h[i] = 0.f;
     bool failed = false;
     for (int t = 0; t < tmax; ++t) {
+        const uint32_t abuf = sbase + ((t & 1) ? TC_OFF_A1 : TC_OFF_A0);
         if (tid == 0) {
-            U::fence_after_sync();
-            constexpr uint32_t kRZ = U::idesc_bf16_f32(TC_M, 2 * HD), kN = U::idesc_bf16_f32(TC_M, HD);
-            for (int ks = 0; ks < TC_K / 16; ++ks)  // r, z: X [W_ih | W_hh]^T, K = 192
-                U::mma_bf16(tmem, U::smem_desc(sbase + TC_OFF_X + ks * 2 * (TC_M * 16), TC_M * 16, 128),
-                            U::smem_desc(sbase + TC_OFF_WRZ + ks * 2 * (2 * HD * 16), 2 * HD * 16, 128), kRZ, ks);
-            for (int ks = 0; ks < C1 / 16; ++ks)  // Win a: the first 64 columns of X
-                U::mma_bf16(tmem + 2 * HD, U::smem_desc(sbase + TC_OFF_X + ks * 2 * (TC_M * 16), TC_M * 16, 128),
-                            U::smem_desc(sbase + TC_OFF_WIN + ks * 2 * (HD * 16), HD * 16, 128), kN, ks);
-            for (int ks = 0; ks < HD / 16; ++ks)  // Whn h: columns 64..191 of X
-                U::mma_bf16(tmem + 3 * HD,
-                            U::smem_desc(sbase + TC_OFF_X + (C1 / 8 + ks * 2) * (TC_M * 16), TC_M * 16, 128),
-                            U::smem_desc(sbase + TC_OFF_WHN + ks * 2 * (HD * 16), HD * 16, 128), kN, ks);
-            U::commit(bar);
+            // a_t has landed in buffer t % 2 (its (t / 2)-th use)
+            if (U::mbar_wait((t & 1) ? abar1 : abar0, (uint32_t)((t >> 1) & 1), TC_WAIT_CYCLES)) {
+                pend = -1;
+                U::fence_after_sync();
+                constexpr uint32_t kRZ = U::idesc_bf16_f32(TC_M, 2 * HD), kN = U::idesc_bf16_f32(TC_M, HD);
+                constexpr uint32_t kLBO = TC_M * 16;  // K-chunk stride of the 128-row operands
+                for (int ks = 0; ks < TC_K / 16; ++ks) {  // r, z: [a_t | h_t] [W_ih | W_hh]^T, K = 192
+                    const uint32_t a = ks < C1 / 16 ? abuf + ks * 2 * kLBO : sbase + TC_OFF_XH + (ks - C1 / 16) * 2 * kLBO;
+                    U::mma_bf16(tmem, U::smem_desc(a, kLBO, 128),
+                                U::smem_desc(sbase + TC_OFF_WRZ + ks * 2 * (2 * HD * 16), 2 * HD * 16, 128), kRZ, ks);
+                }
+                for (int ks = 0; ks < C1 / 16; ++ks)  // Win a_t
+                    U::mma_bf16(tmem + 2 * HD, U::smem_desc(abuf + ks * 2 * kLBO, kLBO, 128),
+                                U::smem_desc(sbase + TC_OFF_WIN + ks * 2 * (HD * 16), HD * 16, 128), kN, ks);
+                for (int ks = 0; ks < HD / 16; ++ks)  // Whn h_t
+                    U::mma_bf16(tmem + 3 * HD, U::smem_desc(sbase + TC_OFF_XH + ks * 2 * kLBO, kLBO, 128),
+                                U::smem_desc(sbase + TC_OFF_WHN + ks * 2 * (HD * 16), HD * 16, 128), kN, ks);
+                U::commit(mbar);
+                if (t + 1 < tmax) {  // a_{t+1} into the other buffer (its last reader, step t-1, has completed)
+                    const uint32_t nb = (t & 1) ? abar0 : abar1;
+                    U::mbar_arrive_expect_tx(nb, TC_A_BYTES);
+                    U::bulk_load(sbase + ((t & 1) ? TC_OFF_A0 : TC_OFF_A1), img + (int64_t)(t + 1) * (TC_M * C1),
+                                 TC_A_BYTES, nb);
+                    pend = t + 1;
+                }
+            }
         }
-        float4 an[8];  // a_{t+1}, loaded while the tensor cores run
-        load_a32(A, b, B, t + 1, T, hc, an);
-        const bool ok = U::mbar_wait(bar, (uint32_t)(t & 1), TC_WAIT_CYCLES);
+        const bool ok = U::mbar_wait(mbar, (uint32_t)(t & 1), TC_WAIT_CYCLES);
         if (__syncthreads_or(!ok)) {
             failed = true;
             break;
@@ -672,15 +749,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const float* _
                 h[16 * c + j] = hv[j];
             }
             if (live) {
-                *reinterpret_cast<uint4*>(X + U::core_offset(row, C1 + k0, TC_M)) = pack8_bf16(hv);
-                *reinterpret_cast<uint4*>(X + U::core_offset(row, C1 + k0 + 8, TC_M)) = pack8_bf16(hv + 8);
+                *reinterpret_cast<uint4*>(XH + U::core_offset(row, k0, TC_M)) = pack8_bf16(hv);
+                *reinterpret_cast<uint4*>(XH + U::core_offset(row, k0 + 8, TC_M)) = pack8_bf16(hv + 8);
             }
         }
-        store_a32(X, row, hc, an);
         U::fence_smem_async();
         U::fence_before_sync();
         __syncthreads();
     }
+    if (tid == 0 && pend >= 0)  // after a failure: let this CTA's copy in flight land before exiting
+        U::mbar_wait((pend & 1) ? abar1 : abar0, (uint32_t)((pend >> 1) & 1), TC_WAIT_CYCLES);
     if (b < B) {
         float* dst = hl + (int64_t)b * HD + 64 * hc;
 #pragma unroll
@@ -772,7 +850,7 @@ int enc_forward(const float* params, const float* pts, const int64_t* off, const
     if (rc) return rc;
     enc_gru_fwd<<<(B + S - 1) / S, GRU_THREADS, kGruFwdSmem, s>>>(w.A, len, B, T, w.wq, params, w.H, w.R, w.Z, w.N,
                                                                    w.GHN, w.hl);
-    enc_head_fwd<<<(unsigned)(((int64_t)B * ED + 255) / 256), 256, 0, s>>>(w.hl, B, params, w.E);
+    enc_head_fwd<<<(unsigned)((B + HEAD_B - 1) / HEAD_B), ED, 0, s>>>(w.hl, B, params, w.E);
     return enc_check(cudaGetLastError(), "encoder forward launch");
 }
 
@@ -803,9 +881,11 @@ int enc_backward(const float* params, const float* pts, const int64_t* off, cons
     return enc_check(cudaGetLastError(), "encoder backward launch");
 }
 
-// Inference workspace: conv output, last hidden states, embeddings, BF16 weights.
+// Inference workspace: the BF16 a_t images (B rounded up to 128 rows), last
+// hidden states, embeddings, BF16 weights.
 struct EmbWs {
-    float *A, *hl, *E;
+    __nv_bfloat16* Ab;
+    float *hl, *E;
     __nv_bfloat16* wq;
 };
 
@@ -816,12 +896,13 @@ int64_t emb_layout(int B, int T, float* base, EmbWs* w) {
         o += align64(n);
         return q;
     };
-    float* A = take((int64_t)B * T * enc::C1);
+    const int64_t Bp = ((int64_t)B + enc::TC_M - 1) / enc::TC_M * enc::TC_M;
+    float* Ab = take(Bp * T * enc::C1 / 2);
     float* hl = take((int64_t)B * enc::HD);
     float* E = take((int64_t)B * enc::ED);
     float* wqf = take((enc::N_PARAMS + 1) / 2);
     if (w) {
-        w->A = A;
+        w->Ab = reinterpret_cast<__nv_bfloat16*>(Ab);
         w->hl = hl;
         w->E = E;
         w->wq = reinterpret_cast<__nv_bfloat16*>(wqf);
@@ -901,14 +982,15 @@ int tsm_enc_embed(const float* params, const float* pts, const int64_t* off, con
     cudaStream_t s = (cudaStream_t)stream;
     const float4 n4 = make_float4(nrm[0], nrm[1], nrm[2], nrm[3]);
     enc_round_bf16<<<(OFF_WO + 255) / 256, 256, 0, s>>>(params, w.wq);
-    const int64_t tot = (int64_t)B * T * C1;
-    enc_conv_fwd<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(reinterpret_cast<const float2*>(pts), off, len, B, T,
-                                                                n4, w.wq, params, w.A);
+    const int Bp = (B + TC_M - 1) / TC_M * TC_M;
+    const int64_t tot = (int64_t)Bp * T;
+    enc_conv_fwd_tc<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(reinterpret_cast<const float2*>(pts), off, len, B,
+                                                                   Bp, T, n4, w.wq, params, w.Ab);
     rc = enc_check(cudaFuncSetAttribute(enc_gru_embed_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM),
                    "cudaFuncSetAttribute(enc_gru_embed_tc)");
     if (rc) return rc;
-    enc_gru_embed_tc<<<(B + TC_M - 1) / TC_M, TC_THREADS, TC_SMEM, s>>>(w.A, len, B, T, w.wq, params, w.hl);
-    enc_head_fwd<<<(unsigned)(((int64_t)B * ED + 255) / 256), 256, 0, s>>>(w.hl, B, params, emb);
+    enc_gru_embed_tc<<<Bp / TC_M, TC_THREADS, TC_SMEM, s>>>(w.Ab, len, B, T, w.wq, params, w.hl);
+    enc_head_fwd<<<(unsigned)((B + HEAD_B - 1) / HEAD_B), ED, 0, s>>>(w.hl, B, params, emb);
     return enc_check(cudaGetLastError(), "tsm_enc_embed launch");
 }
 

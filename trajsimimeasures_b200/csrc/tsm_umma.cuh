@@ -1,7 +1,7 @@
 // Fifth-generation tensor-core primitives (tcgen05, sm_100a) in inline PTX:
 // shared-memory matrix descriptors, the instruction descriptor of a BF16 x
-// BF16 -> FP32 MMA, tensor-memory allocation, MMA issue and completion, and
-// tensor-memory loads.
+// BF16 -> FP32 MMA, tensor-memory allocation, MMA issue and completion,
+// tensor-memory loads, and bulk global -> shared copies on an mbarrier.
 //
 // Operand layout used with these descriptors (K-major, no swizzle): the matrix
 // is cut into "core matrices" of 8 rows x 16 bytes (8 BF16 along K), each
@@ -87,6 +87,22 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar_saddr, uint32_t parity, l
         if (done) return true;
         if (clock64() - t0 > max_cycles) return false;
     }
+}
+
+// Arrival on the mbarrier that also expects `bytes` of asynchronous copies
+// to land in the current phase.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar_saddr, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(bar_saddr) : "memory");
+}
+
+// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned)
+// from this GPU's global memory into shared memory, completing on the
+// mbarrier's transaction count (no multicast).
+__device__ __forceinline__ void bulk_load(uint32_t dst_saddr, const void* src, uint32_t bytes, uint32_t bar_saddr) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     dst_saddr),
+                 "l"(src), "r"(bytes), "r"(bar_saddr)
+                 : "memory");
 }
 
 // Tensor-memory allocation by one whole warp: ncols columns (a power of two

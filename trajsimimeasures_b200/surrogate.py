@@ -103,39 +103,41 @@ class Encoder:
         lib = _lib.load()
         batch = batch or (self.TC_BATCH if tensor_cores else 4096)
         idx = torch.arange(s.n, device=s.device) if idx is None else torch.as_tensor(idx, device=s.device).long()
-        out = torch.empty((idx.shape[0], EMB), dtype=torch.float32, device=s.device)
-        lens_h = s.lens_host if s.lens_host is not None else s.lens.cpu().numpy()
-        idx_h = idx.cpu().numpy()
-        # length order: a kernel CTA runs as many steps as its longest trajectory
-        perm_h = np.argsort(lens_h[idx_h], kind="stable") if tensor_cores else np.arange(idx_h.shape[0])
-        perm = torch.from_numpy(perm_h).to(s.device)
-        for b0 in range(0, idx.shape[0], batch):
-            pos = perm[b0:b0 + batch]
-            sel = idx[pos]
-            B = int(sel.shape[0])
-            T = max(int(lens_h[idx_h[perm_h[b0:b0 + batch]]].max()), 1)
-            off, ln = s.off[sel].contiguous(), s.lens[sel].contiguous()
-            res = torch.empty((B, EMB), dtype=torch.float32, device=s.device)
+        n = int(idx.shape[0])
+        out = torch.empty((n, EMB), dtype=torch.float32, device=s.device)
+        if n == 0:
+            return out
+        # length order on the device: a kernel CTA runs as many steps as its longest trajectory
+        lens_d = s.lens[idx]
+        perm = torch.argsort(lens_d, stable=True) if tensor_cores else torch.arange(n, device=s.device)
+        sel_all = idx[perm]
+        off_all, ln_all = s.off[sel_all].contiguous(), s.lens[sel_all].contiguous()
+        starts = list(range(0, n, batch))
+        ends = [min(b0 + batch, n) for b0 in starts]
+        if tensor_cores:  # sorted: a batch's longest trajectory is its last
+            tmax = ln_all[torch.tensor([e - 1 for e in ends], device=s.device)].cpu().numpy()
+        else:
+            tmax = torch.stack([ln_all[b0:e].max() for b0, e in zip(starts, ends)]).cpu().numpy()
+        res = torch.empty((n, EMB), dtype=torch.float32, device=s.device)  # in processing order
+        if tensor_cores:  # one workspace for the largest batch
+            need = max(lib.tsm_enc_embed_workspace_bytes(e - b0, max(int(t), 1))
+                       for b0, e, t in zip(starts, ends, tmax))
+            if self._ews is None or self._ews.numel() * 4 < need:
+                self._ews = torch.empty(need // 4 + 64, dtype=torch.float32, device=self.params.device)
+        for b0, e, t in zip(starts, ends, tmax):
+            B, T = e - b0, max(int(t), 1)
+            off, ln, r = off_all[b0:e], ln_all[b0:e], res[b0:e]
             if tensor_cores:
-                ws = self._embed_workspace(B, T)
                 rc = lib.tsm_enc_embed(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T, self._nrm_ptr(),
-                                       _ptr(ws), _ptr(res), _stream_ptr(stream))
+                                       _ptr(self._ews), _ptr(r), _stream_ptr(stream))
                 _lib.check(rc, "tsm_enc_embed")
             else:
                 ws = self._workspace(B, T, 1)
                 rc = lib.tsm_enc_forward(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T,
-                                         self._nrm_ptr(), _ptr(ws), _ptr(res), _stream_ptr(stream))
+                                         self._nrm_ptr(), _ptr(ws), _ptr(r), _stream_ptr(stream))
                 _lib.check(rc, "tsm_enc_forward")
-            out[pos] = res
+        out[perm] = res
         return out
-
-    def _embed_workspace(self, B, T):
-        nb = _lib.load().tsm_enc_embed_workspace_bytes(B, T)
-        if nb <= 0:
-            raise ValueError("bad encoder batch shape")
-        if self._ews is None or self._ews.numel() * 4 < nb:
-            self._ews = torch.empty(nb // 4 + 64, dtype=torch.float32, device=self.params.device)
-        return self._ews
 
     # -- training -----------------------------------------------------------------
     def loss_grad(self, s: TrajSet, tidx, ia, ib, y, stream=None):
