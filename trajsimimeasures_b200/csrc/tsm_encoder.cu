@@ -404,43 +404,58 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_bwd(
 }
 
 // C[m][n] += sum_k A[k*lda + m] * Bm[k*ldb + n] over k in this CTA's K slice.
-// Tile 32 x 32 outputs per CTA (256 threads, 4 outputs each), K split across
-// blockIdx.z; partial sums are atomically added.  Weight gradients are
-// reductions over (trajectory, time) with K up to a few 10^5.
+// Tile 64 x 64 outputs per CTA (256 threads, a 4 x 4 register block each:
+// two 16-byte shared loads feed 16 FMAs), K split across blockIdx.z; partial
+// sums are atomically added.  Weight gradients are reductions over
+// (trajectory, time) with K up to a few 10^5.
 // bgroup > 0: B has one extra row after every bgroup rows (H holds T+1 rows
 // per trajectory, the gate gradients T), i.e. B row = k + k / bgroup.
+constexpr int GT = 64;  // output tile edge
+constexpr int GK = 32;  // k per shared-memory stage
 __global__ void __launch_bounds__(256) enc_gemm_tn(const float* __restrict__ Am, int64_t lda,
                                                    const float* __restrict__ Bm, int64_t ldb, int64_t K, int M,
                                                    int Nn, int64_t kchunk, int bgroup, float* __restrict__ C,
                                                    int ldc) {
-    __shared__ float as[32][33];
-    __shared__ float bs[32][33];
-    const int m0 = blockIdx.x * 32, n0 = blockIdx.y * 32;
+    __shared__ __align__(16) float as[GK][GT];
+    __shared__ __align__(16) float bs[GK][GT];
+    const int m0 = blockIdx.x * GT, n0 = blockIdx.y * GT;
     const int64_t k_begin = (int64_t)blockIdx.z * kchunk;
     const int64_t k_end = min(K, k_begin + kchunk);
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // ty 0..7
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    for (int64_t k0 = k_begin; k0 < k_end; k0 += 32) {
-        for (int r = ty; r < 32; r += 8) {
+    const int tid = threadIdx.x;
+    const int tn = tid & 15, tm = tid >> 4;  // outputs n0 + 4 tn .. +3, m0 + 4 tm .. +3
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+    for (int64_t k0 = k_begin; k0 < k_end; k0 += GK) {
+        for (int e = tid; e < GK * GT; e += 256) {  // coalesced rows of A and B
+            const int r = e / GT, c = e % GT;
             const int64_t k = k0 + r;
-            as[r][tx] = (k < k_end && m0 + tx < M) ? Am[k * lda + m0 + tx] : 0.f;
+            as[r][c] = (k < k_end && m0 + c < M) ? Am[k * lda + m0 + c] : 0.f;
             const int64_t kb = bgroup > 0 ? k + k / bgroup : k;
-            bs[r][tx] = (k < k_end && n0 + tx < Nn) ? Bm[kb * ldb + n0 + tx] : 0.f;
+            bs[r][c] = (k < k_end && n0 + c < Nn) ? Bm[kb * ldb + n0 + c] : 0.f;
         }
         __syncthreads();
 #pragma unroll 8
-        for (int kk = 0; kk < 32; ++kk) {
-            const float bv = bs[kk][tx];
+        for (int kk = 0; kk < GK; ++kk) {
+            const float4 a = *reinterpret_cast<const float4*>(&as[kk][4 * tm]);
+            const float4 b = *reinterpret_cast<const float4*>(&bs[kk][4 * tn]);
+            const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
-            for (int q = 0; q < 4; ++q) acc[q] = fmaf(as[kk][ty + 8 * q], bv, acc[q]);
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int m = m0 + ty + 8 * q, n = n0 + tx;
-        if (m < M && n < Nn) atomicAdd(C + (int64_t)m * ldc + n, acc[q]);
-    }
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int m = m0 + 4 * tm + i, n = n0 + 4 * tn + j;
+            if (m < M && n < Nn) atomicAdd(C + (int64_t)m * ldc + n, acc[i][j]);
+        }
 }
 
 // Column sums: out[n] += sum_k A[k*lda + n] (bias gradients).
@@ -869,9 +884,9 @@ int enc_backward(const float* params, const float* pts, const int64_t* off, cons
     const int64_t K = (int64_t)B * T;
     const int64_t kchunk = 2048;
     const unsigned kz = (unsigned)((K + kchunk - 1) / kchunk);
-    enc_gemm_tn<<<dim3(G3 / 32, C1 / 32, kz), 256, 0, s>>>(w.G, G3, w.A, C1, K, G3, C1, kchunk, 0,
+    enc_gemm_tn<<<dim3(G3 / GT, C1 / GT, kz), 256, 0, s>>>(w.G, G3, w.A, C1, K, G3, C1, kchunk, 0,
                                                            grad + OFF_WIH, C1);  // dWih[j][c] += G . A
-    enc_gemm_tn<<<dim3(G3 / 32, HD / 32, kz), 256, 0, s>>>(w.GH, G3, w.H, HD, K, G3, HD, kchunk, T,
+    enc_gemm_tn<<<dim3(G3 / GT, HD / GT, kz), 256, 0, s>>>(w.GH, G3, w.H, HD, K, G3, HD, kchunk, T,
                                                            grad + OFF_WHH, HD);  // dWhh[j][k] += GH . H[t]
     enc_colsum<<<dim3((G3 + 127) / 128, kz), 128, 0, s>>>(w.G, G3, K, G3, kchunk, grad + OFF_BIH);
     enc_colsum<<<dim3((G3 + 127) / 128, kz), 128, 0, s>>>(w.GH, G3, K, G3, kchunk, grad + OFF_BHH);
