@@ -153,7 +153,7 @@ class SurrogateIndex:
     a ladder whose recall@k reaches the target; if none does within the
     speed budget, queries fall back to the exhaustive search."""
 
-    LADDER = (200, 500, 1000, 2000, 5000, 10000, 20000, 50000)
+    LADDER = (200, 500, 1000, 1500, 2000, 2500, 3000, 4000, 5000, 7000, 10000, 20000, 50000)
 
     # embedding width + 1 (the squared norm), padded to a multiple of 4 floats
     AUG = 132
