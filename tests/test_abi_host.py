@@ -97,7 +97,10 @@ def test_pair_order_groups_shapes():
     assert sorted(o.tolist()) == list(range(1000))
     nr = np.maximum(la, lb)[o]
     blocks = (nr + 7) // 8
-    assert np.all(np.diff(blocks) >= 0)
+    assert np.all(np.diff(blocks) <= 0)  # largest first
+    nc = np.minimum(la, lb)[o]
+    same = np.diff(blocks) == 0
+    assert np.all(np.diff(nc)[same] <= 0)
 
 
 def test_generators_are_seeded_and_shaped():

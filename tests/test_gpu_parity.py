@@ -216,20 +216,26 @@ def test_full_size_all_pairs_properties(oracle_mod, full_set, m):
 @pytest.mark.parametrize("rows", [4, 8, 16])
 def test_long_pairs_wave_kernel_exact(oracle_mod, rows):
     """Pairs whose shorter side exceeds the tile kernel's boundary row
-    (256 points) run one warp per pair; mixed in one batch with short pairs."""
+    (256 points), and pairs longer than 256 points whose one-lane tile loop
+    would exceed 2048 steps (e.g. 2000 x 256 and 600 x 200 at every
+    rows_per_thread, 2000 x 33 at 4 and 8), run one warp per pair; mixed in
+    one batch with short pairs, in the given order and the shape order."""
     O = oracle_mod
     from trajsimimeasures_b200 import datagen as D
-    la = np.array([257, 300, 513, 1000, 2000, 2000, 40, 700, 256, 999, 1, 2000])
-    lb = np.array([300, 257, 600, 1000, 2000, 31, 2000, 1500, 257, 1001, 2000, 1999])
+    la = np.array([257, 300, 513, 1000, 2000, 2000, 40, 700, 256, 999, 1, 2000,
+                   2000, 600, 513, 1999, 1500, 2000, 33, 2000])
+    lb = np.array([300, 257, 600, 1000, 2000, 31, 2000, 1500, 257, 1001, 2000, 1999,
+                   256, 200, 100, 2, 64, 33, 2000, 3])
     pts, off, lens = D._walks(np.random.default_rng(rows), np.concatenate([la, lb]), D.STEP_SIGMA)
     n = len(la)
     ia, ib = np.arange(n), np.arange(n) + n
     for m in (0, 1, 2, 3, 4):
-        got, cnt = run_pairs(m, pts, off, lens, ia, ib, exact=True, rows=rows)
         want, wcnt = O.pairs_idx(O.pairs_f32, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
-        np.testing.assert_array_equal(got, want, err_msg=NAMES[m])
-        if m in (1, 2):
-            np.testing.assert_array_equal(cnt, wcnt)
+        for order in (True, False):
+            got, cnt = run_pairs(m, pts, off, lens, ia, ib, exact=True, rows=rows, order=order)
+            np.testing.assert_array_equal(got, want, err_msg=NAMES[m])
+            if m in (1, 2):
+                np.testing.assert_array_equal(cnt, wcnt)
 
 
 def test_lognormal_batch(oracle_mod):

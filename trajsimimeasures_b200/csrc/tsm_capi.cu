@@ -37,6 +37,7 @@ int cuda_fail(cudaError_t e, const char* what) {
 // on the tile kernel (one thread per pair, a kTileCap-float boundary row per
 // thread); longer ones on the wave kernel (one warp per pair).
 constexpr int kTileCap = 256;
+static_assert(tsm::kHeavyRows >= kTileCap, "a tile-heavy pair must have a side longer than the tile capacity");
 // Matrix mode keeps the query as the tile kernel's columns: its boundary
 // rows (32 per warp) and staged columns must fit one CTA's shared memory.
 constexpr int kMatrixQueryMax = 1400;
@@ -216,16 +217,27 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
         int rc = launch(fn, grid, dim3(threads), smem, args, s);
         if (rc != TSM_OK) return rc;
     }
-    if (max_len <= cap) return TSM_OK;
-    // pairs whose shorter side exceeds cap: one warp each
+    if (max_len <= cap) return TSM_OK;  // (a tile-heavy pair has a side longer than kHeavyRows > kTileCap)
+    // pairs whose shorter side exceeds cap, or whose tile loop would be very long: one warp each
     const void* wfn = exact ? pick_wave_m<true>(measure, R) : pick_wave_m<false>(measure, R);
     int wcap = (max_len + 3) & ~3;
     const int per_warp = tsm::wave_warp_floats(wcap) * 4;
-    int W = (kSmemPerCta / per_warp) < 1 ? 1 : (kSmemPerCta / per_warp);
-    if (W > 4) W = 4;
+    const int W = 4;
     const int smem = W * per_warp;
     if (smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_pairs: wave kernel needs %d bytes", smem);
-    dim3 grid((unsigned)((n + W - 1) / W));
+    // persistent: the GPU's resident warps stride over the pairs
+    cudaError_t e = set_smem(wfn, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaDeviceGetAttribute");
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wfn, 32 * W, smem)) != cudaSuccess)
+        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per_sm < 1) return fail(TSM_ETOOLONG, "tsm_pairs: the wave kernel does not fit on an SM");
+    int64_t blocks = (int64_t)sms * per_sm;
+    if (blocks > (n + W - 1) / W) blocks = (n + W - 1) / W;
+    dim3 grid((unsigned)blocks);
     int tcap = cap;
     void* args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &tcap, &wcap, &ml, (void*)&kp, &out, &out_counts};
     return launch(wfn, grid, dim3(32 * W), smem, args, s);

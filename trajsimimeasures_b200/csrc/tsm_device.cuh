@@ -76,6 +76,17 @@ __device__ __forceinline__ float d2nr(float2 nr, float2 c) {
     return __fmaf_rn(d.y, d.y, __fmul_rn(d.x, d.x));
 }
 
+// Pairs mode: a pair whose longer side exceeds kHeavyRows and whose one-lane
+// tile loop (passes of 2R rows, nc + 1 steps each) would exceed kTileStepMax
+// steps goes to the wave kernel instead: its 32 lanes finish it sooner, and
+// one such pair no longer holds a whole tile launch's tail.
+constexpr int kHeavyRows = 256;
+constexpr int kTileStepMax = 2048;
+template <int R>
+__host__ __device__ __forceinline__ bool tile_heavy(int nr, int nc) {
+    return nr > kHeavyRows && nc > 0 && (int64_t)((nr + 2 * R - 1) / (2 * R)) * (nc + 1) > kTileStepMax;
+}
+
 // Kernel parameters (device copy of tsm_params, pre-digested on the host).
 struct KParams {
     float eps2;        // (float)(eps*eps)

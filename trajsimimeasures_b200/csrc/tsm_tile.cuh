@@ -354,6 +354,7 @@ __device__ __forceinline__ float dp_pair(const float2* __restrict__ rowp, int nr
 
 
 // Pairs mode ------------------------------------------------------------------
+
 // Block = 32*W threads, dynamic shared memory = W*32*cap floats.
 template <int M, int R, bool EXACT>
 __global__ void __launch_bounds__(128) dp_pairs_kernel(
@@ -378,7 +379,7 @@ __global__ void __launch_bounds__(128) dp_pairs_kernel(
     const float2* rowp = a_rows ? a : b;
     const float2* colp = a_rows ? b : a;
     const int nr = a_rows ? na : nb, nc = a_rows ? nb : na;
-    if (nc > cap) return;  // both trajectories longer than cap: the wave kernel's pair
+    if (nc > cap || tile_heavy<R>(nr, nc)) return;  // the wave kernel's pair
     float srow = 0.f, scol = 0.f;
     if constexpr (M == ERP) {
         srow = gapsum<EXACT>(rowp, nr, p);

@@ -1,32 +1,145 @@
-// Wave kernel: one warp per long trajectory pair, a systolic wavefront over
-// the warp's 32 lanes.
+// Wave kernel: one warp per long trajectory pair (pairs mode): the pairs
+// whose shorter side exceeds the tile kernel's boundary-row capacity, and the
+// pairs whose one-lane tile loop would be very long (tile_heavy).
 //
-// The pair's rows (the longer trajectory) are cut into strips of R rows.
-// Lane l owns strips l, l+32, l+64, ...: strip g = 32*m + l in round m.  Lane l
-// computes column j of its round-m strip at step t = m*T + l + j, with the
-// round period T = max(ncols, 32).  Within a round, strip g needs the bottom
-// row of strip g-1 at the same column, which lane l-1 produced one step
-// earlier: it arrives by __shfl_up_sync.  Lane 0 of round m needs the bottom
-// row of strip 32m-1 (lane 31, round m-1), produced T-31 >= 1 steps earlier:
-// lane 31 writes it to a one-row ring in shared memory and lane 0 reads it
-// back, so consecutive rounds overlap with no pipeline drain.  The column
-// trajectory is staged in shared memory once per pair; each lane keeps its R
-// row points and R DP values in registers and prefetches the points of its
-// next strip one round ahead.
+// Persistent: a grid sized to the GPU's resident warps; in round i the nw
+// warps take pairs i nw .. i nw + nw - 1 of the processing order, warp w the
+// w-th of them in even rounds and the (nw-1-w)-th in odd ones (a snake, so
+// that in the largest-first order no warp collects the largest pair of every
+// round).  A warp tests 32 of its pairs at once (one per lane), keeps the wave
+// pairs by a ballot and runs them one after another; every other pair is the
+// tile kernel's.
 //
-// Per step and lane: R cells of arithmetic, one shuffle, one shared-memory
-// column load, and (lanes 0 and 31) one ring access.  The only idle steps are
-// the 31-step ramps at the start and end of a pair, which is why the tile
-// kernel (one thread per pair) takes the short pairs and this kernel the
-// pairs whose shorter side exceeds the tile kernel's boundary-row capacity.
+// A pair's rows are swept in super-strips of 32 R rows: lane l holds rows
+// l R .. l R + R - 1 of the strip in registers and computes column j at step
+// l + j, taking its top value from lane l-1 (one step earlier) by a shuffle;
+// lane 0 reads the bottom row of the strip above from a ring in shared
+// memory, which lane 31 rewrites 31 steps behind.  The column points come
+// through the L1 cache, loaded one step ahead (the warp reads 32 consecutive
+// points per step); the ring is the only per-column shared memory.  The step
+// loop is unrolled by two with the R values alternating between two register
+// arrays, and the rows of the next strip are prefetched one strip ahead.  Per
+// step and lane: R cells, one shuffle, one column load, and (lanes 0 and 31)
+// one ring access; a strip costs nc + 31 steps.
 #pragma once
 
 #include "tsm_device.cuh"
 
 namespace tsm {
 
-// Per-warp shared memory of the wave kernel, in floats, for column capacity cap.
-__host__ __device__ constexpr int wave_warp_floats(int cap) { return 4 * cap + cap; }
+// Per-warp shared memory of the wave kernel, in floats, for column capacity
+// cap: the ring (one float per point of the longer trajectory, which also
+// serves as scratch for the ERP gap sums).
+__host__ __device__ constexpr int wave_warp_floats(int cap) { return cap; }
+
+// DP of one wave pair (rows = the longer trajectory, nr >= nc >= 1) by the
+// calling warp; writes out[k] (and counts[k]).
+template <int M, int R, bool EXACT>
+__device__ __forceinline__ void wave_pair(const float2* __restrict__ rowp, const float2* __restrict__ colp, int nr,
+                                          int nc, int na, int nb, float* ring, int lane, const KParams& p,
+                                          float* __restrict__ out_k, int32_t* __restrict__ count_k) {
+    using C = typename CellOf<M, EXACT>::type;
+    float srow = 0.f, scol = 0.f;
+    if constexpr (M == ERP) {
+        // column gap distances into the ring, summed in column order by lane 0
+        for (int j = lane; j < nc; j += 32) {
+            const float2 v = __ldg(colp + j);
+            ring[j] = gapdist<EXACT>(v.x, v.y, p);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            double s = 0.0;
+            for (int j = 0; j < nc; ++j) s = __dadd_rn(s, (double)ring[j]);
+            scol = (float)s;
+            srow = gapsum<EXACT>(rowp, nr, p);
+        }
+        srow = __shfl_sync(0xffffffffu, srow, 0);
+        scol = __shfl_sync(0xffffffffu, scol, 0);
+        __syncwarp();
+    }
+    for (int j = lane; j < nc; j += 32) ring[j] = C::topb(scol, j);
+
+    constexpr int SS = 32 * R;
+    const int n_ss = (nr + SS - 1) / SS;
+    const int span = nc + 31;
+    const int last_u = ((nr - 1) % SS) / R, last_r = (nr - 1) % R;
+    float px[R], py[R];  // this lane's rows of the next strip
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const float2 q = __ldg(rowp + min(lane * R + r, nr - 1));
+        px[r] = q.x;
+        py[r] = q.y;
+    }
+    float dlast = 0.f;
+    __syncwarp();
+    for (int ss = 0; ss < n_ss; ++ss) {
+        const int row0 = ss * SS + lane * R;
+        const bool on = row0 < nr;
+        float2 rn[R];  // negated row points (d2nr)
+        float rg[R], DA[R], DB[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            rn[r] = make_float2(-px[r], -py[r]);
+            rg[r] = C::kGap ? gapdist<EXACT>(px[r], py[r], p) : 0.f;
+            DA[r] = DB[r] = C::rowb(srow, row0 + r);
+        }
+        if (on && ss + 1 < n_ss) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const float2 q = __ldg(rowp + min(row0 + SS + r, nr - 1));
+                px[r] = q.x;
+                py[r] = q.y;
+            }
+        }
+        float diag = (row0 == 0) ? C::corner() : C::rowb(srow, row0 - 1);
+        float bottom = 0.f;
+        float2 cnext = __ldg(colp);  // column of step 0 (lane 0's; the other lanes are idle at step 0)
+        auto step = [&](const float (&Din)[R], float (&Dout)[R], int s) {
+            const float2 c = cnext;
+            cnext = __ldg(colp + min(max(s + 1 - lane, 0), nc - 1));
+            const float from_left = __shfl_up_sync(0xffffffffu, bottom, 1);
+            const int j = s - lane;
+            if (on && (unsigned)j < (unsigned)nc) {
+                const float top = (lane == 0) ? ring[j] : from_left;
+                const float cg = C::kGap ? gapdist<EXACT>(c.x, c.y, p) : 0.f;
+                float up = top, dg = diag;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const float left = Din[r];
+                    const float nv = C::cell(dg, up, left, d2nr<C::kPackedSmem>(rn[r], c), rg[r], cg, p.eps2);
+                    Dout[r] = nv;
+                    dg = left;
+                    up = nv;
+                }
+                diag = top;
+                bottom = up;
+                if (lane == 31) ring[j] = up;
+            }
+            __syncwarp();
+        };
+        int s = 0;
+        for (; s + 1 < span; s += 2) {
+            step(DA, DB, s);
+            step(DB, DA, s + 1);
+        }
+        if (s < span) step(DA, DB, s);
+        if (on && ss == n_ss - 1 && lane == last_u) {
+            // the lane's last column nc-1 was step lane + nc - 1: even steps wrote DB, odd ones DA
+            const bool in_b = ((lane + nc - 1) & 1) == 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (r == last_r) dlast = in_b ? DB[r] : DA[r];
+        }
+    }
+    if (lane == last_u) {
+        float o;
+        int c;
+        finalize<M>(dlast, na, nb, o, c);
+        *out_k = o;
+        if (count_k) *count_k = c;
+    }
+    __syncwarp();  // the ring is free for the warp's next pair
+}
 
 template <int M, int R, bool EXACT>
 __global__ void __launch_bounds__(128) dp_wave_kernel(
@@ -34,115 +147,39 @@ __global__ void __launch_bounds__(128) dp_wave_kernel(
     const int64_t* __restrict__ off_b, const int32_t* __restrict__ len_b, const int32_t* __restrict__ order,
     int64_t n, int tile_cap, int cap, int max_len, KParams p, float* __restrict__ out,
     int32_t* __restrict__ counts) {
-    using C = typename CellOf<M, EXACT>::type;
     extern __shared__ float smem[];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
-    float4* cols = reinterpret_cast<float4*>(smem + w * wave_warp_floats(cap));
-    float* ring = smem + w * wave_warp_floats(cap) + 4 * cap;
-    const int64_t t_pair = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
-    if (t_pair >= n) return;
-    const int64_t k = order ? (int64_t)order[t_pair] : t_pair;
-    const int na = len_a[k], nb = len_b[k];
+    float* ring = smem + w * wave_warp_floats(cap);
+    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
+    const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
     const bool count = (M == EDR || M == LCSS) && counts != nullptr;
-    if (na < 0 || nb < 0 || na > max_len || nb > max_len) {
-        if (lane == 0) {
-            out[k] = CUDART_NAN_F;
-            if (count) counts[k] = -1;
-        }
-        return;
-    }
-    const bool a_rows = na >= nb;
-    const int nr = a_rows ? na : nb, nc = a_rows ? nb : na;
-    if (nc <= tile_cap) return;  // the tile kernel's pair
-    const float2* rowp = pts + (a_rows ? off_a[k] : off_b[k]);
-    const float2* colp = pts + (a_rows ? off_b[k] : off_a[k]);
-
-    for (int j = lane; j < nc; j += 32) {
-        const float2 v = __ldg(colp + j);
-        cols[j] = make_float4(v.x, v.y, C::kGap ? gapdist<EXACT>(v.x, v.y, p) : 0.f, 0.f);
-    }
-    __syncwarp();
-    float srow = 0.f, scol = 0.f;
-    if constexpr (M == ERP) {
-        if (lane == 0) {
-            double s = 0.0;
-            for (int j = 0; j < nc; ++j) s = __dadd_rn(s, (double)cols[j].z);
-            scol = (float)s;
-            srow = gapsum<EXACT>(rowp, nr, p);
-        }
-        srow = __shfl_sync(0xffffffffu, srow, 0);
-        scol = __shfl_sync(0xffffffffu, scol, 0);
-    }
-
-    const int n_strips = (nr + R - 1) / R;
-    const int T = nc > 32 ? nc : 32;
-    const int last_strip = n_strips - 1;
-    const int total = (last_strip / 32) * T + (last_strip % 32) + nc;  // steps until the last cell
-    const int res_lane = last_strip % 32;
-    const int res_r = (nr - 1) - last_strip * R;
-
-    float rx[R], ry[R], rg[R], D[R];
-    float px[R], py[R];  // prefetched points of this lane's next strip
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const float2 q = __ldg(rowp + min(lane * R + r, nr - 1));
-        px[r] = q.x;
-        py[r] = q.y;
-        rx[r] = ry[r] = rg[r] = D[r] = 0.f;
-    }
-    float diag = 0.f, bottom = 0.f, dlast = 0.f;
-    for (int t = 0; t < total; ++t) {
-        const int tau = t - lane;
-        const int m = tau >= 0 ? tau / T : 0;
-        const int j = tau - m * T;
-        const int g = 32 * m + lane;
-        const bool act = tau >= 0 && j < nc && g < n_strips;
-        const float from_left = __shfl_up_sync(0xffffffffu, bottom, 1);
-        if (act) {
-            if (j == 0) {  // start strip g: take the prefetched points, prefetch strip g+32
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    rx[r] = px[r];
-                    ry[r] = py[r];
-                    rg[r] = C::kGap ? gapdist<EXACT>(px[r], py[r], p) : 0.f;
-                    D[r] = C::rowb(srow, g * R + r);
-                    const float2 q = __ldg(rowp + min((g + 32) * R + r, nr - 1));
-                    px[r] = q.x;
-                    py[r] = q.y;
-                }
-                diag = (g == 0) ? C::corner() : C::rowb(srow, g * R - 1);
-            }
-            float top;
-            if (lane == 0) top = (m == 0) ? C::topb(scol, j) : ring[j];
-            else top = from_left;
-            const float4 c = cols[j];
-            float up = top, dg = diag;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const float left = D[r];
-                const float nv = C::cell(dg, up, left, d2f(rx[r], ry[r], c.x, c.y), rg[r], c.z, p.eps2);
-                D[r] = nv;
-                dg = left;
-                up = nv;
-            }
-            diag = top;
-            bottom = up;
-            if (lane == 31) ring[j] = up;
-            if (g == last_strip && j == nc - 1) {
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-                    if (r == res_r) dlast = D[r];
+    for (int64_t i0 = 0; i0 * nw < n; i0 += 32) {
+        const int64_t i = i0 + lane;
+        const int64_t t = i * nw + ((i & 1) ? nw - 1 - gw : gw);
+        int64_t k = 0;
+        bool mine = false;
+        if (t < n) {
+            k = order ? (int64_t)order[t] : t;
+            const int na = len_a[k], nb = len_b[k];
+            // pairs with bad lengths are flagged by the tile kernel
+            if (na >= 0 && nb >= 0 && na <= max_len && nb <= max_len) {
+                const int nr = max(na, nb), nc = min(na, nb);
+                mine = nc > tile_cap || tile_heavy<R>(nr, nc);
             }
         }
-        __syncwarp();
-    }
-    if (lane == res_lane) {
-        float o;
-        int c;
-        finalize<M>(dlast, na, nb, o, c);
-        out[k] = o;
-        if (count) counts[k] = c;
+        unsigned todo = __ballot_sync(0xffffffffu, mine);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int64_t kk = __shfl_sync(0xffffffffu, k, src);
+            const int na = len_a[kk], nb = len_b[kk];
+            const bool a_rows = na >= nb;
+            const float2* rowp = pts + (a_rows ? off_a[kk] : off_b[kk]);
+            const float2* colp = pts + (a_rows ? off_b[kk] : off_a[kk]);
+            wave_pair<M, R, EXACT>(rowp, colp, a_rows ? na : nb, a_rows ? nb : na, na, nb, ring, lane, p, out + kk,
+                                   count ? counts + kk : nullptr);
+        }
     }
 }
 

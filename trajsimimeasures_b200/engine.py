@@ -130,12 +130,14 @@ class TrajSet:
 def pair_order(len_a: np.ndarray, len_b: np.ndarray, rows=DEFAULT_ROWS) -> np.ndarray:
     """Processing order for a paired batch: pairs grouped by (row blocks,
     columns) of their DP so that a warp's 32 threads run loops of near-equal
-    trip counts.  Rows are the longer trajectory, columns the shorter."""
+    trip counts, the largest first (the longest loops start at once instead of
+    forming the launch's tail).  Rows are the longer trajectory, columns the
+    shorter."""
     la = np.asarray(len_a, dtype=np.int64)
     lb = np.asarray(len_b, dtype=np.int64)
     nr, nc = np.maximum(la, lb), np.minimum(la, lb)
     key = ((nr + rows - 1) // rows) * 65536 + nc
-    return np.argsort(key, kind="stable").astype(np.int32)
+    return np.argsort(-key, kind="stable").astype(np.int32)
 
 
 # ---------------------------------------------------------------------------

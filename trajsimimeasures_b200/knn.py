@@ -113,12 +113,12 @@ def knn_rerank(Q: TrajSet, D: TrajSet, cand: torch.Tensor, k=10, measure="dtw", 
 
 def shape_order(len_a: torch.Tensor, len_b: torch.Tensor, rows=DEFAULT_ROWS) -> torch.Tensor:
     """engine.pair_order on the device: the pairs ordered by (row blocks,
-    columns) of their DP, so a warp's 32 lanes run loops of equal trip counts
-    (int32 processing order for tsm_pairs)."""
+    columns) of their DP, the largest first, so a warp's 32 lanes run loops of
+    equal trip counts (int32 processing order for tsm_pairs)."""
     la, lb = len_a.long(), len_b.long()
     nr, nc = torch.maximum(la, lb), torch.minimum(la, lb)
     key = ((nr + rows - 1) // rows) * 65536 + nc
-    return torch.argsort(key, stable=True).to(torch.int32)
+    return torch.argsort(-key, stable=True).to(torch.int32)
 
 
 def recall_at_k(approx_idx, exact_idx) -> float:
