@@ -91,6 +91,11 @@ int32_t tsm_max_supported_len(void);
  *   out     float32 [n_pairs]
  *   out_counts int32 [n_pairs] or NULL: EDR/LCSS edit/match counts before
  *           normalisation (ignored for other measures)
+ * When max_len exceeds 256, the long pairs' kernel runs on a stream of the
+ * calling thread forked from `stream` (an event record / wait on each side;
+ * the side stream and its two events are created once per thread and
+ * device).  `stream` waits for it before the call returns, so later work on
+ * `stream`, and a graph captured from it, see the complete result.
  */
 int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t* len_a,
               const int64_t* off_b, const int32_t* len_b, const int32_t* order, int64_t n_pairs,

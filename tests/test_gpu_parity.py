@@ -238,6 +238,93 @@ def test_long_pairs_wave_kernel_exact(oracle_mod, rows):
                 np.testing.assert_array_equal(cnt, wcnt)
 
 
+def _long_batch(seed, n=600):
+    from trajsimimeasures_b200 import datagen as D
+    rng = np.random.default_rng(seed)
+    la = rng.integers(1, 1200, n)
+    lb = rng.integers(1, 300, n)
+    pts, off, lens = D._walks(rng, np.concatenate([la, lb]), D.STEP_SIGMA)
+    return pts, off, lens, np.arange(n), np.arange(n) + n
+
+
+def _pairs_dev(pts, off, lens, ia, ib):
+    from trajsimimeasures_b200.engine import pair_order
+    la, lb = lens[ia], lens[ib]
+    return (_dev(pts, np.float32), _dev(off[ia], np.int64), _dev(la, np.int32), _dev(off[ib], np.int64),
+            _dev(lb, np.int32)), int(max(la.max(), lb.max())), _dev(pair_order(la, lb), np.int32)
+
+
+def test_long_pairs_stream_order(oracle_mod):
+    """The long-pair kernel runs on a forked side stream: work enqueued on the
+    caller's stream right after tsm_pairs (no host sync) sees every result."""
+    from trajsimimeasures_b200.engine import pairs_raw
+    pts, off, lens, ia, ib = _long_batch(11)
+    T, mx, o = _pairs_dev(pts, off, lens, ia, ib)
+    want, _ = oracle_mod.pairs_idx(oracle_mod.pairs_f32, 0, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        for rep in range(3):
+            out = torch.full((len(ia),), -7.0, device="cuda")
+            pairs_raw(0, *T, mx, out=out, order=o, exact=True, stream=st)
+            snap = out.clone()  # on st, ordered after tsm_pairs
+            snap_host = snap.cpu()
+            np.testing.assert_array_equal(snap_host.numpy(), want)
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("fresh_thread", [False, True])
+def test_long_pairs_graph_capture(oracle_mod, fresh_thread):
+    """tsm_pairs with long pairs inside a CUDA graph capture: on a thread that
+    already has its side stream (fork / join captured into the graph), and on
+    a new thread whose first call is the captured one (everything on the
+    captured stream)."""
+    import threading
+    from trajsimimeasures_b200.engine import pairs_raw
+    pts, off, lens, ia, ib = _long_batch(12)
+    T, mx, o = _pairs_dev(pts, off, lens, ia, ib)
+    want, wcnt = oracle_mod.pairs_idx(oracle_mod.pairs_f32, 1, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+    res = {}
+
+    def body():
+        out = torch.full((len(ia),), -7.0, device="cuda")
+        cnt = torch.full((len(ia),), -7, dtype=torch.int32, device="cuda")
+        if not fresh_thread:  # creates this thread's side stream outside the capture
+            pairs_raw(1, *T, mx, out=out, counts=cnt, order=o, eps=EPS, exact=True)
+            torch.cuda.synchronize()
+        s = torch.cuda.Stream()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                pairs_raw(1, *T, mx, out=out, counts=cnt, order=o, eps=EPS, exact=True, stream=s)
+        for _ in range(2):
+            out.fill_(-7.0)
+            cnt.fill_(-7)
+            g.replay()
+            torch.cuda.synchronize()
+            res.setdefault("out", []).append(out.cpu().numpy().copy())
+            res.setdefault("cnt", []).append(cnt.cpu().numpy().copy())
+        del g
+
+    if fresh_thread:
+        err = []
+
+        def run():
+            try:
+                body()
+            except BaseException as e:  # surfaced in the test thread
+                err.append(e)
+        t = threading.Thread(target=run)
+        t.start()
+        t.join()
+        if err:
+            raise err[0]
+    else:
+        body()
+    for got, cnt in zip(res["out"], res["cnt"]):
+        np.testing.assert_array_equal(got, want)
+        np.testing.assert_array_equal(cnt, wcnt)
+
+
 def test_lognormal_batch(oracle_mod):
     """20k pairs of the uneven (lognormal, clipped to [10, 2000]) workload."""
     O = oracle_mod

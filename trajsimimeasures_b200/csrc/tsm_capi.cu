@@ -2,7 +2,8 @@
 //
 // Host-side launch logic only: argument checks, kernel selection by
 // (measure, rows-per-thread, exact), shared-memory sizing, launch on the
-// caller's stream.  No device allocation happens here.
+// caller's stream (tsm_pairs' long-pair kernel on a side stream forked from
+// and joined back to it).  No device allocation happens here.
 #include <cuda_runtime.h>
 
 #include <cstdarg>
@@ -163,6 +164,44 @@ int launch(const void* fn, dim3 grid, dim3 block, int smem, void** args, cudaStr
     return TSM_OK;
 }
 
+// The calling thread's side stream (and fork / join events) on device dev,
+// created on first use.  nullptr when they cannot be made, and when they do
+// not exist yet while the caller's stream is being captured into a graph
+// (creating them then could invalidate the capture): the caller then
+// launches everything on its own stream.
+struct SideStream {
+    cudaStream_t st = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    bool failed = false;
+};
+constexpr int kMaxDevices = 64;
+thread_local SideStream g_side[kMaxDevices];
+
+SideStream* side_stream(int dev, cudaStream_t caller) {
+    if (dev < 0 || dev >= kMaxDevices) return nullptr;
+    SideStream& r = g_side[dev];
+    if (r.st) return &r;
+    if (r.failed) return nullptr;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(caller, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    SideStream t;
+    if (cudaStreamCreateWithFlags(&t.st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&t.fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&t.join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (t.join) cudaEventDestroy(t.join);
+        if (t.fork) cudaEventDestroy(t.fork);
+        if (t.st) cudaStreamDestroy(t.st);
+        r.failed = true;
+        return nullptr;
+    }
+    r = t;
+    return &r;
+}
+
 }  // namespace
 
 // Internal (hidden, not part of the ABI): lets other translation units of the
@@ -208,39 +247,52 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
     const void* fn = exact ? pick_dp_m<true>(measure, false, R) : pick_dp_m<false>(measure, false, R);
     if (!fn) return fail(TSM_EINVAL, "tsm_pairs: rows_per_thread must be 4, 8 or 16");
     int cap = max_len < 1 ? 1 : (max_len < kTileCap ? max_len : kTileCap);
-    {
-        const int W = warps_for(cap, 0);
-        const int threads = 32 * W;
-        const int smem = W * 32 * cap * 4;
-        dim3 grid((unsigned)((n + threads - 1) / threads));
-        void* args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &cap, &ml, (void*)&kp, &out, &out_counts};
-        int rc = launch(fn, grid, dim3(threads), smem, args, s);
-        if (rc != TSM_OK) return rc;
-    }
-    if (max_len <= cap) return TSM_OK;  // (a tile-heavy pair has a side longer than kHeavyRows > kTileCap)
-    // pairs whose shorter side exceeds cap, or whose tile loop would be very long: one warp each
+    const int tW = warps_for(cap, 0);
+    const int t_smem = tW * 32 * cap * 4;
+    const dim3 t_grid((unsigned)((n + 32 * tW - 1) / (32 * tW)));
+    void* t_args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &cap, &ml, (void*)&kp, &out, &out_counts};
+    // (a tile-heavy pair has a side longer than kHeavyRows >= kTileCap)
+    if (max_len <= cap) return launch(fn, t_grid, dim3(32 * tW), t_smem, t_args, s);
+
+    // pairs whose shorter side exceeds cap, or whose tile loop would be very
+    // long: the persistent wave kernel, one warp per pair
     const void* wfn = exact ? pick_wave_m<true>(measure, R) : pick_wave_m<false>(measure, R);
     int wcap = (max_len + 3) & ~3;
-    const int per_warp = tsm::wave_warp_floats(wcap) * 4;
     const int W = 4;
-    const int smem = W * per_warp;
-    if (smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_pairs: wave kernel needs %d bytes", smem);
-    // persistent: the GPU's resident warps stride over the pairs
-    cudaError_t e = set_smem(wfn, smem);
+    const int w_smem = W * tsm::wave_warp_floats(wcap) * 4;
+    if (w_smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_pairs: wave kernel needs %d bytes", w_smem);
+    cudaError_t e = set_smem(wfn, w_smem);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
     int dev = 0, sms = 0, per_sm = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
         return cuda_fail(e, "cudaDeviceGetAttribute");
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wfn, 32 * W, smem)) != cudaSuccess)
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wfn, 32 * W, w_smem)) != cudaSuccess)
         return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (per_sm < 1) return fail(TSM_ETOOLONG, "tsm_pairs: the wave kernel does not fit on an SM");
     int64_t blocks = (int64_t)sms * per_sm;
     if (blocks > (n + W - 1) / W) blocks = (n + W - 1) / W;
-    dim3 grid((unsigned)blocks);
+    const dim3 w_grid((unsigned)blocks);
     int tcap = cap;
-    void* args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &tcap, &wcap, &ml, (void*)&kp, &out, &out_counts};
-    return launch(wfn, grid, dim3(32 * W), smem, args, s);
+    void* w_args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &tcap, &wcap, &ml, (void*)&kp, &out, &out_counts};
+
+    // The two kernels write disjoint outputs: the wave kernel (few warps with
+    // long, uneven loops) runs on a side stream forked from the caller's, so
+    // the tile kernel's blocks fill the SMs its warps leave idle; the caller's
+    // stream then waits for both.
+    SideStream* side = side_stream(dev, s);
+    if (!side) {
+        int rc = launch(fn, t_grid, dim3(32 * tW), t_smem, t_args, s);
+        return rc != TSM_OK ? rc : launch(wfn, w_grid, dim3(32 * W), w_smem, w_args, s);
+    }
+    if ((e = cudaEventRecord(side->fork, s)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if ((e = cudaStreamWaitEvent(side->st, side->fork, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+    int rc = launch(wfn, w_grid, dim3(32 * W), w_smem, w_args, side->st);
+    const int rc_tile = launch(fn, t_grid, dim3(32 * tW), t_smem, t_args, s);
+    // join even after a failed launch, so that the side stream is not left forked from a capture
+    if ((e = cudaEventRecord(side->join, side->st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if ((e = cudaStreamWaitEvent(s, side->join, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+    return rc != TSM_OK ? rc : rc_tile;
 }
 
 namespace {
