@@ -251,7 +251,10 @@ struct LowerFirst<LCSS, SmemCols> {
 // so no register copies are needed.  A final pass of at most R rows uses one
 // block.  (Packing the two blocks into FP32x2 instructions was measured
 // slower: assembling the pairs around the scalar min/max costs more than the
-// packed arithmetic saves.)
+// packed arithmetic saves.  Packing only the squared distances, with the row
+// points held as (upper, lower) pairs and one column pair per step, was
+// measured too: all-pairs 2000 x 2000 DTW 15.25 -> 19.1 ms, Frechet 12.37 ->
+// 17.6 ms, ERP 18.86 -> 23.96 ms on B200, bit-identical results.)
 template <int M, int R, bool EXACT, class Cols>
 __device__ __forceinline__ float dp_pair_prefetch(const float2* __restrict__ rowp, int nr, const Cols& cols,
                                                   int nc, float* buf, const KParams& p, float srow, float scol) {
