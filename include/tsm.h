@@ -91,7 +91,8 @@ int32_t tsm_max_supported_len(void);
  *   out     float32 [n_pairs]
  *   out_counts int32 [n_pairs] or NULL: EDR/LCSS edit/match counts before
  *           normalisation (ignored for other measures)
- * When max_len exceeds 256, the long pairs' kernel runs on a stream of the
+ * When max_len exceeds 256 (Hausdorff: when max_len^2 exceeds 2^17), the
+ * long pairs' kernel runs on a stream of the
  * calling thread forked from `stream` (an event record / wait on each side;
  * the side stream and its two events are created once per thread and
  * device).  `stream` waits for it before the call returns, so later work on

@@ -218,8 +218,9 @@ def test_long_pairs_wave_kernel_exact(oracle_mod, rows):
     """Pairs whose shorter side exceeds the tile kernel's boundary row
     (256 points), and pairs longer than 256 points whose one-lane tile loop
     would exceed 2048 steps (e.g. 2000 x 256 and 600 x 200 at every
-    rows_per_thread, 2000 x 33 at 4 and 8), run one warp per pair; mixed in
-    one batch with short pairs, in the given order and the shape order."""
+    rows_per_thread, 2000 x 33 at 4 and 8), run one warp per pair; so do the
+    Hausdorff pairs of more than 2^17 point products.  Mixed in one batch with
+    short pairs, in the given order and the shape order."""
     O = oracle_mod
     from trajsimimeasures_b200 import datagen as D
     la = np.array([257, 300, 513, 1000, 2000, 2000, 40, 700, 256, 999, 1, 2000,
@@ -229,7 +230,7 @@ def test_long_pairs_wave_kernel_exact(oracle_mod, rows):
     pts, off, lens = D._walks(np.random.default_rng(rows), np.concatenate([la, lb]), D.STEP_SIGMA)
     n = len(la)
     ia, ib = np.arange(n), np.arange(n) + n
-    for m in (0, 1, 2, 3, 4):
+    for m in (0, 1, 2, 3, 4, 5):
         want, wcnt = O.pairs_idx(O.pairs_f32, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
         for order in (True, False):
             got, cnt = run_pairs(m, pts, off, lens, ia, ib, exact=True, rows=rows, order=order)
@@ -260,15 +261,16 @@ def test_long_pairs_stream_order(oracle_mod):
     from trajsimimeasures_b200.engine import pairs_raw
     pts, off, lens, ia, ib = _long_batch(11)
     T, mx, o = _pairs_dev(pts, off, lens, ia, ib)
-    want, _ = oracle_mod.pairs_idx(oracle_mod.pairs_f32, 0, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
     st = torch.cuda.Stream()
-    with torch.cuda.stream(st):
-        for rep in range(3):
-            out = torch.full((len(ia),), -7.0, device="cuda")
-            pairs_raw(0, *T, mx, out=out, order=o, exact=True, stream=st)
-            snap = out.clone()  # on st, ordered after tsm_pairs
-            snap_host = snap.cpu()
-            np.testing.assert_array_equal(snap_host.numpy(), want)
+    for m in (0, 5):  # DTW; Hausdorff (its own long-pair kernel)
+        want, _ = oracle_mod.pairs_idx(oracle_mod.pairs_f32, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+        with torch.cuda.stream(st):
+            for rep in range(3):
+                out = torch.full((len(ia),), -7.0, device="cuda")
+                pairs_raw(m, *T, mx, out=out, order=o, exact=True, stream=st)
+                snap = out.clone()  # on st, ordered after tsm_pairs
+                snap_host = snap.cpu()
+                np.testing.assert_array_equal(snap_host.numpy(), want)
     torch.cuda.synchronize()
 
 

@@ -147,6 +147,15 @@ const void* haus_fn(bool matrix) {
     return matrix ? (const void*)&tsm::hausdorff_matrix_kernel<R, E> : (const void*)&tsm::hausdorff_pairs_kernel<R, E>;
 }
 
+const void* pick_haus_wave(int R, bool exact) {
+    switch (R) {
+        case 4: return exact ? (const void*)&tsm::hausdorff_wave_kernel<4, true> : (const void*)&tsm::hausdorff_wave_kernel<4, false>;
+        case 8: return exact ? (const void*)&tsm::hausdorff_wave_kernel<8, true> : (const void*)&tsm::hausdorff_wave_kernel<8, false>;
+        case 16: return exact ? (const void*)&tsm::hausdorff_wave_kernel<16, true> : (const void*)&tsm::hausdorff_wave_kernel<16, false>;
+        default: return nullptr;
+    }
+}
+
 const void* pick_haus(bool matrix, int R, bool exact) {
     switch (R) {
         case 4: return exact ? haus_fn<4, true>(matrix) : haus_fn<4, false>(matrix);
@@ -202,6 +211,49 @@ SideStream* side_stream(int dev, cudaStream_t caller) {
     return &r;
 }
 
+// Grid of a persistent kernel: the blocks that fit on the device at once
+// (at most max_blocks).
+int persistent_grid(const char* who, const void* fn, int threads, int smem, int64_t max_blocks, dim3& grid,
+                    int& dev) {
+    cudaError_t e = set_smem(fn, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    int sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaDeviceGetAttribute");
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem)) != cudaSuccess)
+        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per_sm < 1) return fail(TSM_ETOOLONG, "%s: the long-pair kernel does not fit on an SM", who);
+    int64_t blocks = (int64_t)sms * per_sm;
+    if (blocks > max_blocks) blocks = max_blocks;
+    grid = dim3((unsigned)blocks);
+    return TSM_OK;
+}
+
+// tsm_pairs' two kernels, which write disjoint outputs: `main` (the short
+// pairs, as a callable taking the stream) on the caller's stream and the
+// long-pair kernel on the calling thread's side stream, forked from and
+// joined back to the caller's; on the caller's stream one after the other
+// when there is no side stream.
+template <class Main>
+int launch_with_side(Main main, const void* wfn, dim3 w_grid, dim3 w_block, int w_smem, void** w_args,
+                     cudaStream_t s, int dev) {
+    SideStream* side = side_stream(dev, s);
+    if (!side) {
+        const int rc = main(s);
+        return rc != TSM_OK ? rc : launch(wfn, w_grid, w_block, w_smem, w_args, s);
+    }
+    cudaError_t e;
+    if ((e = cudaEventRecord(side->fork, s)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if ((e = cudaStreamWaitEvent(side->st, side->fork, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+    const int rc = launch(wfn, w_grid, w_block, w_smem, w_args, side->st);
+    const int rc_main = main(s);
+    // join even after a failed launch, so that the side stream is not left forked from a capture
+    if ((e = cudaEventRecord(side->join, side->st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if ((e = cudaStreamWaitEvent(s, side->join, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+    return rc != TSM_OK ? rc : rc_main;
+}
+
 }  // namespace
 
 // Internal (hidden, not part of the ABI): lets other translation units of the
@@ -241,7 +293,16 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
         const int threads = 128;
         dim3 grid((unsigned)((n + threads - 1) / threads));
         void* args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &ml, &out};
-        return launch(fn, grid, dim3(threads), 0, args, s);
+        if ((int64_t)max_len * max_len <= tsm::kHausWarpCells) return launch(fn, grid, dim3(threads), 0, args, s);
+        // long pairs: one warp each, persistent, on the side stream
+        const void* wfn = pick_haus_wave(R, exact);
+        dim3 w_grid;
+        int dev = 0;
+        int rc = persistent_grid("tsm_pairs", wfn, threads, 0, (n + 3) / 4, w_grid, dev);
+        if (rc != TSM_OK) return rc;
+        void* w_args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &ml, &out};
+        return launch_with_side([&](cudaStream_t st) { return launch(fn, grid, dim3(threads), 0, args, st); }, wfn,
+                                w_grid, dim3(threads), 0, w_args, s, dev);
     }
     if (max_len > kMaxLen) return fail(TSM_ETOOLONG, "tsm_pairs: max_len %d > %d", max_len, kMaxLen);
     const void* fn = exact ? pick_dp_m<true>(measure, false, R) : pick_dp_m<false>(measure, false, R);
@@ -261,38 +322,16 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
     const int W = 4;
     const int w_smem = W * tsm::wave_warp_floats(wcap) * 4;
     if (w_smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_pairs: wave kernel needs %d bytes", w_smem);
-    cudaError_t e = set_smem(wfn, w_smem);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-    int dev = 0, sms = 0, per_sm = 0;
-    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
-        return cuda_fail(e, "cudaDeviceGetAttribute");
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wfn, 32 * W, w_smem)) != cudaSuccess)
-        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (per_sm < 1) return fail(TSM_ETOOLONG, "tsm_pairs: the wave kernel does not fit on an SM");
-    int64_t blocks = (int64_t)sms * per_sm;
-    if (blocks > (n + W - 1) / W) blocks = (n + W - 1) / W;
-    const dim3 w_grid((unsigned)blocks);
+    dim3 w_grid;
+    int dev = 0;
+    int rc = persistent_grid("tsm_pairs", wfn, 32 * W, w_smem, (n + W - 1) / W, w_grid, dev);
+    if (rc != TSM_OK) return rc;
     int tcap = cap;
     void* w_args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &tcap, &wcap, &ml, (void*)&kp, &out, &out_counts};
-
-    // The two kernels write disjoint outputs: the wave kernel (few warps with
-    // long, uneven loops) runs on a side stream forked from the caller's, so
-    // the tile kernel's blocks fill the SMs its warps leave idle; the caller's
-    // stream then waits for both.
-    SideStream* side = side_stream(dev, s);
-    if (!side) {
-        int rc = launch(fn, t_grid, dim3(32 * tW), t_smem, t_args, s);
-        return rc != TSM_OK ? rc : launch(wfn, w_grid, dim3(32 * W), w_smem, w_args, s);
-    }
-    if ((e = cudaEventRecord(side->fork, s)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
-    if ((e = cudaStreamWaitEvent(side->st, side->fork, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
-    int rc = launch(wfn, w_grid, dim3(32 * W), w_smem, w_args, side->st);
-    const int rc_tile = launch(fn, t_grid, dim3(32 * tW), t_smem, t_args, s);
-    // join even after a failed launch, so that the side stream is not left forked from a capture
-    if ((e = cudaEventRecord(side->join, side->st)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
-    if ((e = cudaStreamWaitEvent(s, side->join, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
-    return rc != TSM_OK ? rc : rc_tile;
+    // the wave kernel (few warps with long, uneven loops) on the side stream:
+    // the tile kernel's blocks fill the SMs its warps leave idle
+    return launch_with_side([&](cudaStream_t st) { return launch(fn, t_grid, dim3(32 * tW), t_smem, t_args, st); },
+                            wfn, w_grid, dim3(32 * W), w_smem, w_args, s, dev);
 }
 
 namespace {

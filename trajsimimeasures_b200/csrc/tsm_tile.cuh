@@ -690,7 +690,14 @@ __global__ void __launch_bounds__(128) hausdorff_matrix_kernel(
     if (mirror) out[dj * ld + qi] = v;
 }
 
-// Pairs kernel: one thread per pair, both trajectories from global memory.
+// Pairs mode: a pair with more than kHausWarpCells point products (na * nb)
+// runs one warp per pair (hausdorff_wave_kernel): on one thread, a pair of
+// two 2000-point trajectories is 8M evaluations and would hold a launch's
+// tail for tens of milliseconds.
+constexpr int64_t kHausWarpCells = 1 << 17;
+
+// Pairs kernel: one thread per pair, both trajectories from global memory
+// (the pairs up to kHausWarpCells point products; it also flags bad lengths).
 template <int R, bool EXACT>
 __global__ void __launch_bounds__(128) hausdorff_pairs_kernel(
     const float2* __restrict__ pts, const int64_t* __restrict__ off_a, const int32_t* __restrict__ len_a,
@@ -704,11 +711,53 @@ __global__ void __launch_bounds__(128) hausdorff_pairs_kernel(
         out[k] = CUDART_NAN_F;
         return;
     }
+    if ((int64_t)na * nb > kHausWarpCells) return;  // the warp kernel's pair
     const float2* a = pts + off_a[k];
     const float2* b = pts + off_b[k];
     const float m1 = directed_max2<R, EXACT>(GlobalCols{a}, na, b, nb);
     const float m2 = directed_max2<R, EXACT>(GlobalCols{b}, nb, a, na);
     out[k] = __fsqrt_rn(fmaxf(m1, m2));
+}
+
+// Long pairs (more than kHausWarpCells point products), one warp each.
+// Persistent, with the pair assignment of dp_wave_kernel (rounds of nw
+// pairs in snake order, a ballot over 32 pairs at a time).  Lane l takes
+// point blocks l, l+32, ... of both directions; the lanes' maxima are
+// reduced with one warp max (exact), so the result is the one-thread
+// kernel's, bit for bit.
+template <int R, bool EXACT>
+__global__ void __launch_bounds__(128) hausdorff_wave_kernel(
+    const float2* __restrict__ pts, const int64_t* __restrict__ off_a, const int32_t* __restrict__ len_a,
+    const int64_t* __restrict__ off_b, const int32_t* __restrict__ len_b, const int32_t* __restrict__ order,
+    int64_t n, int max_len, float* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i0 = 0; i0 * nw < n; i0 += 32) {
+        const int64_t i = i0 + lane;
+        const int64_t t = i * nw + ((i & 1) ? nw - 1 - gw : gw);
+        int64_t k = 0;
+        bool mine = false;
+        if (t < n) {
+            k = order ? (int64_t)order[t] : t;
+            const int na = len_a[k], nb = len_b[k];
+            mine = na >= 0 && nb >= 0 && na <= max_len && nb <= max_len && (int64_t)na * nb > kHausWarpCells;
+        }
+        unsigned todo = __ballot_sync(0xffffffffu, mine);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int64_t kk = __shfl_sync(0xffffffffu, k, src);
+            const int na = len_a[kk], nb = len_b[kk];
+            const float2* a = pts + off_a[kk];
+            const float2* b = pts + off_b[kk];
+            float m = fmaxf(directed_max2<R, EXACT>(GlobalCols{a}, na, b, nb, lane * R, 32 * R),
+                            directed_max2<R, EXACT>(GlobalCols{b}, nb, a, na, lane * R, 32 * R));
+            // non-negative floats order like their bit patterns
+            m = __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(m)));
+            if (lane == 0) out[kk] = __fsqrt_rn(m);
+        }
+    }
 }
 
 }  // namespace tsm
