@@ -201,7 +201,10 @@ class SurrogateIndex:
         finally:
             mm.allow_tf32 = prev
 
-    def candidates(self, Q: TrajSet, c: int, chunk=256) -> torch.Tensor:
+    def candidates(self, Q: TrajSet, c: int, chunk=1024) -> torch.Tensor:
+        """Candidate indices [nq, c] (int64, any order).  chunk queries per
+        scan: one [chunk, n] float32 distance block (4 GB at 1024 x 1M); 1,000
+        queries x 1M on B200, ms: 4.76 at 256, 4.56 at 512, 4.23 at 1024."""
         eq = self.enc.embed(Q)
         out = torch.empty((Q.n, c), dtype=torch.int64, device=Q.device)
         for q0 in range(0, Q.n, chunk):
