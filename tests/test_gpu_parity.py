@@ -162,6 +162,19 @@ def test_list_inputs_and_device_tensors_agree():
     c = core.dtw(torch.from_numpy(t1).cuda(), lens[ia], torch.from_numpy(t2).cuda(), lens[ib])
     np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(a, c.cpu().numpy())
+    # host padded arrays go through one pinned staging buffer, reused and grown
+    # by later calls: calls in a row of other sizes and measures still agree
+    for n, m in ((300, 1), (2000, 0), (40, 1)):
+        pts, off, lens, ia, ib = D.pairs_uniform(n, seed=12 + n)
+        ta, tb = D.unpack(pts, off, lens, ia), D.unpack(pts, off, lens, ib)
+        w = int(lens.max())
+        t1, t2 = D.pad(ta, w), D.pad(tb, w)
+        kw = dict(eps=D.EPS_DEG) if m == 1 else {}
+        a, ca = core.pairs(m, t1, lens[ia], t2, lens[ib], counts=True, **kw)
+        b, cb = core.pairs(m, ta, None, tb, None, counts=True, **kw)
+        np.testing.assert_array_equal(a, b)
+        if m == 1:
+            np.testing.assert_array_equal(ca, cb)
 
 
 @pytest.mark.parametrize("m", MEAS)

@@ -33,6 +33,8 @@ and ``<measure>_matrix(...)``.
 """
 from __future__ import annotations
 
+import threading
+
 import numpy as np
 import torch
 
@@ -70,6 +72,47 @@ def _as_points(t):
     return None
 
 
+_tls = threading.local()
+
+
+def _pinned(nbytes):
+    """The calling thread's pinned host staging buffer (uint8, at least
+    nbytes; grown by doubling and kept).  A call that uploads from it
+    synchronises before returning, so the next call may overwrite it."""
+    b = getattr(_tls, "pinned", None)
+    if b is None or b.numel() < nbytes:
+        size = max(nbytes, 2 * (b.numel() if b is not None else 0), 1 << 20)
+        b = torch.empty(size, dtype=torch.uint8, pin_memory=True)
+        _tls.pinned = b
+    return b
+
+
+def _stage_padded(a1, a2, la, lb, order, dev):
+    """Padded host pair arrays [n, L, >=2] to the device through one pinned
+    buffer and one copy: the points are rounded to float32 straight into the
+    buffer (the rounding of astype), followed by the int32 lengths and
+    processing order; the offsets are made on the device.
+    -> (pts [n*L1 + n*L2, 2] float32, len_a, len_b, order int32, off_a, off_b int64)."""
+    n, L1, L2 = a1.shape[0], a1.shape[1], a2.shape[1]
+    nf1, nf2 = n * L1 * 2, n * L2 * 2
+    pts_bytes = 4 * (nf1 + nf2)  # a multiple of 8: nf1 and nf2 are even
+    nbytes = pts_bytes + 12 * n
+    pin = _pinned(nbytes)
+    host = pin.numpy()
+    f = host[:pts_bytes].view(np.float32)
+    np.copyto(f[:nf1].reshape(n, L1, 2), a1[..., :2], casting="unsafe")
+    np.copyto(f[nf1:].reshape(n, L2, 2), a2[..., :2], casting="unsafe")
+    ints = host[pts_bytes:nbytes].view(np.int32)
+    ints[:n] = la
+    ints[n:2 * n] = lb
+    ints[2 * n:] = order
+    d = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    d.copy_(pin[:nbytes], non_blocking=True)
+    di = d[pts_bytes:].view(torch.int32)
+    ar = torch.arange(n, dtype=torch.int64, device=dev)
+    return d[:pts_bytes].view(torch.float32).view(-1, 2), di[:n], di[n:2 * n], di[2 * n:], ar * L1, n * L1 + ar * L2
+
+
 def _normalise_counts(m, counts, la, lb):
     """Reference normalisation in float64 (edr.py:51, lcss.py:52)."""
     c = counts.astype(np.float64)
@@ -85,6 +128,22 @@ def pairs(measure, t1, len1, t2, len2, *, eps=0.0, gpoint=(0.0, 0.0), exact=Fals
     Returns float64 (NumPy for host inputs, CUDA tensor for CUDA inputs); with
     counts=True also the int32 EDR/LCSS counts."""
     m = measure_id(measure)
+    if (isinstance(t1, np.ndarray) and isinstance(t2, np.ndarray) and t1.ndim == 3 and t2.ndim == 3
+            and t1.shape[-1] >= 2 and t2.shape[-1] >= 2 and t1.shape[0] == t2.shape[0] and t1.shape[0] > 0
+            and t1.shape[1] > 0 and t2.shape[1] > 0):
+        # padded host arrays (the reference's input): one staged upload
+        n, L1, L2 = t1.shape[0], t1.shape[1], t2.shape[1]
+        la, lb = _lens_np(len1, n), _lens_np(len2, n)
+        if la.min() < 0 or lb.min() < 0 or la.max() > L1 or lb.max() > L2:
+            raise ValueError("a length is negative or exceeds the padded width")
+        dev = torch.device("cuda")
+        max_len = int(max(la.max(), lb.max()))
+        pts_t, la_t, lb_t, order_t, off_a_t, off_b_t = _stage_padded(t1, t2, la, lb, pair_order(la, lb), dev)
+        out = torch.empty(n, dtype=torch.float32, device=dev)
+        cnt = torch.empty(n, dtype=torch.int32, device=dev) if m in (_lib.EDR, _lib.LCSS) else None
+        pairs_raw(m, pts_t, off_a_t, la_t, off_b_t, lb_t, max_len, out=out, counts=cnt, order=order_t, eps=eps,
+                  gpoint=gpoint, exact=exact, rows=rows)
+        return _host_result(m, out, cnt, la, lb, counts)
     p1, p2 = _as_points(t1), _as_points(t2)
     if p1 is None or p2 is None:  # lists of trajectories
         n = len(t1)
@@ -135,6 +194,11 @@ def pairs(measure, t1, len1, t2, len2, *, eps=0.0, gpoint=(0.0, 0.0), exact=Fals
         else:
             res = out.double()
         return (res, cnt) if counts else res
+    return _host_result(m, out, cnt, la, lb, counts)
+
+
+def _host_result(m, out, cnt, la, lb, counts):
+    """float64 host result of a pair batch (EDR/LCSS: the normalised counts)."""
     if cnt is not None:
         c_h = cnt.cpu().numpy()
         res = _normalise_counts(m, c_h, la, lb)
