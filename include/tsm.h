@@ -60,6 +60,7 @@ extern "C" {
 #define TSM_EINVAL -1   /* bad argument */
 #define TSM_ECUDA -2    /* a CUDA runtime call failed (message has the CUDA error) */
 #define TSM_ETOOLONG -3 /* max_len beyond what the library supports */
+#define TSM_ETIMEOUT -4 /* a bounded wait inside a kernel ran out (see tsm_enc_embed_status) */
 
 typedef struct tsm_params {
     double eps;       /* EDR/LCSS match threshold (same units as the points); the
@@ -252,6 +253,22 @@ int tsm_enc_forward(const float* params, const float* pts, const int64_t* off, c
 int64_t tsm_enc_embed_workspace_bytes(int32_t B, int32_t T);
 int tsm_enc_embed(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
                   int32_t T, const float* nrm, void* workspace, float* emb, void* stream);
+/* Status of the last tsm_enc_embed call on this workspace: synchronises
+ * `stream`, copies the status word (the first 4 bytes of the workspace, set to
+ * 0 by each call) into *status and returns TSM_OK if it is 0.  The kernel's
+ * waits on its own copies and tensor-core MMAs are bounded (about 1 s of SM
+ * clocks); a wait that runs out sets a bit (1: an a_t copy, 2: an MMA step,
+ * 4: tensor memory left allocated because MMAs were still pending -- the
+ * context should then be reset), writes NaN for that CTA's trajectories and
+ * makes this call return TSM_ETIMEOUT with a message. */
+int tsm_enc_embed_status(const void* workspace, int32_t* status, void* stream);
+/* tsm_enc_embed with its wait limit (SM clocks, >= 1) and a failure-path test
+ * hook: stall_step >= 0 announces that step's a_t copy on its mbarrier but
+ * never issues it, so that every CTA's wait for it runs out with no MMA in
+ * flight; -1 in normal use.  tsm_enc_embed = (wait limit ~1 s, -1). */
+int tsm_enc_embed_opts(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
+                       int32_t T, const float* nrm, void* workspace, float* emb, int64_t wait_cycles,
+                       int32_t stall_step, void* stream);
 /* Forward + pair loss + backward.  Pairs (ia[p], ib[p]) index the batch,
  * y[p] the target distances; loss = mean_p (||e_ia - e_ib|| - y)^2.
  * grad float32 [param_count] (overwritten), loss float32 [1], pred [P]

@@ -28,8 +28,7 @@ _ref = None
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(ORACLE_SO):
-            build_oracle()
+        build_oracle()  # (re)builds only when missing or older than its source
         L = ctypes.CDLL(ORACLE_SO)
         L.tsm_oracle_pairs_f64.argtypes = [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _i64, _dbl, _dbl, _dbl, _vp, _vp]
         L.tsm_oracle_pairs_f32.argtypes = [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _i64, _flt, _dbl, _dbl, _vp, _vp]
@@ -55,14 +54,15 @@ def _p(a):
     return a.ctypes.data_as(_vp)
 
 
-def _pairs_args(pts, off_a, len_a, off_b, len_b):
-    pts = _c(pts, np.float32).reshape(-1, 2)
+def _pairs_args(pts, off_a, len_a, off_b, len_b, dt=np.float32):
+    pts = _c(pts, dt).reshape(-1, 2)
     return (pts, _c(off_a, np.int64), _c(len_a, np.int32), _c(off_b, np.int64), _c(len_b, np.int32))
 
 
 def pairs_f64(measure, pts, off_a, len_a, off_b, len_b, eps=0.0, gpoint=(0.0, 0.0)):
-    """FP64 restatement -> (dist float64 [n], counts int64 [n])."""
-    pts, oa, la, ob, lb = _pairs_args(pts, off_a, len_a, off_b, len_b)
+    """FP64 restatement -> (dist float64 [n], counts int64 [n]).  The points
+    are read as float64 (float32 inputs convert exactly)."""
+    pts, oa, la, ob, lb = _pairs_args(pts, off_a, len_a, off_b, len_b, np.float64)
     n = oa.shape[0]
     out = np.empty(n, dtype=np.float64)
     cnt = np.zeros(n, dtype=np.int64)
@@ -99,7 +99,8 @@ def pairs_idx(fn, measure, pts, off, lens, ia, ib, **kw):
 def matrix_idx(fn, measure, pts_q, off_q, len_q, pts_d, off_d, len_d, **kw):
     """All pairs Q x D through the pair form -> ([nq, nd] dist, [nq, nd] counts)."""
     nq, nd = len(off_q), len(off_d)
-    pts = np.concatenate([np.asarray(pts_q, np.float32).reshape(-1, 2), np.asarray(pts_d, np.float32).reshape(-1, 2)])
+    dt = np.result_type(np.asarray(pts_q).dtype, np.asarray(pts_d).dtype, np.float32)
+    pts = np.concatenate([np.asarray(pts_q, dt).reshape(-1, 2), np.asarray(pts_d, dt).reshape(-1, 2)])
     shift = np.asarray(pts_q).reshape(-1, 2).shape[0]
     qi = np.repeat(np.arange(nq), nd)
     di = np.tile(np.arange(nd), nq)

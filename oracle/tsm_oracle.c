@@ -6,9 +6,11 @@
  * `--impl reference` arm) may load it.  The product path
  * (trajsimimeasures_b200) never calls it.
  *
- * Two families of functions, each over the same packed layout that the CUDA
- * C-ABI uses (float32 points [n_points][2], per-pair int64 offsets and int32
- * lengths):
+ * Two families of functions, each over the packed layout that the CUDA
+ * C-ABI uses (points [n_points][2], per-pair int64 offsets and int32
+ * lengths).  The FP64 restatement reads float64 points, the reference's own
+ * input type (utilities/data_loader.py:78-79 reads float64 Mercator metres);
+ * the FP32 twin reads the float32 points that the kernels see:
  *
  *  1. *_f64: an FP64 restatement of the reference GPU kernels in core/*.py,
  *     following their exact semantics (boundaries, quirks, normalisation):
@@ -58,7 +60,7 @@ static double sq64(double ax, double ay, double bx, double by) {
 
 /* Row-major full DP over (n1+1) x (n2+1); the reference keeps a 3-diagonal
  * ring (dtw.py:35-37) but every cell value is the same. */
-static double dtw64(const float* a, int n1, const float* b, int n2) {
+static double dtw64(const double* a, int n1, const double* b, int n2) {
     /* dtw.py: D(-1,-1)=0, other borders +inf; empty inputs: both empty -> 0,
      * one empty -> +inf (the ring slot read at :52 keeps its init value). */
     if (n1 == 0 && n2 == 0) return 0.0;
@@ -83,7 +85,7 @@ static double dtw64(const float* a, int n1, const float* b, int n2) {
     return r;
 }
 
-static double dfrechet64(const float* a, int n1, const float* b, int n2) {
+static double dfrechet64(const double* a, int n1, const double* b, int n2) {
     /* discret_frechet.py:9-50: max(d, min(three neighbours)), same borders as DTW. */
     if (n1 == 0 && n2 == 0) return 0.0;
     if (n1 == 0 || n2 == 0) return INFINITY;
@@ -108,7 +110,7 @@ static double dfrechet64(const float* a, int n1, const float* b, int n2) {
 }
 
 /* edr.py:10-52 / lcss.py:12-53: integer counts with every DP border 0. */
-static int64_t edr_count64(const float* a, int n1, const float* b, int n2, double eps) {
+static int64_t edr_count64(const double* a, int n1, const double* b, int n2, double eps) {
     if (n1 == 0 || n2 == 0) return 0;
     double seps = eps * eps;
     int64_t* prev = (int64_t*)calloc(n2 + 1, sizeof(int64_t));
@@ -129,7 +131,7 @@ static int64_t edr_count64(const float* a, int n1, const float* b, int n2, doubl
     return r;
 }
 
-static int64_t lcss_count64(const float* a, int n1, const float* b, int n2, double eps) {
+static int64_t lcss_count64(const double* a, int n1, const double* b, int n2, double eps) {
     if (n1 == 0 || n2 == 0) return 0;
     double seps = eps * eps;
     int64_t* prev = (int64_t*)calloc(n2 + 1, sizeof(int64_t));
@@ -154,7 +156,7 @@ static int64_t lcss_count64(const float* a, int n1, const float* b, int n2, doub
 /* erp.py:10-91.  Gap distances to g; S1, S2 are serial sums (:44-49); the
  * borders are the TOTAL sums: D(i,-1)=S1, D(-1,j)=S2, D(-1,-1)=0 (:62-78).
  * With an empty input the reference returns its zero-initialised ring slot. */
-static double erp64(const float* a, int n1, const float* b, int n2, double gx, double gy) {
+static double erp64(const double* a, int n1, const double* b, int n2, double gx, double gy) {
     if (n1 == 0 || n2 == 0) return 0.0;
     double* g1 = (double*)malloc(sizeof(double) * n1);
     double* g2 = (double*)malloc(sizeof(double) * n2);
@@ -203,7 +205,7 @@ static double p2s64(double px, double py, double p1x, double p1y, double p2x, do
 }
 
 /* hausdorff.py:48-69 p2t_dist: min over the t_len-1 segments, 0.0 if none. */
-static double p2t64(double px, double py, const float* t, int n) {
+static double p2t64(double px, double py, const double* t, int n) {
     double dist = 0.0, d1 = 0.0, d2 = 0.0;
     for (int i = 0; i < n - 1; ++i) {
         if (i == 0) {
@@ -219,7 +221,7 @@ static double p2t64(double px, double py, const float* t, int n) {
     return dist;
 }
 
-static double hausdorff64(const float* a, int n1, const float* b, int n2) {
+static double hausdorff64(const double* a, int n1, const double* b, int n2) {
     double m = 0.0;
     for (int i = 0; i < n1; ++i) { double d = p2t64(a[2 * i], a[2 * i + 1], b, n2); if (d > m) m = d; }
     for (int j = 0; j < n2; ++j) { double d = p2t64(b[2 * j], b[2 * j + 1], a, n1); if (d > m) m = d; }
@@ -436,15 +438,15 @@ int tsm_oracle_get_threads(void) {
 
 /* FP64 restatement.  out64[k] = distance of pair k; counts (nullable) gets
  * the EDR/LCSS counts. */
-int tsm_oracle_pairs_f64(int measure, const float* pts, const int64_t* off_a, const int32_t* len_a,
+int tsm_oracle_pairs_f64(int measure, const double* pts, const int64_t* off_a, const int32_t* len_a,
                          const int64_t* off_b, const int32_t* len_b, int64_t n, double eps,
                          double gx, double gy, double* out64, int64_t* counts) {
     if (measure < 0 || measure > 5) return -1;
     int nt = tsm_oracle_get_threads();
 #pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
     for (int64_t k = 0; k < n; ++k) {
-        const float* a = pts + 2 * off_a[k];
-        const float* b = pts + 2 * off_b[k];
+        const double* a = pts + 2 * off_a[k];
+        const double* b = pts + 2 * off_b[k];
         int n1 = len_a[k], n2 = len_b[k];
         double r = 0.0;
         int64_t c = 0;

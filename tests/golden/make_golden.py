@@ -1,9 +1,9 @@
 """Generates tests/golden/*.npz from the reference's own code.
 
-Run in a checkout that has the reference at /root/reference (or
-TSM_REFERENCE_ROOT) -- it is not needed afterwards:
+Run with a checkout of the reference at the path in the TSM_REFERENCE_ROOT
+environment variable -- it is not needed afterwards:
 
-    NUMBA_ENABLE_CUDASIM=1 python tests/golden/make_golden.py [--force]
+    NUMBA_ENABLE_CUDASIM=1 TSM_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden.py [--force]
 
 For each case it runs
   * the reference GPU kernels of core/*.py (dtw, edr, lcss, erp, dfrechet
@@ -14,9 +14,14 @@ For each case it runs
     simulator on the CPU, and
   * the reference C++ measures (query/cpp/spatial/traj.cpp) through
     oracle/_ref/libtsm_ref.so,
-on small seeded inputs whose coordinates are float32 values (stored as
-float64 for the reference).  The fixtures hold the inputs (packed) and the
-outputs.
+on small seeded inputs.  Most cases use coordinates that are float32 values
+(stored as float64 for the reference).  Two cases use float64 coordinates
+that float32 cannot hold, as the reference's drivers read them: Porto near
+pairs in Mercator metres with eps = 200 m and the default gap point (0, 0)
+(utilities/data_loader.py:78-79, config.py:52), and in lon/lat degrees.  The
+reference C++ measures take float32 points (query/cpp/spatial/point.h), so
+those two cases carry no C++ outputs.  The fixtures hold the inputs (packed,
+in their own dtype) and the outputs.
 """
 from __future__ import annotations
 
@@ -57,7 +62,15 @@ def ref_hausdorff(t1, l1, t2, l2):
     return np.sqrt(p2t.copy_to_host().max(-1).max(-1))
 
 
-def run_case(name, trajs_a, trajs_b, eps, gpoint):
+def pack64(trajs):
+    """pack_lists without the float32 rounding (float64 fixtures)."""
+    lens = np.array([len(t) for t in trajs], dtype=np.int32)
+    off = np.zeros(len(trajs), dtype=np.int64)
+    np.cumsum(lens[:-1], out=off[1:])
+    return np.concatenate([np.asarray(t, np.float64).reshape(-1, 2) for t in trajs]), off, lens
+
+
+def run_case(name, trajs_a, trajs_b, eps, gpoint, f64=False):
     path = os.path.join(HERE, f"{name}.npz")
     if os.path.exists(path) and "--force" not in sys.argv:
         print(f"{path}: exists (--force regenerates)")
@@ -80,14 +93,15 @@ def run_case(name, trajs_a, trajs_b, eps, gpoint):
     out["erp"] = refcore.erp(t1e, np.append(l1, 1), t2e, np.append(l2, w), list(gpoint), threads_per_traj=TPT)[:n]
     out["dfrechet"] = refcore.dfrechet(t1, l1, t2, l2, threads_per_traj=TPT)
     out["hausdorff"] = ref_hausdorff(t1, l1, t2, l2)
-    pts, off, lens = pack_lists(list(trajs_a) + list(trajs_b))
+    pts, off, lens = (pack64 if f64 else pack_lists)(list(trajs_a) + list(trajs_b))
     ia = np.arange(n)
     ib = ia + n
-    rs = O.RefSet(pts, off, lens)
     cpp = {}
-    for m, key in ((O.DTW, "dtw"), (O.ERP, "erp"), (O.DFRECHET, "dfrechet"), (O.HAUSDORFF, "hausdorff")):
-        cpp["cpp_" + key] = rs.pairs(m, ia, ib, gpoint=gpoint).astype(np.float64)
-    rs.close()
+    if not f64:
+        rs = O.RefSet(pts, off, lens)
+        for m, key in ((O.DTW, "dtw"), (O.ERP, "erp"), (O.DFRECHET, "dfrechet"), (O.HAUSDORFF, "hausdorff")):
+            cpp["cpp_" + key] = rs.pairs(m, ia, ib, gpoint=gpoint).astype(np.float64)
+        rs.close()
     np.savez_compressed(path, pts=pts, off=off, lens=lens, ia=ia, ib=ib, eps=np.float64(eps),
                         gpoint=np.asarray(gpoint, np.float64), **out, **cpp)
     print(f"{path}: {n} pairs, lengths {lens.min()}..{lens.max()}")
@@ -116,6 +130,14 @@ def main():
     ua = [rng.uniform(size=(int(n), 2)).astype(np.float32) for n in rng.integers(1, 30, 16)]
     ub = [rng.uniform(size=(int(n), 2)).astype(np.float32) for n in rng.integers(1, 30, 16)]
     run_case("unit_square", ua, ub, 0.3, (0.0, 0.0))
+    # 5, 6. float64 near pairs that float32 cannot hold: Porto in Mercator
+    #    metres (eps 200 m, the drivers' default gap point (0, 0)) and in
+    #    lon/lat degrees (eps 3e-4 deg, gap point at the box centre)
+    for name, units, eps, g in (("merc_near_f64", "merc", G.MERC_EPS_M, (0.0, 0.0)),
+                                ("lonlat_near_f64", "deg", G.EPS_DEG, G.BOX_CENTRE)):
+        p, o, l, ia, ib = G.near_pairs_f64(24, lo=3, hi=30, seed=4242 if units == "merc" else 4343, units=units)
+        t = G.unpack(p, o, l)
+        run_case(name, [t[i] for i in ia], [t[i] for i in ib], eps, g, f64=True)
 
 
 if __name__ == "__main__":

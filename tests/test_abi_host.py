@@ -72,8 +72,58 @@ def test_invalid_arguments_fail_before_cuda(lib):
     rc = lib.tsm_allpairs_sym(7, dummy, dummy, dummy, dummy, 3, 10, ctypes.byref(p), dummy, 3, nul, nul)
     assert rc == -1 and b"unknown measure" in lib.tsm_last_error()
     assert lib.tsm_allpairs_sym(0, nul, nul, nul, nul, 0, 10, ctypes.byref(p), nul, 0, nul, nul) == 0
+    st = ctypes.c_int32(0)
+    assert lib.tsm_enc_embed_status(nul, ctypes.byref(st), nul) == -1
+    rc = lib.tsm_enc_embed_opts(dummy, dummy, dummy, dummy, 4, 8, (ctypes.c_float * 4)(0, 0, 1, 1), dummy, dummy, 0,
+                                -1, nul)
+    assert rc == -1 and b"wait limit" in lib.tsm_last_error()
     with pytest.raises(_lib.TsmError):
         _lib.check(-1, "x")
+
+
+def test_float64_inputs_get_an_fp64_origin():
+    """Host logic of the FP64 origin: float32 input is taken as is; float64
+    input is translated per pair (ERP: per call, with the gap point) by an
+    FP32-rounded origin, in FP64, and rounded once; for FP32 values near the
+    origin the translation is exact (Sterbenz)."""
+    from trajsimimeasures_b200 import core
+    from trajsimimeasures_b200.engine import TrajSet, origin_of_points, pack_lists, pack_padded, shift_gpoint
+    rng = np.random.default_rng(1)
+    t1 = np.stack([rng.uniform(-9.7e5, -9.6e5, (5, 7)), rng.uniform(5.03e6, 5.04e6, (5, 7))], axis=-1)
+    t2 = t1 + rng.normal(0, 100.0, t1.shape)
+    l1, l2 = np.array([7, 0, 3, 7, 1]), np.array([7, 4, 0, 2, 7])
+    assert core.pair_origins(0, t1.astype(np.float32), l1, t2.astype(np.float32), l2) is None
+    o = core.pair_origins(0, t1, l1, t2, l2)
+    assert o.shape == (5, 2) and np.array_equal(o[0], t1[0, 0].astype(np.float32))
+    assert np.array_equal(o[1], t2[1, 0].astype(np.float32))  # empty t1: t2's first point
+    assert np.all(o.astype(np.float32) == o)
+    g = core.pair_origins(3, t1, l1, t2, l2)
+    assert g.shape == (2,) and np.all(np.float32(g) == g)
+    f = np.concatenate([t1[l1 > 0, 0], t2[l2 > 0, 0]])
+    assert np.allclose(g, 0.5 * (f.min(0) + f.max(0)), rtol=1e-7)
+    assert shift_gpoint((0.0, 0.0), g) == (-g[0], -g[1])
+    # one rounding of the FP64 difference
+    pts, off, lens = pack_lists([t1[0]], origin=o[0])
+    assert np.array_equal(pts, (t1[0] - o[0]).astype(np.float32))
+    p2, _, _ = pack_padded(t1[:2], [7, 7], origin=o[:2])
+    assert np.array_equal(p2.reshape(2, 7, 2), (t1[:2] - o[:2, None, :]).astype(np.float32))
+    # FP32 values near the origin: exact
+    x = t1.astype(np.float32).astype(np.float64)
+    ox = core.pair_origins(0, x, l1, x, l1)
+    assert np.array_equal((x - ox[:, None, :]).astype(np.float32).astype(np.float64), x - ox[:, None, :])
+    # a set origin is shared by Q and D; no origin for float32 sets or none given
+    t2f = t2.astype(np.float32)
+    assert core.set_origin((t1, l1), (t2f, l2)) == origin_of_points(np.concatenate([t1[l1 > 0, 0], t2f[l2 > 0, 0]]))
+    assert core.set_origin((t1.astype(np.float32), l1)) is None
+    assert origin_of_points(np.zeros((0, 2))) == (0.0, 0.0)
+    # TrajSet records the origin it was built with; TrajSet.from_packed picks its own for float64
+    from trajsimimeasures_b200.engine import same_origin
+    a = TrajSet.__new__(TrajSet)
+    a.origin = (1.0, 2.0)
+    b = TrajSet.__new__(TrajSet)
+    b.origin = (1.0, 2.5)
+    with pytest.raises(ValueError, match="different origins"):
+        same_origin(a, b)
 
 
 def test_pack_lists_and_padded():

@@ -137,3 +137,37 @@ def test_trained_filter_gains_over_exhaustive_and_falls_back():
     assert c is None, rec
     _, ans = idx.query(Q, 10)
     np.testing.assert_array_equal(ans.cpu().numpy(), exact.cpu().numpy())
+
+
+def test_embed_wait_timeout_is_reported_and_context_survives():
+    """The tensor-core GRU's waits are bounded.  The test hook announces one
+    step's a_t copy on its mbarrier but never issues it, so every CTA's wait
+    for it runs out (with a short limit) while no MMA is in flight.  The
+    status word reports it (bit 1), tsm_enc_embed_status returns
+    TSM_ETIMEOUT, Encoder.embed raises instead of returning NaN rows, and
+    the context stays usable: a normal call afterwards gives the same
+    embeddings as before."""
+    import ctypes
+    from trajsimimeasures_b200 import _lib, datagen as D
+    from trajsimimeasures_b200.surrogate import Encoder
+    rng = np.random.default_rng(8)
+    pts, off, lens = D._walks(rng, rng.integers(20, 60, 300), D.STEP_SIGMA)
+    s = _set(D.unpack(pts, off, lens))
+    enc = Encoder.init(s, seed=9)
+    before = enc.embed(s)
+    torch.cuda.synchronize()
+    assert torch.isfinite(before).all()
+    lib = _lib.load()
+    st = ctypes.c_int32(-1)
+    assert lib.tsm_enc_embed_status(ctypes.c_void_p(enc._ews.data_ptr()), ctypes.byref(st), None) == 0
+    assert st.value == 0
+    enc._wait_override = (2_000_000, 3)  # ~1 ms of SM clocks; step 3's copy never issued
+    with pytest.raises(_lib.TsmError, match="wait ran out"):
+        enc.embed(s)
+    rc = lib.tsm_enc_embed_status(ctypes.c_void_p(enc._ews.data_ptr()), ctypes.byref(st), None)
+    assert rc == -4 and st.value & 1 and not st.value & 4, (rc, st.value)
+    enc._wait_override = None
+    after = enc.embed(s)
+    torch.cuda.synchronize()
+    assert torch.equal(before, after)
+    assert lib.tsm_enc_embed_status(ctypes.c_void_p(enc._ews.data_ptr()), ctypes.byref(st), None) == 0

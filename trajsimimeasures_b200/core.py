@@ -39,10 +39,12 @@ import numpy as np
 import torch
 
 from . import _lib
-from .engine import TrajSet, allpairs_sym_raw, pack_lists, pair_order, pairs_raw, matrix_raw, measure_id
+from .engine import (TrajSet, allpairs_sym_raw, first_points_lists, matrix_raw, measure_id, needs_origin,
+                     origin_of_points, pack_lists, pair_order, pairs_raw, shift_gpoint)
 
 __all__ = ["dtw", "edr", "lcss", "erp", "dfrechet", "hausdorff", "matrix", "dtw_matrix", "edr_matrix",
-           "lcss_matrix", "erp_matrix", "dfrechet_matrix", "hausdorff_matrix", "pairs"]
+           "lcss_matrix", "erp_matrix", "dfrechet_matrix", "hausdorff_matrix", "pairs", "allpairs", "matrix_many",
+           "pair_origins", "set_origin"]
 
 
 def _check_tpt(threads_per_traj):
@@ -60,37 +62,134 @@ def _lens_np(lens, n):
 
 
 def _as_points(t):
-    """padded array/tensor -> (float32 [N, L, 2] host array or CUDA tensor, N, L); list -> None."""
+    """padded array/tensor -> (its [N, L, 2] coordinates in their own dtype, N, L); list -> None."""
     if isinstance(t, torch.Tensor):
         if t.dim() != 3 or t.shape[-1] < 2:
             raise ValueError("expected a padded [batch, seq, 2] tensor")
-        return t[..., :2].to(torch.float32).contiguous(), t.shape[0], t.shape[1]
+        return t[..., :2], t.shape[0], t.shape[1]
     if isinstance(t, np.ndarray):
         if t.ndim != 3 or t.shape[-1] < 2:
             raise ValueError("expected a padded [batch, seq, 2] array")
-        return np.ascontiguousarray(t[..., :2], dtype=np.float32), t.shape[0], t.shape[1]
+        return t[..., :2], t.shape[0], t.shape[1]
     return None
+
+
+def _to_f32(a, origin):
+    """[N, L, 2] host array or tensor -> float32, translated by origin (None,
+    [2] or per-trajectory [N, 2]) in FP64 first."""
+    if isinstance(a, torch.Tensor):
+        if origin is None:
+            return a.to(torch.float32).contiguous()
+        o = torch.as_tensor(np.asarray(origin, dtype=np.float64).reshape(-1, 1, 2), device=a.device)
+        return (a.to(torch.float64) - o).to(torch.float32).contiguous()
+    if origin is None:
+        return np.ascontiguousarray(a, dtype=np.float32)
+    out = np.empty(a.shape, dtype=np.float32)
+    np.subtract(a, np.asarray(origin, dtype=np.float64).reshape(-1, 1, 2), out=out, dtype=np.float64,
+                casting="unsafe")
+    return out
+
+
+def _first_points(a, lens):
+    """[N, 2] float64 first point of each padded trajectory (rows of empty ones are unused)."""
+    if isinstance(a, torch.Tensor):
+        return a[:, 0, :2].detach().to(torch.float64).cpu().numpy() if a.shape[1] else np.zeros((a.shape[0], 2))
+    return np.asarray(a[:, 0, :2], dtype=np.float64) if a.shape[1] else np.zeros((a.shape[0], 2))
+
+
+def _dtype_of(t):
+    if isinstance(t, (torch.Tensor, np.ndarray)):
+        return t.dtype
+    for x in t:
+        if len(x):
+            return np.asarray(x).dtype
+    return np.dtype(np.float32)
+
+
+def pair_origins(measure, t1, len1, t2, len2):
+    """The FP64 origin(s) a paired batch is translated by before rounding to
+    float32: None for float32 input; else one origin per pair, the pair's
+    first point rounded to FP32 (every measure but ERP), or one for the whole
+    call (ERP, whose gap point is one per call), the FP32-rounded midpoint of
+    the bounding box of the trajectories' first points.
+    -> None, float64 [n, 2] or float64 [2]."""
+    if not (needs_origin(_dtype_of(t1)) or needs_origin(_dtype_of(t2))):
+        return None
+    p1, p2 = _as_points(t1), _as_points(t2)
+    n = len(t1)
+    if p1 is None or p2 is None:
+        la = _lens_np(len1, n) if len1 is not None else np.array([len(x) for x in t1])
+        lb = _lens_np(len2, n) if len2 is not None else np.array([len(x) for x in t2])
+        f1, f2 = np.zeros((n, 2)), np.zeros((n, 2))
+        for k in range(n):
+            if la[k]:
+                f1[k] = np.asarray(t1[k], dtype=np.float64).reshape(-1, np.shape(t1[k])[-1])[0, :2]
+            if lb[k]:
+                f2[k] = np.asarray(t2[k], dtype=np.float64).reshape(-1, np.shape(t2[k])[-1])[0, :2]
+    else:
+        la, lb = _lens_np(len1, n), _lens_np(len2, n)
+        f1, f2 = _first_points(p1[0], la), _first_points(p2[0], lb)
+    if measure_id(measure) == _lib.ERP:
+        return np.asarray(origin_of_points(np.concatenate([f1[la > 0], f2[lb > 0]])), dtype=np.float64)
+    o = np.where((la > 0)[:, None], f1, np.where((lb > 0)[:, None], f2, 0.0))
+    o = o.astype(np.float32).astype(np.float64)
+    o[~np.isfinite(o).all(axis=1)] = 0.0
+    return o
+
+
+def set_origin(*sets):
+    """The FP64 origin that the sets of one Q x D or all-pairs call share:
+    a TrajSet's own origin if one is given; None if every set is float32;
+    else the FP32-rounded midpoint of the bounding box of all first points."""
+    firsts = []
+    for t, lens in sets:
+        if isinstance(t, TrajSet):
+            return None if tuple(t.origin) == (0.0, 0.0) else t.origin
+    if not any(needs_origin(_dtype_of(t)) for t, _ in sets):
+        return None
+    for t, lens in sets:
+        p = _as_points(t)
+        if p is None:
+            tl = list(t) if lens is None else [np.asarray(x)[:l] for x, l in zip(t, _lens_np(lens, len(t)))]
+            firsts.append(first_points_lists(tl))
+        else:
+            la = _lens_np(lens, p[1])
+            firsts.append(_first_points(p[0], la)[la > 0])
+    return origin_of_points(np.concatenate(firsts) if firsts else np.zeros((0, 2)))
 
 
 _tls = threading.local()
 
 
+PINNED_KEEP_BYTES = 64 << 20  # largest staging buffer a thread keeps between calls
+
+
 def _pinned(nbytes):
-    """The calling thread's pinned host staging buffer (uint8, at least
-    nbytes; grown by doubling and kept).  A call that uploads from it
-    synchronises before returning, so the next call may overwrite it."""
+    """A pinned host staging buffer (uint8, at least nbytes).  Up to
+    PINNED_KEEP_BYTES the calling thread's buffer is reused (grown by
+    doubling); a larger request gets a buffer of its own, released with the
+    call.  A call that uploads from it synchronises before returning, so the
+    next call may overwrite it."""
+    if nbytes > PINNED_KEEP_BYTES:
+        return torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
     b = getattr(_tls, "pinned", None)
     if b is None or b.numel() < nbytes:
-        size = max(nbytes, 2 * (b.numel() if b is not None else 0), 1 << 20)
+        size = min(max(nbytes, 2 * (b.numel() if b is not None else 0), 1 << 20), PINNED_KEEP_BYTES)
         b = torch.empty(size, dtype=torch.uint8, pin_memory=True)
         _tls.pinned = b
     return b
 
 
-def _stage_padded(a1, a2, la, lb, order, dev):
+def release_staging():
+    """Frees the calling thread's pinned staging buffer."""
+    _tls.pinned = None
+
+
+def _stage_padded(a1, a2, la, lb, order, dev, origin=None):
     """Padded host pair arrays [n, L, >=2] to the device through one pinned
     buffer and one copy: the points are rounded to float32 straight into the
-    buffer (the rounding of astype), followed by the int32 lengths and
+    buffer (the rounding of astype; with an origin, [2] or per pair [n, 2],
+    after an FP64 translation by it), followed by the int32 lengths and
     processing order; the offsets are made on the device.
     -> (pts [n*L1 + n*L2, 2] float32, len_a, len_b, order int32, off_a, off_b int64)."""
     n, L1, L2 = a1.shape[0], a1.shape[1], a2.shape[1]
@@ -100,8 +199,13 @@ def _stage_padded(a1, a2, la, lb, order, dev):
     pin = _pinned(nbytes)
     host = pin.numpy()
     f = host[:pts_bytes].view(np.float32)
-    np.copyto(f[:nf1].reshape(n, L1, 2), a1[..., :2], casting="unsafe")
-    np.copyto(f[nf1:].reshape(n, L2, 2), a2[..., :2], casting="unsafe")
+    if origin is None:
+        np.copyto(f[:nf1].reshape(n, L1, 2), a1[..., :2], casting="unsafe")
+        np.copyto(f[nf1:].reshape(n, L2, 2), a2[..., :2], casting="unsafe")
+    else:
+        o = np.asarray(origin, dtype=np.float64).reshape(-1, 1, 2)
+        np.subtract(a1[..., :2], o, out=f[:nf1].reshape(n, L1, 2), dtype=np.float64, casting="unsafe")
+        np.subtract(a2[..., :2], o, out=f[nf1:].reshape(n, L2, 2), dtype=np.float64, casting="unsafe")
     ints = host[pts_bytes:nbytes].view(np.int32)
     ints[:n] = la
     ints[n:2 * n] = lb
@@ -126,7 +230,8 @@ def pairs(measure, t1, len1, t2, len2, *, eps=0.0, gpoint=(0.0, 0.0), exact=Fals
     """Paired batch: result[k] = measure(t1[k][:len1[k]], t2[k][:len2[k]]).
 
     Returns float64 (NumPy for host inputs, CUDA tensor for CUDA inputs); with
-    counts=True also the int32 EDR/LCSS counts."""
+    counts=True also the int32 EDR/LCSS counts.  Inputs that are not float32
+    are translated by an FP64 origin before rounding (``pair_origins``)."""
     m = measure_id(measure)
     if (isinstance(t1, np.ndarray) and isinstance(t2, np.ndarray) and t1.ndim == 3 and t2.ndim == 3
             and t1.shape[-1] >= 2 and t2.shape[-1] >= 2 and t1.shape[0] == t2.shape[0] and t1.shape[0] > 0
@@ -138,7 +243,11 @@ def pairs(measure, t1, len1, t2, len2, *, eps=0.0, gpoint=(0.0, 0.0), exact=Fals
             raise ValueError("a length is negative or exceeds the padded width")
         dev = torch.device("cuda")
         max_len = int(max(la.max(), lb.max()))
-        pts_t, la_t, lb_t, order_t, off_a_t, off_b_t = _stage_padded(t1, t2, la, lb, pair_order(la, lb), dev)
+        origin = pair_origins(m, t1, la, t2, lb)
+        if origin is not None and origin.ndim == 1:
+            gpoint = shift_gpoint(gpoint, origin)
+        pts_t, la_t, lb_t, order_t, off_a_t, off_b_t = _stage_padded(t1, t2, la, lb, pair_order(la, lb), dev,
+                                                                     origin)
         out = torch.empty(n, dtype=torch.float32, device=dev)
         cnt = torch.empty(n, dtype=torch.int32, device=dev) if m in (_lib.EDR, _lib.LCSS) else None
         pairs_raw(m, pts_t, off_a_t, la_t, off_b_t, lb_t, max_len, out=out, counts=cnt, order=order_t, eps=eps,
@@ -151,7 +260,11 @@ def pairs(measure, t1, len1, t2, len2, *, eps=0.0, gpoint=(0.0, 0.0), exact=Fals
             raise ValueError("t1 and t2 hold different numbers of trajectories")
         la = _lens_np(len1, n) if len1 is not None else np.array([len(x) for x in t1])
         lb = _lens_np(len2, n) if len2 is not None else np.array([len(x) for x in t2])
-        pts, off, lens = pack_lists([np.asarray(x)[:l] for x, l in zip(list(t1) + list(t2), np.concatenate([la, lb]))])
+        origin = pair_origins(m, t1, la, t2, lb)
+        if origin is not None and origin.ndim == 2:
+            origin = np.concatenate([origin, origin])  # per trajectory: t1's, then t2's
+        pts, off, lens = pack_lists([np.asarray(x)[:l] for x, l in zip(list(t1) + list(t2), np.concatenate([la, lb]))],
+                                    origin)
         off_a, off_b = off[:n], off[n:]
         on_device = False
         dev = torch.device("cuda")
@@ -162,16 +275,20 @@ def pairs(measure, t1, len1, t2, len2, *, eps=0.0, gpoint=(0.0, 0.0), exact=Fals
         la, lb = _lens_np(len1, n), _lens_np(len2, n)
         if n and (la.min() < 0 or lb.min() < 0 or la.max() > L1 or lb.max() > L2):
             raise ValueError("a length is negative or exceeds the padded width")
+        origin = pair_origins(m, t1, la, t2, lb) if n else None
         on_device = isinstance(a1, torch.Tensor) and a1.is_cuda
         dev = a1.device if on_device else torch.device("cuda")
         off_a = np.arange(n, dtype=np.int64) * L1
         off_b = n * L1 + np.arange(n, dtype=np.int64) * L2
+        a1, a2 = _to_f32(a1, origin), _to_f32(a2.to(dev) if on_device else a2, origin)
         if on_device:
-            pts = torch.cat([a1.reshape(-1, 2), a2.to(dev).reshape(-1, 2)])
+            pts = torch.cat([a1.reshape(-1, 2), a2.reshape(-1, 2)])
         else:
             a1 = a1.numpy() if isinstance(a1, torch.Tensor) else a1
             a2 = a2.numpy() if isinstance(a2, torch.Tensor) else a2
             pts = np.concatenate([a1.reshape(-1, 2), a2.reshape(-1, 2)])
+    if origin is not None and origin.ndim == 1:
+        gpoint = shift_gpoint(gpoint, origin)
     max_len = int(max(la.max(initial=0), lb.max(initial=0)))
     order = pair_order(la, lb)
 
@@ -262,21 +379,24 @@ def hausdorff(t1, len1, t2, len2, threads_per_traj=64):
 # Q x D / all-pairs
 # ---------------------------------------------------------------------------
 
-def _set_of(t, lens, device):
+def _set_of(t, lens, device, origin=None):
+    """A device TrajSet of host/device input (translated by origin, if any)."""
     if isinstance(t, TrajSet):
         return t
     p = _as_points(t)
+    o = (0.0, 0.0) if origin is None else origin
     if p is None:
         trajs = list(t) if lens is None else [np.asarray(x)[:l] for x, l in zip(t, _lens_np(lens, len(t)))]
-        return TrajSet.from_lists(trajs, device=device)
+        return TrajSet.from_lists(trajs, device=device, origin=o)
     a, n, L = p
     la = _lens_np(lens, n)
     if isinstance(a, torch.Tensor) and a.is_cuda:
         off = torch.arange(n, dtype=torch.int64, device=a.device) * L
         lens_t = torch.as_tensor(la, dtype=torch.int32).to(a.device)
-        return TrajSet(a.reshape(-1, 2), off, lens_t, int(la.max(initial=0)), la.astype(np.int32))
+        a = _to_f32(a, origin)
+        return TrajSet(a.reshape(-1, 2), off, lens_t, int(la.max(initial=0)), la.astype(np.int32), origin=o)
     a = a.numpy() if isinstance(a, torch.Tensor) else a
-    return TrajSet.from_packed(a.reshape(-1, 2), np.arange(n, dtype=np.int64) * L, la, device=device)
+    return TrajSet.from_padded(a, la, device=device, origin=o)
 
 
 def matrix(measure, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False, rows=0, counts=False):
@@ -288,8 +408,9 @@ def matrix(measure, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False, rows
     m = measure_id(measure)
     dev = torch.device("cuda")
     on_device = isinstance(Q, TrajSet) or (isinstance(Q, torch.Tensor) and Q.is_cuda)
-    qs = _set_of(Q, lenQ, dev)
-    ds = _set_of(D, lenD, qs.device)
+    origin = set_origin((Q, lenQ), (D, lenD))
+    qs = _set_of(Q, lenQ, dev, origin)
+    ds = _set_of(D, lenD, qs.device, origin)
     out = torch.empty((qs.n, ds.n), dtype=torch.float32, device=qs.device)
     cnt = torch.empty((qs.n, ds.n), dtype=torch.int32, device=qs.device) if m in (_lib.EDR, _lib.LCSS) else None
     matrix_raw(m, qs, ds, out=out, counts=cnt, eps=eps, gpoint=_gpoint(gpoint), exact=exact, rows=rows)
@@ -326,7 +447,7 @@ def allpairs(measure, S, lenS=None, *, eps=0.0, gpoint=None, exact=False, rows=0
     m = measure_id(measure)
     dev = torch.device("cuda")
     on_device = isinstance(S, TrajSet) or (isinstance(S, torch.Tensor) and S.is_cuda)
-    ss = _set_of(S, lenS, dev)
+    ss = _set_of(S, lenS, dev, set_origin((S, lenS)))
     out = torch.empty((ss.n, ss.n), dtype=torch.float32, device=ss.device)
     cnt = torch.empty((ss.n, ss.n), dtype=torch.int32, device=ss.device) if m in (_lib.EDR, _lib.LCSS) else None
     allpairs_sym_raw(m, ss, out=out, counts=cnt, eps=eps, gpoint=_gpoint(gpoint), exact=exact, rows=rows)
@@ -343,8 +464,9 @@ def matrix_many(measures, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False
     1 - count / min(n1, n2)) and copied into pinned host memory on a side
     stream, overlapping the next measure's kernel."""
     dev = torch.device("cuda")
-    qs = _set_of(Q, lenQ, dev)
-    ds = qs if (D is Q and lenD is lenQ) else _set_of(D, lenD, dev)
+    origin = set_origin((Q, lenQ), (D, lenD))
+    qs = _set_of(Q, lenQ, dev, origin)
+    ds = qs if (D is Q and lenD is lenQ) else _set_of(D, lenD, dev, origin)
     g = _gpoint(gpoint)
     s = stream if stream is not None else torch.cuda.current_stream(dev)
     copy = torch.cuda.Stream(device=dev)

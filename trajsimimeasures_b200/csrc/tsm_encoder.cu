@@ -626,15 +626,26 @@ __global__ void __launch_bounds__(256) enc_conv_fwd_tc(const float2* __restrict_
     }
 }
 
+// Bits of the embedding status word (the first word of the embed workspace).
+constexpr int TC_ERR_COPY = 1;      // an a_t copy did not land within the wait limit (no MMA issued for it)
+constexpr int TC_ERR_MMA = 2;       // the MMAs of a step did not complete within the wait limit
+constexpr int TC_ERR_TMEM_HELD = 4; // ... nor within a second limit: the CTA exited without freeing tensor memory
+
 // hl[b][128] = h after the last valid step of trajectory b.  Ab: the a_t
 // images of enc_conv_fwd_tc (T steps per block of 128).  wq: BF16 weights; p:
 // FP32 parameters (biases).  If the tensor cores or a copy do not complete
-// within TC_WAIT_CYCLES, the CTA writes NaN to its rows of hl and stops.
+// within wait_cycles, the CTA ORs a TC_ERR_* bit into *status, writes NaN to
+// its rows of hl and stops: after waiting (bounded) for its copy in flight,
+// and, if MMAs of the failed step were issued, once more for them; tensor
+// memory is freed only when no MMA can still write it.  stall_step >= 0 is a
+// test hook: the a_t copy of that step is announced on its mbarrier but never
+// issued, so that its wait runs out with no MMA in flight (-1 in normal use).
 __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfloat16* __restrict__ Ab,
                                                                    const int32_t* __restrict__ len, int B, int T,
                                                                    const __nv_bfloat16* __restrict__ wq,
                                                                    const float* __restrict__ p,
-                                                                   float* __restrict__ hl) {
+                                                                   float* __restrict__ hl, int* __restrict__ status,
+                                                                   long long wait_cycles, int stall_step) {
     namespace U = tsm::umma;
     extern __shared__ __align__(1024) unsigned char sm[];
     unsigned char* XH = sm + TC_OFF_XH;
@@ -692,21 +703,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfl
         if (bi < B) tmax = max(tmax, len[bi]);
     }
     tmax = min(tmax, T);
-    int pend = -1;  // thread 0: the step whose a_t copy is issued and not yet waited for
+    int pend = -1;    // thread 0: the step whose a_t copy is issued and not yet waited for
+    int issued = -1;  // thread 0: the last step whose MMAs were committed
     if (tid == 0 && tmax > 0) {  // a_0 into buffer 0
         U::mbar_arrive_expect_tx(abar0, TC_A_BYTES);
-        U::bulk_load(sbase + TC_OFF_A0, img, TC_A_BYTES, abar0);
+        if (stall_step != 0) U::bulk_load(sbase + TC_OFF_A0, img, TC_A_BYTES, abar0);
         pend = 0;
     }
     float h[64];
 #pragma unroll
     for (int i = 0; i < 64; ++i) h[i] = 0.f;
     bool failed = false;
+    int fail_t = -1;
     for (int t = 0; t < tmax; ++t) {
         const uint32_t abuf = sbase + ((t & 1) ? TC_OFF_A1 : TC_OFF_A0);
         if (tid == 0) {
             // a_t has landed in buffer t % 2 (its (t / 2)-th use)
-            if (U::mbar_wait((t & 1) ? abar1 : abar0, (uint32_t)((t >> 1) & 1), TC_WAIT_CYCLES)) {
+            if (!U::mbar_wait((t & 1) ? abar1 : abar0, (uint32_t)((t >> 1) & 1), wait_cycles)) {
+                atomicOr(status, TC_ERR_COPY);
+            } else {
                 pend = -1;
                 U::fence_after_sync();
                 constexpr uint32_t kRZ = U::idesc_bf16_f32(TC_M, 2 * HD), kN = U::idesc_bf16_f32(TC_M, HD);
@@ -723,18 +738,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfl
                     U::mma_bf16(tmem + 3 * HD, U::smem_desc(sbase + TC_OFF_XH + ks * 2 * kLBO, kLBO, 128),
                                 U::smem_desc(sbase + TC_OFF_WHN + ks * 2 * (HD * 16), HD * 16, 128), kN, ks);
                 U::commit(mbar);
+                issued = t;
                 if (t + 1 < tmax) {  // a_{t+1} into the other buffer (its last reader, step t-1, has completed)
                     const uint32_t nb = (t & 1) ? abar0 : abar1;
                     U::mbar_arrive_expect_tx(nb, TC_A_BYTES);
-                    U::bulk_load(sbase + ((t & 1) ? TC_OFF_A0 : TC_OFF_A1), img + (int64_t)(t + 1) * (TC_M * C1),
-                                 TC_A_BYTES, nb);
+                    if (t + 1 != stall_step)
+                        U::bulk_load(sbase + ((t & 1) ? TC_OFF_A0 : TC_OFF_A1), img + (int64_t)(t + 1) * (TC_M * C1),
+                                     TC_A_BYTES, nb);
                     pend = t + 1;
                 }
             }
         }
-        const bool ok = U::mbar_wait(mbar, (uint32_t)(t & 1), TC_WAIT_CYCLES);
+        const bool ok = U::mbar_wait(mbar, (uint32_t)(t & 1), wait_cycles);
         if (__syncthreads_or(!ok)) {
             failed = true;
+            fail_t = t;
             break;
         }
         U::fence_after_sync();
@@ -772,8 +790,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfl
         U::fence_before_sync();
         __syncthreads();
     }
-    if (tid == 0 && pend >= 0)  // after a failure: let this CTA's copy in flight land before exiting
-        U::mbar_wait((pend & 1) ? abar1 : abar0, (uint32_t)((pend >> 1) & 1), TC_WAIT_CYCLES);
+    __shared__ int tmem_busy;  // set by thread 0 when MMAs may still write tensor memory
+    if (tid == 0) {
+        tmem_busy = 0;
+        if (pend >= 0)  // after a failure: let this CTA's copy in flight land before exiting
+            U::mbar_wait((pend & 1) ? abar1 : abar0, (uint32_t)((pend >> 1) & 1), wait_cycles);
+        if (failed && issued == fail_t) {  // the failed step's MMAs were committed: wait for them once more
+            atomicOr(status, TC_ERR_MMA);
+            if (!U::mbar_wait(mbar, (uint32_t)(fail_t & 1), wait_cycles)) {
+                atomicOr(status, TC_ERR_TMEM_HELD);
+                tmem_busy = 1;
+            }
+        }
+    }
     if (b < B) {
         float* dst = hl + (int64_t)b * HD + 64 * hc;
 #pragma unroll
@@ -781,7 +810,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfl
     }
     U::fence_before_sync();
     __syncthreads();
-    if (warp == 0) {
+    if (warp == 0 && !tmem_busy) {
         U::fence_after_sync();
         U::tmem_dealloc(tmem, TC_TMEM_COLS);
     }
@@ -899,6 +928,7 @@ int enc_backward(const float* params, const float* pts, const int64_t* off, cons
 // Inference workspace: the BF16 a_t images (B rounded up to 128 rows), last
 // hidden states, embeddings, BF16 weights.
 struct EmbWs {
+    int* status;  // first word of the workspace: TC_ERR_* bits of the last call
     __nv_bfloat16* Ab;
     float *hl, *E;
     __nv_bfloat16* wq;
@@ -911,12 +941,14 @@ int64_t emb_layout(int B, int T, float* base, EmbWs* w) {
         o += align64(n);
         return q;
     };
+    float* st = take(1);
     const int64_t Bp = ((int64_t)B + enc::TC_M - 1) / enc::TC_M * enc::TC_M;
     float* Ab = take(Bp * T * enc::C1 / 2);
     float* hl = take((int64_t)B * enc::HD);
     float* E = take((int64_t)B * enc::ED);
     float* wqf = take((enc::N_PARAMS + 1) / 2);
     if (w) {
+        w->status = reinterpret_cast<int*>(st);
         w->Ab = reinterpret_cast<__nv_bfloat16*>(Ab);
         w->hl = hl;
         w->E = E;
@@ -986,16 +1018,19 @@ int64_t tsm_enc_embed_workspace_bytes(int32_t B, int32_t T) {
     return emb_layout(B, T, nullptr, nullptr) * 4;
 }
 
-int tsm_enc_embed(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
-                  int32_t T, const float* nrm, void* workspace, float* emb, void* stream) {
+int tsm_enc_embed_opts(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
+                       int32_t T, const float* nrm, void* workspace, float* emb, int64_t wait_cycles,
+                       int32_t stall_step, void* stream) {
     int rc = enc_args(params, pts, off, len, B, T, nrm, workspace);
     if (rc) return rc;
     if (!emb) return tsm_internal_fail(TSM_EINVAL, "tsm_enc_embed: null output");
+    if (wait_cycles < 1 || stall_step < -1) return tsm_internal_fail(TSM_EINVAL, "tsm_enc_embed_opts: bad wait limit or stall step");
     using namespace enc;
     EmbWs w;
     emb_layout(B, T, static_cast<float*>(workspace), &w);
     cudaStream_t s = (cudaStream_t)stream;
     const float4 n4 = make_float4(nrm[0], nrm[1], nrm[2], nrm[3]);
+    if ((rc = enc_check(cudaMemsetAsync(w.status, 0, 4, s), "memset embed status"))) return rc;
     enc_round_bf16<<<(OFF_WO + 255) / 256, 256, 0, s>>>(params, w.wq);
     const int Bp = (B + TC_M - 1) / TC_M * TC_M;
     const int64_t tot = (int64_t)Bp * T;
@@ -1004,9 +1039,29 @@ int tsm_enc_embed(const float* params, const float* pts, const int64_t* off, con
     rc = enc_check(cudaFuncSetAttribute(enc_gru_embed_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM),
                    "cudaFuncSetAttribute(enc_gru_embed_tc)");
     if (rc) return rc;
-    enc_gru_embed_tc<<<Bp / TC_M, TC_THREADS, TC_SMEM, s>>>(w.Ab, len, B, T, w.wq, params, w.hl);
+    enc_gru_embed_tc<<<Bp / TC_M, TC_THREADS, TC_SMEM, s>>>(w.Ab, len, B, T, w.wq, params, w.hl, w.status,
+                                                            wait_cycles, stall_step);
     enc_head_fwd<<<(unsigned)((B + HEAD_B - 1) / HEAD_B), ED, 0, s>>>(w.hl, B, params, emb);
     return enc_check(cudaGetLastError(), "tsm_enc_embed launch");
+}
+
+int tsm_enc_embed(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
+                  int32_t T, const float* nrm, void* workspace, float* emb, void* stream) {
+    return tsm_enc_embed_opts(params, pts, off, len, B, T, nrm, workspace, emb, enc::TC_WAIT_CYCLES, -1, stream);
+}
+
+int tsm_enc_embed_status(const void* workspace, int32_t* status, void* stream) {
+    if (!workspace || !status) return tsm_internal_fail(TSM_EINVAL, "tsm_enc_embed_status: null argument");
+    int rc = enc_check(cudaStreamSynchronize((cudaStream_t)stream), "tsm_enc_embed_status: synchronise");
+    if (rc) return rc;
+    if ((rc = enc_check(cudaMemcpy(status, workspace, 4, cudaMemcpyDeviceToHost), "tsm_enc_embed_status: read")))
+        return rc;
+    if (*status == 0) return TSM_OK;
+    char b[256];
+    snprintf(b, sizeof(b), "tsm_enc_embed: a tensor-core wait ran out (status %d: %s%s%s); the affected embeddings are NaN",
+             *status, (*status & enc::TC_ERR_COPY) ? "a_t copy " : "", (*status & enc::TC_ERR_MMA) ? "MMA " : "",
+             (*status & enc::TC_ERR_TMEM_HELD) ? "tensor memory not freed: reset the device" : "");
+    return tsm_internal_fail(TSM_ETIMEOUT, b);
 }
 
 }  // extern "C"

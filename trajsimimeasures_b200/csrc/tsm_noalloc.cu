@@ -18,12 +18,15 @@
 // wrong results; serialise them.  The kernel leaves the queue at zero when it
 // finishes, so consecutive calls start clean.
 //
-// Set-up: the first call on each device (with that device current) looks up
-// the array's device address with cudaGetSymbolAddress -- the array's name in
-// host code is only a host-side stand-in, never a device address -- and
-// clears it (cudaMemset, then a device synchronisation, so every stream sees
-// the zeros).  Make that first call before any stream capture.  No call
-// allocates or frees device memory.
+// Set-up: every call looks up the array's device address in the current
+// context with cudaGetSymbolAddress -- the array's name in host code is only a
+// host-side stand-in, never a device address.  The first call on each device
+// (with that device current) clears the array (cudaMemset, then a device
+// synchronisation, so every stream sees the zeros); make that first call
+// before any stream capture.  The lookup is not cached: after
+// cudaDeviceReset the library's module is loaded again and the array may
+// move, and a later call then uses (and clears once more) the new address.
+// No call allocates or frees device memory.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -42,7 +45,7 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) int g_sched_scratch[kNoallocScratchBytes / 4];
 
 std::mutex g_setup_mu;
-void* g_scratch_addr[kMaxDevices] = {};
+void* g_cleared_addr[kMaxDevices] = {};  // per device: the address last cleared
 
 int fail_cuda(const char* what, cudaError_t e) {
     char b[256];
@@ -70,17 +73,16 @@ int tsm_pairs_sched_noalloc(const float* pts, const int64_t* off_a, const int32_
     if (e != cudaSuccess) return fail_cuda("cudaGetDevice", e);
     if (dev < 0 || dev >= kMaxDevices) return tsm_internal_fail(TSM_EINVAL, "tsm_pairs_sched_noalloc: device ordinal out of range");
     void* scratch = nullptr;
+    e = cudaGetSymbolAddress(&scratch, g_sched_scratch);  // this context's copy of the array
+    if (e != cudaSuccess) return fail_cuda("cudaGetSymbolAddress", e);
     {
         std::lock_guard<std::mutex> lock(g_setup_mu);
-        scratch = g_scratch_addr[dev];
-        if (!scratch) {
-            e = cudaGetSymbolAddress(&scratch, g_sched_scratch);
-            if (e != cudaSuccess) return fail_cuda("cudaGetSymbolAddress", e);
+        if (g_cleared_addr[dev] != scratch) {
             e = cudaMemset(scratch, 0, kNoallocScratchBytes);  // the queue must start at zero
             if (e != cudaSuccess) return fail_cuda("cudaMemset", e);
             e = cudaDeviceSynchronize();  // cleared before any stream's first launch
             if (e != cudaSuccess) return fail_cuda("cudaDeviceSynchronize", e);
-            g_scratch_addr[dev] = scratch;
+            g_cleared_addr[dev] = scratch;
         }
     }
     return tsm_pairs_sched(pts, off_a, len_a, off_b, len_b, order, tasks, n_tasks, max_len, warp_smem_floats,

@@ -25,8 +25,9 @@ SEED_DB = 2000
 SEED_QUERY = 2001
 
 
-def _walks(rng, lens, sigma):
-    """Packed random walks: pts float32 [P, 2], off int64 [N], lens int32 [N]."""
+def _walks(rng, lens, sigma, dtype=np.float32):
+    """Packed random walks: pts [P, 2] (float32 unless dtype says otherwise),
+    off int64 [N], lens int32 [N]."""
     lens = np.asarray(lens, dtype=np.int64)
     n = lens.shape[0]
     off = np.zeros(n, dtype=np.int64)
@@ -47,7 +48,7 @@ def _walks(rng, lens, sigma):
     nz = lens > 0
     base[nz] = cs[off[nz]] - steps[off[nz]]
     pts = start[owner] + cs - base[owner]
-    return pts.astype(np.float32), off, lens.astype(np.int32)
+    return pts.astype(dtype), off, lens.astype(np.int32)
 
 
 def uniform_lengths(rng, n, lo=20, hi=200):
@@ -105,8 +106,50 @@ def near_pairs(n_pairs=200, lo=20, hi=200, seed=SEED_DB + 7, jitter=2e-4, sigma=
     return p, o, l, ia, ia + 1
 
 
+MERC_EPS_M = 200.0  # the reference's EDR/LCSS threshold on Mercator metres (config.py:52)
+
+
+def lonlat_to_merc(lon, lat):
+    """Spherical Web-Mercator metres of lon/lat degrees, the projection of the
+    reference's trajs_merc datasets (utilities/tool_funcs.py:95-100): x = R
+    lon, y = R/2 ln((1 + sin lat)/(1 - sin lat)), R = 6378137 m."""
+    r = 6378137.0
+    lon = np.asarray(lon, dtype=np.float64)
+    t = np.sin(np.radians(np.asarray(lat, dtype=np.float64)))
+    return r * np.radians(lon), 0.5 * r * np.log((1.0 + t) / (1.0 - t))
+
+
+def near_pairs_f64(n_pairs=200, lo=20, hi=200, seed=SEED_DB + 8, units="merc"):
+    """float64 near pairs as the reference's drivers read them: random walks
+    in the Porto-like box, either in lon/lat degrees (step 2e-4 deg, jitter
+    2e-4 deg, for eps = EPS_DEG) or projected to Mercator metres (step and
+    jitter ~120 m, for eps = MERC_EPS_M = 200 m).  The second trajectory of a
+    pair is a jittered, resampled copy of the first, so the EDR/LCSS threshold
+    fires on both sides.  Coordinates are float64 values that float32 cannot
+    hold.  -> (pts float64 [P, 2], off, lens, ia, ib)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    lens = uniform_lengths(rng, n_pairs, lo, hi)
+    sig, jit = (2e-4, 2e-4) if units == "deg" else (1e-3, 1e-3)
+    pts, off, lens = _walks(rng, lens, sig, dtype=np.float64)
+    trajs = []
+    for k in range(n_pairs):
+        a = pts[off[k]:off[k] + lens[k]]
+        keep = np.sort(rng.choice(lens[k], size=max(1, int(lens[k] * rng.uniform(0.6, 1.0))), replace=False))
+        b = a[keep] + rng.normal(0.0, jit, size=(keep.shape[0], 2))
+        trajs += [a, b]
+    if units == "merc":
+        trajs = [np.stack(lonlat_to_merc(t[:, 0], t[:, 1]), axis=1) for t in trajs]
+    elif units != "deg":
+        raise ValueError(f"units must be 'deg' or 'merc', got {units!r}")
+    lens = np.array([len(t) for t in trajs], dtype=np.int32)
+    off = np.zeros(len(trajs), dtype=np.int64)
+    np.cumsum(lens[:-1], out=off[1:])
+    ia = np.arange(0, 2 * n_pairs, 2, dtype=np.int64)
+    return np.concatenate(trajs).astype(np.float64), off, lens, ia, ia + 1
+
+
 def unpack(pts, off, lens, idx=None):
-    """Packed -> list of float32 [n, 2] arrays (views)."""
+    """Packed -> list of [n, 2] arrays (views, in the dtype of pts)."""
     idx = range(len(off)) if idx is None else idx
     return [pts[off[k]:off[k] + lens[k]] for k in idx]
 

@@ -45,46 +45,128 @@ def measure_id(measure) -> int:
 
 
 # ---------------------------------------------------------------------------
+# float64 inputs: one FP64 origin per call
+# ---------------------------------------------------------------------------
+#
+# The reference computes in FP64 on float64 inputs, e.g. Mercator metres read
+# by utilities/data_loader.py:78-79 (x ~ -9.7e5, y ~ 5.0e6 m in Porto, where
+# FP32 spacing is 0.5 m) with eps = 200 m (config.py:52).  Every measure here
+# depends on point differences only (and ERP on differences to the gap point),
+# so the points are translated by an FP64 origin before they are rounded to
+# FP32 and the gap point is translated with them: the rounding error of a
+# coordinate is then half an FP32 ulp of its distance to the origin instead of
+# half an ulp of its absolute value.
+#
+# The origin is rounded to FP32 itself.  x - o is then exact in FP64, rounded
+# once to FP32, and for FP32-representable inputs within a factor of two of o
+# it is exact (Sterbenz), so the kernels see the same point differences as
+# without the translation.  float32 (and float16/bfloat16) inputs are taken
+# as they are: rounding them again could only add error.
+
+_EXACT_IN_F32 = {np.dtype(np.float32), np.dtype(np.float16)}
+
+
+def needs_origin(dtype) -> bool:
+    """True if coordinates of this dtype lose precision when rounded to FP32."""
+    if isinstance(dtype, torch.dtype):
+        return dtype not in (torch.float32, torch.float16, torch.bfloat16)
+    return np.dtype(dtype) not in _EXACT_IN_F32
+
+
+def origin_of_points(first_pts) -> tuple:
+    """Origin of one call: the FP32-rounded midpoint of the bounding box of the
+    given points (one per non-empty trajectory, [k, 2]); (0, 0) for none."""
+    p = np.asarray(first_pts, dtype=np.float64).reshape(-1, 2)
+    if p.shape[0] == 0:
+        return (0.0, 0.0)
+    mid = 0.5 * (p.min(axis=0) + p.max(axis=0))
+    m32 = mid.astype(np.float32)
+    if not np.all(np.isfinite(m32)):
+        return (0.0, 0.0)
+    return (float(m32[0]), float(m32[1]))
+
+
+def first_points_padded(arr, lens) -> np.ndarray:
+    """First point of every non-empty trajectory of a padded [N, L, >=2] array."""
+    a = np.asarray(arr)
+    lens = np.asarray(lens).reshape(-1)
+    return np.asarray(a[lens > 0, 0, :2], dtype=np.float64)
+
+
+def first_points_lists(trajs) -> np.ndarray:
+    firsts = [np.asarray(t, dtype=np.float64).reshape(-1, np.shape(t)[-1])[0, :2] for t in trajs if len(t)]
+    return np.array(firsts, dtype=np.float64).reshape(-1, 2)
+
+
+def _nonzero(origin):
+    return None if origin is None or tuple(float(v) for v in origin) == (0.0, 0.0) else origin
+
+
+def shift_gpoint(gpoint, origin) -> tuple:
+    """The ERP gap point in the coordinates of a set translated by origin."""
+    return (float(gpoint[0]) - float(origin[0]), float(gpoint[1]) - float(origin[1]))
+
+
+# ---------------------------------------------------------------------------
 # host packing
 # ---------------------------------------------------------------------------
 
-def pack_lists(trajs):
-    """List of [n_i, 2] sequences -> (pts float32 [P,2], off int64 [N], lens int32 [N])."""
+def pack_lists(trajs, origin=None):
+    """List of [n_i, 2] sequences -> (pts float32 [P,2], off int64 [N], lens int32 [N]).
+    With an origin ([2], or [N, 2] per trajectory) the points are translated
+    by it in FP64 and then rounded to float32."""
     lens = np.fromiter((len(t) for t in trajs), dtype=np.int32, count=len(trajs))
     off = np.zeros(len(trajs), dtype=np.int64)
     if len(trajs) > 1:
         np.cumsum(lens[:-1], out=off[1:])
     total = int(lens.sum()) if len(trajs) else 0
     pts = np.empty((total, 2), dtype=np.float32)
+    o = None if origin is None else np.broadcast_to(np.asarray(origin, dtype=np.float64).reshape(-1, 2),
+                                                    (len(trajs), 2))
     for k, t in enumerate(trajs):
         if lens[k]:
-            pts[off[k]:off[k] + lens[k]] = np.asarray(t, dtype=np.float32).reshape(-1, 2)[:, :2]
+            a = np.asarray(t)
+            a = a.reshape(-1, a.shape[-1])[:, :2]
+            if o is None:
+                pts[off[k]:off[k] + lens[k]] = a
+            else:
+                np.subtract(a, o[k], out=pts[off[k]:off[k] + lens[k]], dtype=np.float64, casting="unsafe")
     return pts, off, lens
 
 
-def pack_padded(arr, lens):
+def pack_padded(arr, lens, origin=None):
     """Padded [N, L, 2] (+ lengths) -> packed views without moving points:
-    trajectory k starts at point k*L of the flattened array."""
-    a = np.ascontiguousarray(np.asarray(arr)[..., :2], dtype=np.float32)
-    n, L = a.shape[0], a.shape[1]
+    trajectory k starts at point k*L of the flattened array.  With an origin
+    the points are translated by it in FP64 before rounding to float32."""
+    src = np.asarray(arr)
+    n, L = src.shape[0], src.shape[1]
     lens = np.asarray(lens, dtype=np.int64).reshape(-1)
     if lens.shape[0] != n:
         raise ValueError(f"{lens.shape[0]} lengths for {n} trajectories")
     if n and (lens.min() < 0 or lens.max() > L):
         raise ValueError("a length exceeds the padded width")
+    if origin is None:
+        a = np.ascontiguousarray(src[..., :2], dtype=np.float32)
+    else:
+        a = np.empty((n, L, 2), dtype=np.float32)
+        np.subtract(src[..., :2], np.asarray(origin, dtype=np.float64).reshape(-1, 1, 2), out=a, dtype=np.float64,
+                    casting="unsafe")
     off = np.arange(n, dtype=np.int64) * L
     return a.reshape(-1, 2), off, lens.astype(np.int32)
 
 
 @dataclass
 class TrajSet:
-    """Packed trajectories resident on one CUDA device."""
+    """Packed trajectories resident on one CUDA device.  ``origin`` is the FP64
+    point the float32 coordinates are relative to ((0, 0) unless the set was
+    built from float64 input); sets used together in one call must share it."""
     pts: torch.Tensor
     off: torch.Tensor
     lens: torch.Tensor
     max_len: int
     lens_host: np.ndarray = field(repr=False, default=None)
     _order: torch.Tensor = field(repr=False, default=None)
+    origin: tuple = (0.0, 0.0)
 
     @property
     def n(self) -> int:
@@ -95,9 +177,15 @@ class TrajSet:
         return self.pts.device
 
     @classmethod
-    def from_packed(cls, pts, off, lens, device="cuda", non_blocking=False):
+    def from_packed(cls, pts, off, lens, device="cuda", non_blocking=False, origin=None):
+        """origin: None = the set's own (see origin_of_points) when pts is not
+        float32, else (0, 0); or an explicit (x, y), for sets that will be
+        used together."""
         lens_h = np.asarray(lens, dtype=np.int32)
         dev = torch.device(device)
+        off_h = np.asarray(off, dtype=np.int64).reshape(-1)
+        src = np.asarray(pts)
+        src = src.reshape(-1, src.shape[-1]) if src.size else src.reshape(-1, 2)
 
         def up(x, dt):
             t = torch.as_tensor(np.ascontiguousarray(x, dtype=dt))
@@ -105,17 +193,39 @@ class TrajSet:
                 t = t.pin_memory()
             return t.to(dev, non_blocking=non_blocking)
 
-        pts_t = up(np.asarray(pts, dtype=np.float32).reshape(-1, 2), np.float32)
-        return cls(pts_t, up(off, np.int64), up(lens_h, np.int32),
-                   int(lens_h.max()) if lens_h.size else 0, lens_h)
+        if origin is None and needs_origin(src.dtype):
+            origin = origin_of_points(src[off_h[lens_h > 0], :2] if src.shape[0] else src[:0, :2])
+        if origin is None or tuple(origin) == (0.0, 0.0):
+            f32 = np.asarray(src[:, :2], dtype=np.float32)
+            origin = (0.0, 0.0)
+        else:
+            origin = (float(origin[0]), float(origin[1]))
+            f32 = np.empty((src.shape[0], 2), dtype=np.float32)
+            np.subtract(src[:, :2], np.asarray(origin, dtype=np.float64), out=f32, dtype=np.float64, casting="unsafe")
+        return cls(up(f32, np.float32), up(off_h, np.int64), up(lens_h, np.int32),
+                   int(lens_h.max()) if lens_h.size else 0, lens_h, origin=origin)
 
     @classmethod
-    def from_lists(cls, trajs, device="cuda"):
-        return cls.from_packed(*pack_lists(trajs), device=device)
+    def from_lists(cls, trajs, device="cuda", origin=None):
+        """origin as in from_packed."""
+        trajs = list(trajs)
+        if origin is None and any(needs_origin(np.asarray(t).dtype) for t in trajs if len(t)):
+            origin = origin_of_points(first_points_lists(trajs))
+        pts, off, lens = pack_lists(trajs, _nonzero(origin))
+        return cls.from_packed(pts, off, lens, device=device, origin=(0.0, 0.0))._with_origin(origin)
 
     @classmethod
-    def from_padded(cls, arr, lens, device="cuda"):
-        return cls.from_packed(*pack_padded(arr, lens), device=device)
+    def from_padded(cls, arr, lens, device="cuda", origin=None):
+        """origin as in from_packed."""
+        a = np.asarray(arr)
+        if origin is None and needs_origin(a.dtype):
+            origin = origin_of_points(first_points_padded(a, lens))
+        pts, off, ln = pack_padded(a, lens, _nonzero(origin))
+        return cls.from_packed(pts, off, ln, device=device, origin=(0.0, 0.0))._with_origin(origin)
+
+    def _with_origin(self, origin):
+        self.origin = (0.0, 0.0) if origin is None else (float(origin[0]), float(origin[1]))
+        return self
 
     def order_by_length(self) -> torch.Tensor:
         if self._order is None:
@@ -157,12 +267,22 @@ def pairs_raw(measure, pts, off_a, len_a, off_b, len_b, max_len, *, out, counts=
     return out
 
 
+def same_origin(q: TrajSet, d: TrajSet) -> tuple:
+    """The common origin of two sets used in one call (raises if they differ:
+    their float32 coordinates would not be comparable)."""
+    if tuple(q.origin) != tuple(d.origin):
+        raise ValueError(f"the two trajectory sets are relative to different origins ({q.origin} vs {d.origin}); "
+                         "build them with the same origin=")
+    return q.origin
+
+
 def matrix_raw(measure, q: TrajSet, d: TrajSet, *, out, counts=None, d_order=None, eps=0.0,
                gpoint=(0.0, 0.0), exact=False, rows=0, stream=None):
-    """tsm_matrix on two device-resident sets (no copies, no sync)."""
+    """tsm_matrix on two device-resident sets (no copies, no sync).  gpoint is
+    in the sets' original coordinates (translated here by their origin)."""
     m = measure_id(measure)
     lib = _lib.load()
-    p = _lib.params(eps, gpoint, exact, rows)
+    p = _lib.params(eps, shift_gpoint(gpoint, same_origin(q, d)), exact, rows)
     if d_order is None:
         d_order = d.order_by_length()
     rc = lib.tsm_matrix(m, _ptr(q.pts), _ptr(q.off), _ptr(q.lens), q.n, q.max_len,
@@ -181,7 +301,7 @@ def matrix_gather_raw(measure, q: TrajSet, d: TrajSet, cand: torch.Tensor, *, ou
     candidate matrix cand [nq, c] on the device (no copies, no sync)."""
     m = measure_id(measure)
     lib = _lib.load()
-    p = _lib.params(eps, gpoint, exact, rows)
+    p = _lib.params(eps, shift_gpoint(gpoint, same_origin(q, d)), exact, rows)
     if cand.dtype != torch.int32 or cand.dim() != 2 or not cand.is_contiguous():
         raise ValueError("cand must be a contiguous int32 [nq, c] tensor")
     rc = lib.tsm_matrix_gather(m, _ptr(q.pts), _ptr(q.off), _ptr(q.lens), q.n, q.max_len, _ptr(d.pts), _ptr(d.off),
@@ -197,7 +317,7 @@ def allpairs_sym_raw(measure, s: TrajSet, *, out, counts=None, eps=0.0, gpoint=(
     matrix from the upper triangle (no copies, no sync)."""
     m = measure_id(measure)
     lib = _lib.load()
-    p = _lib.params(eps, gpoint, exact, rows)
+    p = _lib.params(eps, shift_gpoint(gpoint, s.origin), exact, rows)
     rc = lib.tsm_allpairs_sym(m, _ptr(s.pts), _ptr(s.off), _ptr(s.lens), _ptr(s.order_by_length()), s.n, s.max_len,
                               ctypes.byref(p), _ptr(out), int(out.stride(0)), _ptr(counts), _stream_ptr(stream))
     _lib.check(rc, "tsm_allpairs_sym")
@@ -228,5 +348,5 @@ def pairs_in_set(measure, s: TrajSet, idx_a, idx_b, *, eps=0.0, gpoint=(0.0, 0.0
     want = (m in (_lib.EDR, _lib.LCSS)) if with_counts is None else with_counts
     counts = torch.empty(n, dtype=torch.int32, device=s.device) if want else None
     pairs_raw(m, s.pts, off_a, len_a, off_b, len_b, s.max_len, out=out, counts=counts, order=order,
-              eps=eps, gpoint=gpoint, exact=exact, rows=rows, stream=stream)
+              eps=eps, gpoint=shift_gpoint(gpoint, s.origin), exact=exact, rows=rows, stream=stream)
     return out, counts

@@ -24,7 +24,7 @@ import torch
 
 from . import _lib
 from .engine import (DEFAULT_ROWS, MATRIX_QUERY_MAX, TrajSet, _ptr, _stream_ptr, matrix_gather_raw, matrix_raw,
-                     measure_id, pairs_raw)
+                     measure_id, pairs_raw, same_origin, shift_gpoint)
 
 
 def topk_rows(d: torch.Tensor, k: int, stream=None):
@@ -44,7 +44,7 @@ def _subset(s: TrajSet, idx: torch.Tensor) -> TrajSet:
     """A view of trajectories idx of s (same point pool)."""
     lens_h = s.lens_host[idx.cpu().numpy()] if s.lens_host is not None else None
     out = TrajSet(s.pts, s.off[idx], s.lens[idx], int(lens_h.max()) if lens_h is not None and lens_h.size
-                  else int(s.lens[idx].max().item()), lens_h)
+                  else int(s.lens[idx].max().item()), lens_h, origin=s.origin)
     out._order = torch.arange(idx.shape[0], dtype=torch.int32, device=s.device)  # idx is length-sorted
     return out
 
@@ -100,8 +100,9 @@ def knn_rerank(Q: TrajSet, D: TrajSet, cand: torch.Tensor, k=10, measure="dtw", 
         off_a, len_a = Q.off[qi] + shift, Q.lens[qi]
         off_b, len_b = D.off[di], D.lens[di]
         dd = torch.empty(nq * c, dtype=torch.float32, device=Q.device)
-        pairs_raw(m, pool, off_a, len_a, off_b, len_b, max(Q.max_len, D.max_len), out=dd, eps=eps, gpoint=gpoint,
-                  exact=exact, stream=stream, order=shape_order(len_a, len_b))
+        pairs_raw(m, pool, off_a, len_a, off_b, len_b, max(Q.max_len, D.max_len), out=dd, eps=eps,
+                  gpoint=shift_gpoint(gpoint, same_origin(Q, D)), exact=exact, stream=stream,
+                  order=shape_order(len_a, len_b))
         dd = dd.view(nq, c)
     # ties to the smaller database index, as in knn_exhaustive
     o = torch.argsort(cand, dim=1)

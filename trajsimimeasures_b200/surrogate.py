@@ -13,6 +13,7 @@ kernel (tsm_pairs) on the GPU.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import math
 from dataclasses import dataclass, field
@@ -57,6 +58,8 @@ class Encoder:
     _ws: torch.Tensor = field(default=None, repr=False)
     _ws_key: tuple = field(default=(0, 0, 0), repr=False)
     _ews: torch.Tensor = field(default=None, repr=False)  # inference workspace (tsm_enc_embed)
+    # failure-path test hook: (wait limit in SM clocks, stalled step) for tsm_enc_embed_opts; None in use
+    _wait_override: tuple = field(default=None, repr=False)
 
     @staticmethod
     def n_params() -> int:
@@ -124,19 +127,30 @@ class Encoder:
                        for b0, e, t in zip(starts, ends, tmax))
             if self._ews is None or self._ews.numel() * 4 < need:
                 self._ews = torch.empty(need // 4 + 64, dtype=torch.float32, device=self.params.device)
+        status = torch.zeros(1, dtype=torch.int32, device=s.device) if tensor_cores else None
         for b0, e, t in zip(starts, ends, tmax):
             B, T = e - b0, max(int(t), 1)
             off, ln, r = off_all[b0:e], ln_all[b0:e], res[b0:e]
             if tensor_cores:
-                rc = lib.tsm_enc_embed(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T, self._nrm_ptr(),
-                                       _ptr(self._ews), _ptr(r), _stream_ptr(stream))
+                if self._wait_override is None:
+                    rc = lib.tsm_enc_embed(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T,
+                                           self._nrm_ptr(), _ptr(self._ews), _ptr(r), _stream_ptr(stream))
+                else:  # failure-path test hook (wait limit, stalled step)
+                    rc = lib.tsm_enc_embed_opts(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T,
+                                                self._nrm_ptr(), _ptr(self._ews), _ptr(r), *self._wait_override,
+                                                _stream_ptr(stream))
                 _lib.check(rc, "tsm_enc_embed")
+                with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
+                    status.bitwise_or_(self._ews[:1].view(torch.int32))  # the batch's status word, no sync
             else:
                 ws = self._workspace(B, T, 1)
                 rc = lib.tsm_enc_forward(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T,
                                          self._nrm_ptr(), _ptr(ws), _ptr(r), _stream_ptr(stream))
                 _lib.check(rc, "tsm_enc_forward")
         out[perm] = res
+        if status is not None and int(status.item()):
+            raise _lib.TsmError(f"tsm_enc_embed: a tensor-core wait ran out (status {int(status.item())}); "
+                                "the affected embeddings are NaN")
         return out
 
     # -- training -----------------------------------------------------------------
