@@ -5,17 +5,26 @@ six measures (DTW, EDR, LCSS, ERP, discrete Frechet, Hausdorff) per step.
 
 One step = the six all-pairs launches over one 2000 x 2000 block (random-walk
 trajectories, lengths U{20..200}, float32; EDR/LCSS eps 3e-4 deg, ERP gap
-point at the box centre).  Under torchrun each rank computes its own
-2000 x 2000 block (rank r: queries = set r, database = set 0; rank 0 is the
-all-pairs matrix of set 0), with no collective on the data path ("weak").
+point at the box centre).  Under torchrun the rows of that one block are
+split across the ranks in contiguous blocks of near-equal work
+(shard.row_shards); each rank computes its rows with no collective on the
+data path, so the total work is fixed as N grows ("strong").
 
-value    = DP cells/s over all ranks (Hausdorff: point-segment evaluations),
-           device time from CUDA events around each step's six launches, inputs
-           resident in HBM, L2 flushed (256 MB write) before every step.
-e2e      = the same cells/s through the public API core.matrix_many with host
-           inputs (padded float64 arrays as the reference takes them): packing,
-           H2D, the six launches, D2H of the six [2000, 2000] results and their
-           float64 normalisation, wall clock per step.
+value    = DP cells/s of the whole block (Hausdorff: point-segment
+           evaluations) over the slowest rank's device time from CUDA events
+           around each step's six launches, inputs resident in HBM, L2 flushed
+           (256 MB write) before every step.
+e2e      = the same cells/s through the public API with host inputs (padded
+           float64 arrays as the reference takes them): core.matrix_many on one
+           GPU, core.matrix_sharded (row blocks + one all-gather per measure)
+           on N; packing, H2D, the six launches, the results to the host as
+           float64 arrays, wall clock per step (max over ranks).
+cfg1     = the 1,000-pair paired call, core.<measure>(t1, len1, t2, len2), per
+           measure: pairs/s through the call (host float64 in, float64 out)
+           and on resident inputs, next to the CPU reference on the same pairs.
+cfg3     = the 500k-pair uneven batch (lognormal lengths), DTW + Frechet + EDR
+           in one autotuned persistent launch replayed as a CUDA graph, next to
+           three plain tsm_pairs launches.
 roofline = the dominant kernel's FP32-issue rate (algorithmic ops per unit x
            units / its event time) against SMs x 128 lanes x max SM clock.
 cpu_baseline = the reference's C++ measures (oracle/_ref: DTW, ERP, Frechet,
@@ -71,6 +80,7 @@ def parse():
     ap.add_argument("--n-db", type=int, default=1_000_000, help="knn: database size")
     ap.add_argument("--n-queries", type=int, default=1000, help="knn: queries")
     ap.add_argument("--checkpoint", default="", help="surrogate: save / knn: load the trained encoder here")
+    ap.add_argument("--no-extra", action="store_true", help="allpairs: skip the cfg1 / cfg3 keys")
     a = ap.parse_args()
     a.measures = [m for m in a.measures.split(",") if m]
     for m in a.measures:
@@ -270,7 +280,7 @@ def run_reference_arm(args, ws, rank):
     line = {
         "metric": "DP cells/s (6 measures, all-pairs 2000x2000)", "value": value, "unit": "cells/s",
         "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * T / len(vals), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": 1e3 * T / len(vals), "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "sample_rows": int(len(rows)), "n_traj": N_TRAJ},
         "cpu_baseline": {"value": value, "unit": "cells/s", "cores": threads, "kind": kind,
@@ -308,12 +318,14 @@ def run_ours(args, ws, rank, local):
     import torch.distributed as dist
     from trajsimimeasures_b200 import datagen as D
     from trajsimimeasures_b200.engine import TrajSet, matrix_raw
+    from trajsimimeasures_b200.shard import row_shards
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    q, d = workload_sets(rank, args.n_traj)
+    q, d = workload_sets(0, args.n_traj)  # one block, its rows split across the ranks
+    r0, r1 = row_shards(q[2], ws)[rank]
     MEAS = args.measures
-    qs = TrajSet.from_packed(*q, device=dev)
+    qs = TrajSet.from_packed(q[0], q[1][r0:r1], q[2][r0:r1], device=dev)
     ds = TrajSet.from_packed(*d, device=dev)
     order = ds.order_by_length()
     nq, nd = qs.n, ds.n
@@ -321,7 +333,8 @@ def run_ours(args, ws, rank, local):
     cnts = {m: torch.empty((nq, nd), dtype=torch.int32, device=dev) for m in ("edr", "lcss") if m in MEAS}
     flush = torch.empty(max(args.flush_mb, 1) * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
-    U = {m: units(m, q[2], d[2]) for m in MEAS}
+    U = {m: units(m, q[2][r0:r1], d[2]) for m in MEAS}  # this rank's block
+    U_all = {m: units(m, q[2], d[2]) for m in MEAS}  # the whole block
 
     def step(evs=None):
         for i, m in enumerate(MEAS):
@@ -366,8 +379,8 @@ def run_ours(args, ws, rank, local):
     if ws > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     max_ms = float(t.item())
-    units_step = sum(U.values())
-    value = ws * units_step * args.steps / (max_ms / 1e3)
+    units_all = sum(U_all.values())
+    value = units_all * args.steps / (max_ms / 1e3)
 
     # e2e through the public API, host inputs
     e2e = None
@@ -375,24 +388,36 @@ def run_ours(args, ws, rank, local):
         from trajsimimeasures_b200 import core
         Qpad = D.pad(D.unpack(*q))
         lq = q[2].copy()
-        Dpad, ld = (Qpad, lq) if rank == 0 else (D.pad(D.unpack(*d)), d[2].copy())
-        core.matrix_many(MEAS, Qpad, lq, Dpad, ld, eps=EPS, gpoint=D.BOX_CENTRE)  # warm
+        if ws == 1:
+            call = lambda: core.matrix_many(MEAS, Qpad, lq, Qpad, lq, eps=EPS, gpoint=D.BOX_CENTRE)  # noqa: E731
+            path = "core.matrix_many(padded float64 host arrays) -> float64 host arrays"
+        else:
+            call = lambda: core.matrix_sharded(MEAS, Qpad, lq, Qpad, lq, eps=EPS, gpoint=D.BOX_CENTRE)  # noqa: E731
+            path = ("core.matrix_sharded(padded float64 host arrays): row blocks per rank, one NCCL all-gather per "
+                    "measure -> float64 host arrays on every rank")
+        call()  # warm
         torch.cuda.synchronize()
         ts = []
         for _ in range(args.e2e_steps):
+            if ws > 1:
+                dist.barrier()
             t0 = time.perf_counter()
-            core.matrix_many(MEAS, Qpad, lq, Dpad, ld, eps=EPS, gpoint=D.BOX_CENTRE)
+            call()
             torch.cuda.synchronize()
             ts.append(time.perf_counter() - t0)
         tt = torch.tensor([sum(ts)], dtype=torch.float64, device=dev)
         if ws > 1:
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        h2d = sum(a.shape[0] * a.shape[1] * 8 + a.shape[0] * 12 for a in ((Qpad,) if Dpad is Qpad else (Qpad, Dpad)))
-        d2h = nq * nd * 4 * len(MEAS)
-        e2e = {"value": ws * units_step * args.e2e_steps / float(tt.item()), "unit": "cells/s",
+        L = Qpad.shape[1]
+        if ws == 1:  # one float32 upload of the set (Q is D), six float64 results back
+            h2d = lq.shape[0] * (L * 8 + 12)
+            d2h = nq * nd * 8 * len(MEAS)
+        else:  # this rank's query rows and the whole database; every rank gets the gathered matrices
+            h2d = (r1 - r0) * (L * 8 + 12) + lq.shape[0] * (L * 8 + 12)
+            d2h = lq.shape[0] * nd * 4 * len(MEAS)
+        e2e = {"value": units_all * args.e2e_steps / float(tt.item()), "unit": "cells/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "ms_per_step": 1e3 * float(tt.item()) / args.e2e_steps,
-               "path": "core.matrix_many(padded float64 host arrays) -> float64 host arrays"}
+               "ms_per_step": 1e3 * float(tt.item()) / args.e2e_steps, "path": path}
 
     if rank != 0:
         return
@@ -422,12 +447,13 @@ def run_ours(args, ws, rank, local):
     line = {
         "metric": "DP cells/s (6 measures, all-pairs 2000x2000)", "value": value, "unit": "cells/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded random walks, Porto-like box)",
         "config": {"workload": WORKLOAD if (args.n_traj == N_TRAJ and MEAS == MEASURES)
                    else f"allpairs_{args.n_traj}x{args.n_traj}_{'+'.join(MEAS)} (profiling case)", "n_traj": args.n_traj, "lengths": "U{20..200}", "eps_deg": EPS,
                    "erp_gpoint": list(D.BOX_CENTRE), "l2": f"flushed before each step ({args.flush_mb} MB write)" if args.flush_mb else "not flushed",
-                   "parallelism": f"weak: one 2000x2000 block per rank x {ws}", "rows_per_thread": args.rows or "default (8; hausdorff 16)"},
+                   "parallelism": f"strong: the rows of one 2000x2000 block split over {ws} rank(s) (rank 0: rows "
+                                  f"{r0}..{r1 - 1})", "rows_per_thread": args.rows or "default (8; hausdorff 16)"},
         "e2e": e2e, "gpu_launches": launches, "roofline": roof, "clocks": clocks, "per_measure": per,
     }
     if not args.no_cpu_baseline:
@@ -439,6 +465,9 @@ def run_ours(args, ws, rank, local):
                                 "sample": f"rows 0..{len(rows) - 1} of the 2000x2000 block x 6 measures "
                                           "(reference C++ for DTW/ERP/Frechet/Hausdorff, FP64 port for EDR/LCSS)"}
         line["cpu_baseline"]["parity_rows_0_3"] = parity_sample(q, d, outs, cnts, np.arange(4))
+    if ws == 1 and not args.no_extra:
+        line["cfg1"] = cfg1_pairs(args)
+        line["cfg3"] = uneven_result(args.n_pairs, 10, 3)
     print(json.dumps(line), flush=True)
 
 
@@ -451,7 +480,79 @@ def _events():
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def run_uneven(args):
+def cfg1_pairs(args, calls=20):
+    """1,000 pairs (lengths U{20..200}, the box's random walks) through the
+    reference-signature paired call core.<measure>(t1, len1, t2, len2), one
+    call per measure on padded float64 host arrays: wall clock per call
+    (staging, H2D, kernels, float64 result on the host), pairs/s; the same
+    kernels on resident inputs (events); the CPU reference on the same pairs
+    with all host threads (reference C++ for DTW/ERP/Frechet/Hausdorff, FP64
+    port for EDR/LCSS).  The reference's paired driver:
+    test_trajsimi_time.py:222-276."""
+    import torch
+    from oracle import oracle as O
+    from trajsimimeasures_b200 import core, datagen as D
+    from trajsimimeasures_b200.engine import pair_order, pairs_raw
+    pts, off, lens, ia, ib = D.pairs_uniform(1000)
+    la, lb = lens[ia], lens[ib]
+    t1, t2 = D.pad(D.unpack(pts, off, lens, ia)), D.pad(D.unpack(pts, off, lens, ib))
+    fns = {"dtw": lambda: core.dtw(t1, la, t2, lb), "edr": lambda: core.edr(t1, la, t2, lb, EPS),
+           "lcss": lambda: core.lcss(t1, la, t2, lb, EPS), "erp": lambda: core.erp(t1, la, t2, lb, D.BOX_CENTRE),
+           "dfrechet": lambda: core.dfrechet(t1, la, t2, lb), "hausdorff": lambda: core.hausdorff(t1, la, t2, lb)}
+    dev = torch.device("cuda", torch.cuda.current_device())
+    up = lambda x, dt: torch.from_numpy(np.ascontiguousarray(x, dtype=dt)).to(dev)  # noqa: E731
+    T = (up(pts, np.float32), up(off[ia], np.int64), up(la, np.int32), up(off[ib], np.int64), up(lb, np.int32))
+    order = up(pair_order(la, lb), np.int32)
+    out = torch.empty(1000, device=dev)
+    cnt = torch.empty(1000, dtype=torch.int32, device=dev)
+    mx = int(max(la.max(), lb.max()))
+    threads = host_threads()
+    O.set_threads(threads)
+    have_ref = O.ref_available()
+    rs = O.RefSet(pts, off, lens) if have_ref else None
+    res = {}
+    for name in MEASURES:
+        m = MID[name]
+        for _ in range(3):
+            fns[name]()
+        ts = []
+        for _ in range(calls):
+            t0 = time.perf_counter()
+            fns[name]()
+            ts.append(time.perf_counter() - t0)
+        call_s = float(np.median(ts))
+        kern = lambda: pairs_raw(m, *T, mx, out=out, counts=cnt if m in (1, 2) else None, order=order,  # noqa: E731
+                                 eps=EPS, gpoint=D.BOX_CENTRE)
+        for _ in range(3):
+            kern()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(calls):
+            kern()
+        e1.record()
+        torch.cuda.synchronize()
+        dev_s = e0.elapsed_time(e1) / 1e3 / calls
+        t0 = time.perf_counter()
+        if rs is not None and m in (0, 3, 4, 5):
+            rs.pairs(m, ia, ib, gpoint=D.BOX_CENTRE, threads=threads)
+            kind = "reference"
+        else:
+            O.pairs_f64(m, pts, off[ia], la, off[ib], lb, eps=EPS, gpoint=D.BOX_CENTRE)
+            kind = "port"
+        cpu_s = time.perf_counter() - t0
+        res[name] = {"call_pairs_per_s": 1000 / call_s, "call_ms": 1e3 * call_s,
+                     "device_pairs_per_s": 1000 / dev_s, "device_ms": 1e3 * dev_s,
+                     "cpu_pairs_per_s": 1000 / cpu_s, "cpu_kind": kind, "call_vs_cpu": cpu_s / call_s}
+    if rs is not None:
+        rs.close()
+    return {"workload": "pairs_1000_uniform_20_200_six_measures", "api": "core.<measure>(t1, len1, t2, len2), "
+            "padded float64 host arrays in, float64 host array out, synchronous", "calls_per_measure": calls,
+            "cpu_cores": threads, "per_measure": res,
+            "h2d_bytes_per_call": int(t1.size * 4 + t2.size * 4 + 12 * 1000),
+            "d2h_bytes_per_call": 1000 * 4}
+
+
+def uneven_result(n_pairs, steps, warmup):
     """500k pairs, lognormal lengths (median 60, sigma 1, clipped 10..2000),
     DTW + Frechet + EDR in ONE persistent launch (autotuned tile/bucket shape,
     CUDA-graph replay), against three plain tsm_pairs launches."""
@@ -459,9 +560,9 @@ def run_uneven(args):
     from trajsimimeasures_b200 import datagen as D, sched
     from trajsimimeasures_b200.engine import pairs_raw, pair_order
     t0 = time.perf_counter()
-    pts, off, lens, ia, ib = D.pairs_lognormal(args.n_pairs, seed=D.SEED_DB)
+    pts, off, lens, ia, ib = D.pairs_lognormal(n_pairs, seed=D.SEED_DB)
     gen_s = time.perf_counter() - t0
-    dev = torch.device("cuda", 0)
+    dev = torch.device("cuda", torch.cuda.current_device())
     up = lambda x, dt: torch.from_numpy(np.ascontiguousarray(x, dtype=dt)).to(dev)  # noqa: E731
     la, lb = lens[ia], lens[ib]
     T = (up(pts, np.float32), up(off[ia], np.int64), up(la, np.int32), up(off[ib], np.int64), up(lb, np.int32))
@@ -475,16 +576,16 @@ def run_uneven(args):
                               len_b_host=lb)
     plan_s = time.perf_counter() - t0
     sc.capture()
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         sc.replay()
     torch.cuda.synchronize()
     e0, e1 = _events()
     e0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         sc.replay()
     e1.record()
     torch.cuda.synchronize()
-    ms_sched = e0.elapsed_time(e1) / args.steps
+    ms_sched = e0.elapsed_time(e1) / steps
     # baseline: one tsm_pairs launch per measure (tile + wave kernels, shape-sorted order)
     order = up(pair_order(la, lb), np.int32)
     out = torch.empty(len(ia), device=dev)
@@ -494,27 +595,31 @@ def run_uneven(args):
     def plain():
         for m in ms_:
             pairs_raw(m, *T[:5], mx, out=out, counts=cnt if m == "edr" else None, order=order, eps=EPS)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         plain()
     torch.cuda.synchronize()
     e0, e1 = _events()
     e0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         plain()
     e1.record()
     torch.cuda.synchronize()
-    ms_plain = e0.elapsed_time(e1) / args.steps
+    ms_plain = e0.elapsed_time(e1) / steps
     kinds = np.bincount(sc.plan.tasks[:, 0], minlength=7).tolist()
-    print(json.dumps({
-        "workload": f"uneven_{args.n_pairs}_pairs_lognormal_dtw+dfrechet+edr", "metric": "DP cells/s",
+    return {
+        "workload": f"uneven_{n_pairs}_pairs_lognormal_dtw+dfrechet+edr", "metric": "DP cells/s",
         "value": cells / (ms_sched / 1e3), "unit": "cells/s", "pairs_per_s": 3 * len(ia) / (ms_sched / 1e3),
         "ms_per_launch": ms_sched, "graph_replay": True,
         "autotuned": {"rows": best[0], "warp_floats": best[1], "max_steps": best[2], "candidates_ms": tried},
         "tasks_by_kind": {"tile": kinds[0], "group4": kinds[5], "group8": kinds[1], "group16": kinds[6],
                           "wave": kinds[2]},
         "plain_tsm_pairs_ms": ms_plain, "speedup_vs_plain": ms_plain / ms_sched,
-        "host_s": {"generate": gen_s, "autotune": tune_s, "plan": plan_s}, "steps": args.steps,
-        "cells_per_launch": cells}), flush=True)
+        "host_s": {"generate": gen_s, "autotune": tune_s, "plan": plan_s}, "steps": steps,
+        "cells_per_launch": cells}
+
+
+def run_uneven(args):
+    print(json.dumps(uneven_result(args.n_pairs, args.steps, args.warmup)), flush=True)
 
 
 def _save_encoder(enc, path, extra):

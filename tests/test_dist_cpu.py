@@ -148,3 +148,80 @@ def test_shard_range_covers():
             rs = [shard_range(n, r, w) for r in range(w)]
             assert rs[0][0] == 0 and rs[-1][1] == n
             assert all(a[1] == b[0] for a, b in zip(rs, rs[1:]))
+
+
+def _oracle_blocks(ids, q_rows, l_rows, D, lenD, origin):
+    """CPU stand-in for the GPU block of core.matrix_sharded: the FP32 twin on
+    the same translated float32 points the kernels would get."""
+    import torch
+    from oracle import oracle as O
+    from trajsimimeasures_b200.engine import pack_padded, shift_gpoint
+    from trajsimimeasures_b200 import datagen as DG
+    o = None if origin is None else origin
+    qp, qo, ql = pack_padded(q_rows, l_rows, o)
+    dp, do, dl = pack_padded(D, lenD, o)
+    g = shift_gpoint(DG.BOX_CENTRE, origin or (0.0, 0.0))
+    out = {}
+    for m in ids:
+        v, c = O.matrix_idx(O.pairs_f32, m, qp, qo, ql, dp, do, dl, eps=DG.EPS_DEG, gpoint=g)
+        out[m] = (torch.from_numpy(v), torch.from_numpy(c) if m in (1, 2) else None)
+    return out
+
+
+def _sharded_case():
+    from trajsimimeasures_b200 import datagen as D
+    p, o, l, ia, ib = D.near_pairs_f64(30, lo=5, hi=40, seed=77, units="deg")
+    t = D.unpack(p, o, l)
+    P = D.pad(t)
+    return P[:37], l[:37], P, l
+
+
+def _sharded_worker(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import oracle as O
+        from trajsimimeasures_b200 import core, datagen as D
+        O.set_threads(1)
+        Q, lq, S, ls = _sharded_case()
+        res = core.matrix_sharded(["dtw", "edr", "lcss", "erp", "dfrechet", "hausdorff"], Q, lq, S, ls,
+                                  eps=D.EPS_DEG, gpoint=D.BOX_CENTRE, block_fn=_oracle_blocks)
+        q.put((rank, res))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_two_rank_gloo_matrix_sharded_matches_single_process():
+    """core.matrix_sharded's real code path (row shards, one all-gather per
+    measure, float64 assembly on every rank) over 2 gloo ranks, the oracle
+    standing in for the kernels: both ranks get the single-process matrix."""
+    from oracle import oracle as O
+    from trajsimimeasures_b200 import core, datagen as D
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_sharded_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=240) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    Q, lq, S, ls = _sharded_case()
+    O.set_threads(1)
+    want = core.matrix_sharded(["dtw", "edr", "lcss", "erp", "dfrechet", "hausdorff"], Q, lq, S, ls, eps=D.EPS_DEG,
+                               gpoint=D.BOX_CENTRE, block_fn=_oracle_blocks)
+    assert set(got) == {0, 1}
+    for r in (0, 1):
+        for name, v in want.items():
+            assert v.shape == (37, 60) and v.dtype == np.float64
+            np.testing.assert_array_equal(got[r][name], v, err_msg=name)
+    # and against the FP64 restatement on the original float64 inputs
+    qp = np.concatenate([Q[i, :lq[i]] for i in range(37)])
+    sp = np.concatenate([S[i, :ls[i]] for i in range(60)])
+    qo = np.concatenate([[0], np.cumsum(lq)[:-1]])
+    so = np.concatenate([[0], np.cumsum(ls)[:-1]])
+    d64, _ = O.matrix_idx(O.pairs_f64, 0, qp, qo, lq, sp, so, ls)
+    assert np.all(np.abs(want["dtw"] - d64) <= 1e-5 * d64)

@@ -67,6 +67,23 @@ def test_exact_mode_bit_identical_to_twin(oracle_mod, cfg_pairs, m, rows):
 
 
 @pytest.mark.parametrize("m", MEAS)
+def test_exact_mode_large_batch_bit_identical_to_twin(oracle_mod, cfg_pairs, m):
+    """A batch too large for the small-batch path (more than 64 pairs per SM):
+    one thread per pair (tile and Hausdorff pairs kernels) for the short
+    pairs; bit-identical to the twin as the warp-per-pair path is."""
+    O = oracle_mod
+    pts, off, lens, ia, ib = cfg_pairs
+    sm = torch.cuda.get_device_properties(0).multi_processor_count
+    reps = 64 * sm // len(ia) + 2
+    ja, jb = np.tile(ia, reps), np.tile(ib, reps)
+    got, cnt = run_pairs(m, pts, off, lens, ja, jb, exact=True, rows=8)
+    want, wcnt = O.pairs_idx(O.pairs_f32, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+    np.testing.assert_array_equal(got, np.tile(want, reps))
+    if m in (1, 2):
+        np.testing.assert_array_equal(cnt, np.tile(wcnt, reps))
+
+
+@pytest.mark.parametrize("m", MEAS)
 def test_default_mode_within_tolerance_of_fp64(oracle_mod, cfg_pairs, m):
     O = oracle_mod
     pts, off, lens, ia, ib = cfg_pairs

@@ -40,11 +40,11 @@ import torch
 
 from . import _lib
 from .engine import (TrajSet, allpairs_sym_raw, first_points_lists, matrix_raw, measure_id, needs_origin,
-                     origin_of_points, pack_lists, pair_order, pairs_raw, shift_gpoint)
+                     origin_of_points, pack_lists, pair_order, pairs_raw, shift_gpoint, sub_origin_f32)
 
 __all__ = ["dtw", "edr", "lcss", "erp", "dfrechet", "hausdorff", "matrix", "dtw_matrix", "edr_matrix",
            "lcss_matrix", "erp_matrix", "dfrechet_matrix", "hausdorff_matrix", "pairs", "allpairs", "matrix_many",
-           "pair_origins", "set_origin"]
+           "matrix_sharded", "pair_origins", "set_origin"]
 
 
 def _check_tpt(threads_per_traj):
@@ -84,10 +84,7 @@ def _to_f32(a, origin):
         return (a.to(torch.float64) - o).to(torch.float32).contiguous()
     if origin is None:
         return np.ascontiguousarray(a, dtype=np.float32)
-    out = np.empty(a.shape, dtype=np.float32)
-    np.subtract(a, np.asarray(origin, dtype=np.float64).reshape(-1, 1, 2), out=out, dtype=np.float64,
-                casting="unsafe")
-    return out
+    return sub_origin_f32(a, np.asarray(origin, dtype=np.float64).reshape(-1, 1, 2), np.empty(a.shape, np.float32))
 
 
 def _first_points(a, lens):
@@ -204,8 +201,8 @@ def _stage_padded(a1, a2, la, lb, order, dev, origin=None):
         np.copyto(f[nf1:].reshape(n, L2, 2), a2[..., :2], casting="unsafe")
     else:
         o = np.asarray(origin, dtype=np.float64).reshape(-1, 1, 2)
-        np.subtract(a1[..., :2], o, out=f[:nf1].reshape(n, L1, 2), dtype=np.float64, casting="unsafe")
-        np.subtract(a2[..., :2], o, out=f[nf1:].reshape(n, L2, 2), dtype=np.float64, casting="unsafe")
+        sub_origin_f32(a1[..., :2], o, f[:nf1].reshape(n, L1, 2))
+        sub_origin_f32(a2[..., :2], o, f[nf1:].reshape(n, L2, 2))
     ints = host[pts_bytes:nbytes].view(np.int32)
     ints[:n] = la
     ints[n:2 * n] = lb
@@ -496,6 +493,89 @@ def matrix_many(measures, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False
         host[_lib.MEASURE_NAMES[m]] = h
     copy.synchronize()
     return {k: v.numpy() for k, v in host.items()}
+
+
+def _rows_of(t, lens, s, e):
+    """Rows s..e of a padded array/tensor or list of trajectories, with their lengths."""
+    if isinstance(t, TrajSet):
+        raise ValueError("matrix_sharded takes host inputs (padded arrays or lists), not a TrajSet")
+    p = _as_points(t)
+    if p is None:
+        tl = list(t)
+        ln = np.array([len(x) for x in tl]) if lens is None else _lens_np(lens, len(tl))
+        return tl[s:e], ln[s:e], ln
+    ln = _lens_np(lens, p[1])
+    return t[s:e], ln[s:e], ln
+
+
+def matrix_sharded(measures, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False, rows=0, group=None,
+                   block_fn=None):
+    """Q x D for several measures over the ranks of a torch.distributed group
+    (one process per GPU): {name: float64 [nq, nd] NumPy array} on every rank.
+
+    The rows of the matrix are split into contiguous blocks of near-equal work
+    (shard.row_shards, by query length); each rank computes its block of
+    every measure on its own GPU with no exchange of intermediate data, and
+    one all-gather per measure (float32 values, int32 EDR/LCSS counts)
+    assembles the matrix.  EDR/LCSS are normalised in float64 as the
+    reference does.  Q and D must be the same host inputs on every rank; they
+    share one FP64 origin (set_origin), so every rank rounds identically.
+    Without an initialised group, or with one rank, this is matrix_many.
+
+    block_fn(measure_ids, Q_rows, len_rows, D, lenD, origin) -> {m: (values
+    float32 [r, nd], counts int32 [r, nd] or None)} replaces the GPU block
+    computation (the tensors' device must suit the group's backend); None =
+    the CUDA kernels on the current device."""
+    import torch.distributed as dist
+    from .shard import row_shards
+    g = _gpoint(gpoint)
+    ids = [measure_id(m) for m in measures]
+    world = dist.get_world_size(group) if dist.is_available() and dist.is_initialized() else 1
+    if world == 1 and block_fn is None:
+        return matrix_many(measures, Q, lenQ, D, lenD, eps=eps, gpoint=gpoint, exact=exact, rows=rows)
+    rank = dist.get_rank(group) if world > 1 else 0
+    lq_all = _rows_of(Q, lenQ, 0, 0)[2]
+    shards = row_shards(lq_all, world)
+    s, e = shards[rank]
+    q_rows, l_rows, _ = _rows_of(Q, lenQ, s, e)
+    origin = set_origin((Q, lenQ), (D, lenD))
+    if block_fn is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        ds = _set_of(D, lenD, dev, origin)
+        qs = _set_of(q_rows, l_rows, dev, origin)
+        blocks = {}
+        for m in ids:
+            out = torch.empty((qs.n, ds.n), dtype=torch.float32, device=dev)
+            cnt = torch.empty((qs.n, ds.n), dtype=torch.int32, device=dev) if m in (_lib.EDR, _lib.LCSS) else None
+            if qs.n:
+                matrix_raw(m, qs, ds, out=out, counts=cnt, eps=eps, gpoint=g, exact=exact, rows=rows)
+            blocks[m] = (out, cnt)
+        ld_all = ds.lens_host if ds.lens_host is not None else ds.lens.cpu().numpy()
+    else:
+        blocks = block_fn(ids, q_rows, l_rows, D, lenD, origin)
+        ld_all = _rows_of(D, lenD, 0, 0)[2]
+    nq, nd = int(lq_all.shape[0]), int(len(ld_all))
+    maxr = max(b - a for a, b in shards)
+
+    def gather(t):
+        pad = torch.zeros((maxr, nd), dtype=t.dtype, device=t.device)
+        pad[:t.shape[0]] = t
+        parts = [torch.empty_like(pad) for _ in range(world)]
+        if world > 1:
+            dist.all_gather(parts, pad, group=group)
+        else:
+            parts = [pad]
+        return torch.cat([p[:b - a] for p, (a, b) in zip(parts, shards)]).cpu().numpy()
+
+    res = {}
+    lq64, ld64 = lq_all.astype(np.int64)[:, None], np.asarray(ld_all, dtype=np.int64)[None, :]
+    for m in ids:
+        out, cnt = blocks[m]
+        if cnt is not None:
+            res[_lib.MEASURE_NAMES[m]] = _normalise_counts(m, gather(cnt), lq64, ld64)
+        else:
+            res[_lib.MEASURE_NAMES[m]] = gather(out).astype(np.float64)
+    return res
 
 
 def dtw_matrix(Q, lenQ, D, lenD, **kw):

@@ -11,10 +11,11 @@
 #include <string>
 
 #include "tsm.h"
-#include "tsm_tile.cuh"
-#include "tsm_wave.cuh"
+#include "tsm_kernels.h"
 #include "tsm_sched.cuh"
+#include "tsm_tile.cuh"
 #include "tsm_topk.cuh"
+#include "tsm_wave.cuh"
 
 namespace {
 
@@ -45,6 +46,12 @@ constexpr int kMatrixQueryMax = 1400;
 // Longest trajectory accepted (wave kernel: 20 bytes of shared memory per
 // column point and warp).
 constexpr int kMaxLen = 8192;
+// A paired batch of at most kSmallBatchPerSm pairs per SM is too small to
+// fill the GPU one thread per pair (the tile and Hausdorff pairs kernels
+// would then run one pair's whole DP serially on a few warps per SM): every
+// non-empty pair runs one warp each on the wave kernels instead, with 4 rows
+// per lane unless rows_per_thread says otherwise.
+constexpr int kSmallBatchPerSm = 64;
 // Shared memory one CTA may use, leaving room for two CTAs per SM at cap 200.
 constexpr int kSmemPerCta = 113 * 1024;
 constexpr int kSmemMax = 227 * 1024;
@@ -80,89 +87,6 @@ int warps_for(int cap, int extra_bytes) {
 cudaError_t set_smem(const void* fn, int bytes) {
     if (bytes <= 48 * 1024) return cudaSuccess;
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-}
-
-// --- kernel tables -----------------------------------------------------------
-
-template <int M, int R, bool E>
-const void* dp_pairs_fn() {
-    return (const void*)&tsm::dp_pairs_kernel<M, R, E>;
-}
-template <int M, int R, bool E>
-const void* dp_matrix_fn() {
-    return (const void*)&tsm::dp_matrix_kernel<M, R, E>;
-}
-
-template <int M, int R, bool E>
-const void* dp_wave_fn() {
-    return (const void*)&tsm::dp_wave_kernel<M, R, E>;
-}
-
-template <int M, bool E>
-const void* pick_wave(int R) {
-    switch (R) {
-        case 4: return dp_wave_fn<M, 4, E>();
-        case 8: return dp_wave_fn<M, 8, E>();
-        case 16: return dp_wave_fn<M, 16, E>();
-        default: return nullptr;
-    }
-}
-
-template <bool E>
-const void* pick_wave_m(int measure, int R) {
-    switch (measure) {
-        case TSM_DTW: return pick_wave<tsm::DTW, E>(R);
-        case TSM_EDR: return pick_wave<tsm::EDR, E>(R);
-        case TSM_LCSS: return pick_wave<tsm::LCSS, E>(R);
-        case TSM_ERP: return pick_wave<tsm::ERP, E>(R);
-        case TSM_DFRECHET: return pick_wave<tsm::DFRECHET, E>(R);
-        default: return nullptr;
-    }
-}
-
-template <int M, bool E>
-const void* pick_dp(bool matrix, int R) {
-    switch (R) {
-        case 4: return matrix ? dp_matrix_fn<M, 4, E>() : dp_pairs_fn<M, 4, E>();
-        case 8: return matrix ? dp_matrix_fn<M, 8, E>() : dp_pairs_fn<M, 8, E>();
-        case 16: return matrix ? dp_matrix_fn<M, 16, E>() : dp_pairs_fn<M, 16, E>();
-        default: return nullptr;
-    }
-}
-
-template <bool E>
-const void* pick_dp_m(int measure, bool matrix, int R) {
-    switch (measure) {
-        case TSM_DTW: return pick_dp<tsm::DTW, E>(matrix, R);
-        case TSM_EDR: return pick_dp<tsm::EDR, E>(matrix, R);
-        case TSM_LCSS: return pick_dp<tsm::LCSS, E>(matrix, R);
-        case TSM_ERP: return pick_dp<tsm::ERP, E>(matrix, R);
-        case TSM_DFRECHET: return pick_dp<tsm::DFRECHET, E>(matrix, R);
-        default: return nullptr;
-    }
-}
-
-template <int R, bool E>
-const void* haus_fn(bool matrix) {
-    return matrix ? (const void*)&tsm::hausdorff_matrix_kernel<R, E> : (const void*)&tsm::hausdorff_pairs_kernel<R, E>;
-}
-
-const void* pick_haus_wave(int R, bool exact) {
-    switch (R) {
-        case 4: return exact ? (const void*)&tsm::hausdorff_wave_kernel<4, true> : (const void*)&tsm::hausdorff_wave_kernel<4, false>;
-        case 8: return exact ? (const void*)&tsm::hausdorff_wave_kernel<8, true> : (const void*)&tsm::hausdorff_wave_kernel<8, false>;
-        case 16: return exact ? (const void*)&tsm::hausdorff_wave_kernel<16, true> : (const void*)&tsm::hausdorff_wave_kernel<16, false>;
-        default: return nullptr;
-    }
-}
-
-const void* pick_haus(bool matrix, int R, bool exact) {
-    switch (R) {
-        case 4: return exact ? haus_fn<4, true>(matrix) : haus_fn<4, false>(matrix);
-        case 8: return exact ? haus_fn<8, true>(matrix) : haus_fn<8, false>(matrix);
-        case 16: return exact ? haus_fn<16, true>(matrix) : haus_fn<16, false>(matrix);
-        default: return nullptr;
-    }
 }
 
 int launch(const void* fn, dim3 grid, dim3 block, int smem, void** args, cudaStream_t s) {
@@ -280,54 +204,70 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
     if (n_pairs == 0) return TSM_OK;
     if (!pts || !off_a || !len_a || !off_b || !len_b || !out) return fail(TSM_EINVAL, "tsm_pairs: null pointer");
     if (max_len < 0) return fail(TSM_EINVAL, "tsm_pairs: max_len < 0");
-    const int R = rows_of(params, measure);
     const bool exact = exact_of(params);
     cudaStream_t s = (cudaStream_t)stream;
     const tsm::KParams kp = make_kparams(params);
     const float2* p2 = reinterpret_cast<const float2*>(pts);
     int64_t n = n_pairs;
     int ml = max_len;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaDeviceGetAttribute");
+    const bool small = n <= (int64_t)kSmallBatchPerSm * sms;
+    const int R = (small && !(params && params->rows_per_thread)) ? 4 : rows_of(params, measure);
     if (measure == TSM_HAUSDORFF) {
-        const void* fn = pick_haus(false, R, exact);
+        const void* fn = tsm_k::haus(false, R, exact);
         if (!fn) return fail(TSM_EINVAL, "tsm_pairs: rows_per_thread must be 4, 8 or 16");
         const int threads = 128;
         dim3 grid((unsigned)((n + threads - 1) / threads));
-        void* args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &ml, &out};
-        if ((int64_t)max_len * max_len <= tsm::kHausWarpCells) return launch(fn, grid, dim3(threads), 0, args, s);
-        // long pairs: one warp each, persistent, on the side stream
-        const void* wfn = pick_haus_wave(R, exact);
+        int64_t warp_cells = small ? 0 : tsm::kHausWarpCells;
+        void* args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &ml, &warp_cells, &out};
+        if ((int64_t)max_len * max_len <= warp_cells) return launch(fn, grid, dim3(threads), 0, args, s);
+        // long pairs (small batch: every non-empty pair): one warp each, persistent
+        const void* wfn = tsm_k::haus_wave(R, exact);
         dim3 w_grid;
-        int dev = 0;
         int rc = persistent_grid("tsm_pairs", wfn, threads, 0, (n + 3) / 4, w_grid, dev);
         if (rc != TSM_OK) return rc;
-        void* w_args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &ml, &out};
+        void* w_args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &ml, &warp_cells, &out};
+        if (small) {  // the pairs kernel only flags bad lengths and empty pairs: one stream, in order
+            rc = launch(fn, grid, dim3(threads), 0, args, s);
+            return rc != TSM_OK ? rc : launch(wfn, w_grid, dim3(threads), 0, w_args, s);
+        }
+        // on the side stream, overlapping the one-thread-per-pair kernel
         return launch_with_side([&](cudaStream_t st) { return launch(fn, grid, dim3(threads), 0, args, st); }, wfn,
                                 w_grid, dim3(threads), 0, w_args, s, dev);
     }
     if (max_len > kMaxLen) return fail(TSM_ETOOLONG, "tsm_pairs: max_len %d > %d", max_len, kMaxLen);
-    const void* fn = exact ? pick_dp_m<true>(measure, false, R) : pick_dp_m<false>(measure, false, R);
+    const void* fn = tsm_k::dp_pairs(measure, R, exact);
     if (!fn) return fail(TSM_EINVAL, "tsm_pairs: rows_per_thread must be 4, 8 or 16");
-    int cap = max_len < 1 ? 1 : (max_len < kTileCap ? max_len : kTileCap);
+    // small batch: tile capacity 0, so the tile kernel keeps only empty and
+    // bad-length pairs and the wave kernel takes every other pair
+    int cap = small ? 0 : (max_len < 1 ? 1 : (max_len < kTileCap ? max_len : kTileCap));
     const int tW = warps_for(cap, 0);
     const int t_smem = tW * 32 * cap * 4;
     const dim3 t_grid((unsigned)((n + 32 * tW - 1) / (32 * tW)));
     void* t_args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &cap, &ml, (void*)&kp, &out, &out_counts};
     // (a tile-heavy pair has a side longer than kHeavyRows >= kTileCap)
-    if (max_len <= cap) return launch(fn, t_grid, dim3(32 * tW), t_smem, t_args, s);
+    if (!small && max_len <= cap) return launch(fn, t_grid, dim3(32 * tW), t_smem, t_args, s);
 
     // pairs whose shorter side exceeds cap, or whose tile loop would be very
     // long: the persistent wave kernel, one warp per pair
-    const void* wfn = exact ? pick_wave_m<true>(measure, R) : pick_wave_m<false>(measure, R);
+    const void* wfn = tsm_k::dp_wave(measure, R, exact);
     int wcap = (max_len + 3) & ~3;
     const int W = 4;
     const int w_smem = W * tsm::wave_warp_floats(wcap) * 4;
     if (w_smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_pairs: wave kernel needs %d bytes", w_smem);
     dim3 w_grid;
-    int dev = 0;
     int rc = persistent_grid("tsm_pairs", wfn, 32 * W, w_smem, (n + W - 1) / W, w_grid, dev);
     if (rc != TSM_OK) return rc;
     int tcap = cap;
     void* w_args[] = {&p2, &off_a, &len_a, &off_b, &len_b, &order, &n, &tcap, &wcap, &ml, (void*)&kp, &out, &out_counts};
+    if (small) {  // the tile kernel has (almost) nothing to do: one stream, in order
+        rc = launch(fn, t_grid, dim3(32 * tW), t_smem, t_args, s);
+        return rc != TSM_OK ? rc : launch(wfn, w_grid, dim3(32 * W), w_smem, w_args, s);
+    }
     // the wave kernel (few warps with long, uneven loops) on the side stream:
     // the tile kernel's blocks fill the SMs its warps leave idle
     return launch_with_side([&](cudaStream_t st) { return launch(fn, t_grid, dim3(32 * tW), t_smem, t_args, st); },
@@ -354,7 +294,7 @@ int matrix_launch(const char* who, int measure, const float* q_pts, const int64_
     int dml = d_max_len;
     int64_t ndd = nd, ld = ld_out, dtot = d_total;
     if (measure == TSM_HAUSDORFF) {
-        const void* fn = pick_haus(true, R, exact);
+        const void* fn = tsm_k::haus(true, R, exact);
         if (!fn) return fail(TSM_EINVAL, "%s: rows_per_thread must be 4, 8 or 16", who);
         const int smem = ((qcap + 1) / 2) * 40;  // staged segment pairs
         if (smem > kSmemMax) return fail(TSM_ETOOLONG, "%s: query length %d too long", who, q_max_len);
@@ -368,7 +308,7 @@ int matrix_launch(const char* who, int measure, const float* q_pts, const int64_
     }
     if (q_max_len > kMatrixQueryMax)
         return fail(TSM_ETOOLONG, "%s: q_max_len %d > %d (use the pairs form)", who, q_max_len, kMatrixQueryMax);
-    const void* fn = exact ? pick_dp_m<true>(measure, true, R) : pick_dp_m<false>(measure, true, R);
+    const void* fn = tsm_k::dp_matrix(measure, R, exact);
     if (!fn) return fail(TSM_EINVAL, "%s: rows_per_thread must be 4, 8 or 16", who);
     const int W = warps_for(qcap, qcap * 16);
     const int threads = 32 * W;
@@ -483,10 +423,8 @@ int tsm_pairs_sched(const float* pts, const int64_t* off_a, const int32_t* len_a
     if (out_stride < 0) return fail(TSM_EINVAL, "tsm_pairs_sched: out_stride < 0");
     const int R = rows_of(params);
     const bool exact = exact_of(params);
-    const void* fn = nullptr;
-    if (R == 4) fn = exact ? (const void*)&tsm::dp_sched_kernel<4, true> : (const void*)&tsm::dp_sched_kernel<4, false>;
-    else if (R == 8) fn = exact ? (const void*)&tsm::dp_sched_kernel<8, true> : (const void*)&tsm::dp_sched_kernel<8, false>;
-    else return fail(TSM_EINVAL, "tsm_pairs_sched: rows_per_thread must be 4 or 8");
+    const void* fn = tsm_k::sched(R, exact);
+    if (!fn) return fail(TSM_EINVAL, "tsm_pairs_sched: rows_per_thread must be 4 or 8");
     const int W = 4;
     const int smem = W * warp_smem_floats * 4;
     if (smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_pairs_sched: %d bytes of shared memory per CTA", smem);

@@ -697,12 +697,14 @@ __global__ void __launch_bounds__(128) hausdorff_matrix_kernel(
 constexpr int64_t kHausWarpCells = 1 << 17;
 
 // Pairs kernel: one thread per pair, both trajectories from global memory
-// (the pairs up to kHausWarpCells point products; it also flags bad lengths).
+// (the pairs up to warp_cells point products -- kHausWarpCells, or 0 when a
+// small batch runs every non-empty pair on the warp kernel; it also flags
+// bad lengths).
 template <int R, bool EXACT>
 __global__ void __launch_bounds__(128) hausdorff_pairs_kernel(
     const float2* __restrict__ pts, const int64_t* __restrict__ off_a, const int32_t* __restrict__ len_a,
     const int64_t* __restrict__ off_b, const int32_t* __restrict__ len_b, const int32_t* __restrict__ order,
-    int64_t n, int max_len, float* __restrict__ out) {
+    int64_t n, int max_len, int64_t warp_cells, float* __restrict__ out) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const int64_t k = order ? (int64_t)order[t] : t;
@@ -711,7 +713,7 @@ __global__ void __launch_bounds__(128) hausdorff_pairs_kernel(
         out[k] = CUDART_NAN_F;
         return;
     }
-    if ((int64_t)na * nb > kHausWarpCells) return;  // the warp kernel's pair
+    if ((int64_t)na * nb > warp_cells) return;  // the warp kernel's pair
     const float2* a = pts + off_a[k];
     const float2* b = pts + off_b[k];
     const float m1 = directed_max2<R, EXACT>(GlobalCols{a}, na, b, nb);
@@ -719,7 +721,7 @@ __global__ void __launch_bounds__(128) hausdorff_pairs_kernel(
     out[k] = __fsqrt_rn(fmaxf(m1, m2));
 }
 
-// Long pairs (more than kHausWarpCells point products), one warp each.
+// Long pairs (more than warp_cells point products), one warp each.
 // Persistent, with the pair assignment of dp_wave_kernel (rounds of nw
 // pairs in snake order, a ballot over 32 pairs at a time).  Lane l takes
 // point blocks l, l+32, ... of both directions; the lanes' maxima are
@@ -729,7 +731,7 @@ template <int R, bool EXACT>
 __global__ void __launch_bounds__(128) hausdorff_wave_kernel(
     const float2* __restrict__ pts, const int64_t* __restrict__ off_a, const int32_t* __restrict__ len_a,
     const int64_t* __restrict__ off_b, const int32_t* __restrict__ len_b, const int32_t* __restrict__ order,
-    int64_t n, int max_len, float* __restrict__ out) {
+    int64_t n, int max_len, int64_t warp_cells, float* __restrict__ out) {
     const int lane = threadIdx.x & 31;
     const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -741,7 +743,7 @@ __global__ void __launch_bounds__(128) hausdorff_wave_kernel(
         if (t < n) {
             k = order ? (int64_t)order[t] : t;
             const int na = len_a[k], nb = len_b[k];
-            mine = na >= 0 && nb >= 0 && na <= max_len && nb <= max_len && (int64_t)na * nb > kHausWarpCells;
+            mine = na >= 0 && nb >= 0 && na <= max_len && nb <= max_len && (int64_t)na * nb > warp_cells;
         }
         unsigned todo = __ballot_sync(0xffffffffu, mine);
         while (todo) {

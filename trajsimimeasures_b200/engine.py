@@ -98,6 +98,17 @@ def first_points_lists(trajs) -> np.ndarray:
     return np.array(firsts, dtype=np.float64).reshape(-1, 2)
 
 
+def sub_origin_f32(src, origin, out):
+    """out (float32 ndarray) = src - origin, computed in FP64 and rounded once.
+    origin broadcasts against src (e.g. [2], or [n, 1, 2] per trajectory).
+    Runs as one multithreaded torch CPU op: NumPy's broadcast subtract with a
+    float32 destination is several times slower on [n, L, 2] arrays."""
+    a = torch.from_numpy(np.asarray(src, dtype=np.float64))
+    o = torch.from_numpy(np.ascontiguousarray(origin, dtype=np.float64))
+    torch.from_numpy(out).copy_(a - o)
+    return out
+
+
 def _nonzero(origin):
     return None if origin is None or tuple(float(v) for v in origin) == (0.0, 0.0) else origin
 
@@ -130,7 +141,7 @@ def pack_lists(trajs, origin=None):
             if o is None:
                 pts[off[k]:off[k] + lens[k]] = a
             else:
-                np.subtract(a, o[k], out=pts[off[k]:off[k] + lens[k]], dtype=np.float64, casting="unsafe")
+                pts[off[k]:off[k] + lens[k]] = np.asarray(a, dtype=np.float64) - o[k]
     return pts, off, lens
 
 
@@ -149,8 +160,7 @@ def pack_padded(arr, lens, origin=None):
         a = np.ascontiguousarray(src[..., :2], dtype=np.float32)
     else:
         a = np.empty((n, L, 2), dtype=np.float32)
-        np.subtract(src[..., :2], np.asarray(origin, dtype=np.float64).reshape(-1, 1, 2), out=a, dtype=np.float64,
-                    casting="unsafe")
+        sub_origin_f32(src[..., :2], np.asarray(origin, dtype=np.float64).reshape(-1, 1, 2), a)
     off = np.arange(n, dtype=np.int64) * L
     return a.reshape(-1, 2), off, lens.astype(np.int32)
 
@@ -201,7 +211,7 @@ class TrajSet:
         else:
             origin = (float(origin[0]), float(origin[1]))
             f32 = np.empty((src.shape[0], 2), dtype=np.float32)
-            np.subtract(src[:, :2], np.asarray(origin, dtype=np.float64), out=f32, dtype=np.float64, casting="unsafe")
+            sub_origin_f32(src[:, :2], np.asarray(origin, dtype=np.float64), f32)
         return cls(up(f32, np.float32), up(off_h, np.int64), up(lens_h, np.int32),
                    int(lens_h.max()) if lens_h.size else 0, lens_h, origin=origin)
 
