@@ -637,15 +637,50 @@ def _load_encoder(path, dev):
     return enc, ck
 
 
+def hit_ratios(Q, Dset, enc, exact_idx, ks=(10, 50), cands=(200, 500)):
+    """HR@k of the embedding alone (the reference's learned-measure metric,
+    utilities/tool_funcs.py:141-158): |top-k by embedding distance  intersect
+    top-k by exact DTW| / k, averaged over the queries; and R10@c, the
+    recall@10 of the top-c candidates, all with FP32 embedding distances."""
+    import torch
+    eq, ed = enc.embed(Q).double(), enc.embed(Dset).double()
+    mu = ed.mean(0)
+    eq, ed = (eq - mu).float(), (ed - mu).float()
+    nd = (ed * ed).sum(1)
+    kmax = max(max(ks), max(cands))
+    tops = []
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        for q0 in range(0, Q.n, 256):
+            d = nd[None, :] - 2.0 * (eq[q0:q0 + 256] @ ed.T)
+            tops.append(torch.topk(d, kmax, dim=1, largest=False).indices.cpu().numpy())
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    top = np.concatenate(tops)
+    ex = np.asarray(exact_idx.cpu() if hasattr(exact_idx, "cpu") else exact_idx)
+    out = {f"HR@{k}": float(np.mean([len(np.intersect1d(top[i, :k], ex[i, :k])) / k for i in range(len(top))]))
+           for k in ks}
+    out.update({f"R10@{c}": float(np.mean([len(np.intersect1d(top[i, :c], ex[i, :10])) / 10 for i in range(len(top))]))
+                for c in cands})
+    return out
+
+
 def run_surrogate(args):
-    """Pool of random-walk trajectories, random pairs labelled by the GPU DTW
-    kernel, normalised by the max label; the encoder trained with MSE by the
-    library's own kernels; held-out Spearman rho; FP64-oracle error of the labels."""
+    """Pool of random-walk trajectories; training pairs: random pairs (the
+    reference protocol) plus each of 10k anchors with its 10 nearest pool
+    trajectories by exact GPU DTW (neighbourhood pairs, as NEUTRAJ samples);
+    labels from the GPU DTW kernel, normalised by the max label; the encoder
+    trained with the relative squared error by the library's own kernels
+    (MSE weighted by 1 / y^2, so that the near pairs count); held-out Spearman rho on
+    random pairs; HR@10 / HR@50 of the embedding on 256 pool queries;
+    FP64-oracle error of the labels."""
     import torch
     from oracle import oracle as O
     from trajsimimeasures_b200 import datagen as D
     from trajsimimeasures_b200.engine import TrajSet
-    from trajsimimeasures_b200.surrogate import Encoder, dtw_labels, spearman
+    from trajsimimeasures_b200.knn import _subset, knn_exhaustive
+    from trajsimimeasures_b200.surrogate import Encoder, dtw_labels, neighbour_pairs, spearman
     dev = torch.device("cuda", 0)
     p, o, l = D.trajectory_set(args.pool, seed=D.SEED_DB)
     s = TrajSet.from_packed(p, o, l, device=dev)
@@ -654,31 +689,45 @@ def run_surrogate(args):
     pa, pb = rng.integers(0, args.pool, n), rng.integers(0, args.pool, n)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    na, nb = neighbour_pairs(s, args.pool // 10, k=10, seed=D.SEED_DB)
+    torch.cuda.synchronize()
+    nb_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
     lab = dtw_labels(s, pa, pb)
+    nlab = dtw_labels(s, na, nb)
     torch.cuda.synchronize()
     label_s = time.perf_counter() - t0
     sample = rng.choice(n, 2000, replace=False)
     d64, _ = O.pairs_idx(O.pairs_f64, 0, p, o, l, pa[sample], pb[sample])
     label_err = float(np.max(np.abs(lab[sample] - d64) / d64))
-    y = lab / lab.max()
+    mx = float(max(lab.max(), nlab.max()))
+    y = lab / mx
     ntr = int(0.9 * n)
+    tr_a, tr_b = np.concatenate([pa[:ntr], na]), np.concatenate([pb[:ntr], nb])
+    tr_y = np.concatenate([y[:ntr], nlab / mx])
+    hq = _subset(s, torch.as_tensor(np.sort(rng.choice(args.pool, 256, replace=False)), device=dev))
+    _, hq_exact = knn_exhaustive(hq, s, 50)
     enc = Encoder.init(s, seed=0)
     rho0 = spearman(enc.predict_pairs(s, pa[ntr:], pb[ntr:]), y[ntr:])
+    hr0 = hit_ratios(hq, s, enc, hq_exact)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    hist = enc.fit(s, pa[:ntr], pb[:ntr], y[:ntr], epochs=args.epochs, batch_pairs=1024, lr=2e-3)
+    hist = enc.fit(s, tr_a, tr_b, tr_y, epochs=args.epochs, batch_pairs=1024, lr=2e-3, relative=True)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     pred = enc.predict_pairs(s, pa[ntr:], pb[ntr:])
     rho = spearman(pred, y[ntr:])
+    hr = hit_ratios(hq, s, enc, hq_exact)
     if args.checkpoint:
-        _save_encoder(enc, args.checkpoint, {"max_label": float(lab.max()), "rho": rho})
+        _save_encoder(enc, args.checkpoint, {"max_label": mx, "rho": rho})
     print(json.dumps({
-        "workload": f"surrogate_pool{args.pool}_pairs{n}", "metric": "held-out Spearman rho", "value": rho,
-        "rho_untrained": rho0, "mse_first_epoch": hist[0], "mse_last_epoch": hist[-1], "epochs": args.epochs,
-        "train_s": train_s, "train_pairs_per_s": args.epochs * ntr / train_s, "label_s": label_s,
-        "label_pairs_per_s": n / label_s, "label_max_rel_err_vs_fp64": label_err,
-        "checkpoint": args.checkpoint or None}), flush=True)
+        "workload": f"surrogate_pool{args.pool}_pairs{n}+neighbours{len(na)}", "metric": "held-out Spearman rho",
+        "value": rho, "rho_untrained": rho0, "hit_ratio": hr, "hit_ratio_untrained": hr0,
+        "skip_scale": float(enc.params[-1].item()), "mse_first_epoch": hist[0], "mse_last_epoch": hist[-1],
+        "epochs": args.epochs, "train_pairs": int(len(tr_a)), "train_s": train_s,
+        "train_pairs_per_s": args.epochs * len(tr_a) / train_s, "label_s": label_s,
+        "label_pairs_per_s": (n + len(na)) / label_s, "neighbour_pairs_s": nb_s,
+        "label_max_rel_err_vs_fp64": label_err, "checkpoint": args.checkpoint or None}), flush=True)
 
 
 def run_knn(args):
@@ -745,11 +794,21 @@ def run_knn(args):
                     "calibration_recall": {str(k): v for k, v in rec.items()},
                     "recall_at_10": recall_at_k(f_i, ex_i), "speedup_vs_exhaustive": ex_s / f_s,
                     "index_build_s": build_s, "calibration_s": cal_s, "encoder_rho": ck.get("rho")})
-        # what training buys: the same filter with the untrained network, same budgets
+        out["branch_weight"] = index.beta
+        out["calibration_by_weight"] = {str(b): {str(k): v for k, v in r.items()}
+                                        for b, r in getattr(index, "calibration", {}).items()}
+        # what training buys: the same filter with the untrained network (its
+        # branch weight calibrated on the same sample), same budgets
         from trajsimimeasures_b200.surrogate import Encoder
         raw = SurrogateIndex(Encoder.init(Dset, seed=0), Dset)
-        out["recall_at_10_untrained"] = {str(cc): recall_at_k(raw.query(Q, 10, c=cc)[1], ex_i)
-                                         for cc in sorted(set(rec) | ({c} if c else set()))}
+        c_raw, _ = raw.calibrate(cal, 10, target=0.99)
+        out["untrained_calibrated"] = {"candidates": c_raw, "branch_weight": raw.beta}
+        counts = sorted(set(rec) | ({c} if c else set()) | {100, 200})
+        out["recall_at_10_trained"] = {str(cc): recall_at_k(index.query(Q, 10, c=cc)[1], ex_i) for cc in counts}
+        out["recall_at_10_untrained"] = {str(cc): recall_at_k(raw.query(Q, 10, c=cc)[1], ex_i) for cc in counts}
+        _, ex50 = knn_exhaustive(Q, Dset, 50)
+        out["hit_ratio"] = hit_ratios(Q, Dset, enc, ex50)
+        out["hit_ratio_untrained"] = hit_ratios(Q, Dset, raw.enc, ex50)
     out["host_generate_s"] = gen_s
     print(json.dumps(out), flush=True)
 

@@ -224,22 +224,59 @@ int tsm_select_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, 
                     void* stream);
 
 /*
+ * Candidate scan of the learned kNN filter on the tensor cores (tcgen05).
+ * Replaces the candidate generation of the reference's filter-and-refine kNN
+ * (query/cpp/DITA.cpp:276-431; the learned kNN's embedding scan,
+ * test_knn_time.py:138-202).  For embeddings of tsm_scan_dim() values
+ * (centred by the caller), d(q, j) = |e_j|^2 - 2 e_q . e_j, computed as one
+ * product of FP16 hi/lo splits, [q_hi | q_lo | q_hi] . [d_hi | d_hi | d_lo],
+ * with FP32 accumulation (about 2^-21 relative per product) and FP32 norms.
+ *   tsm_scan_prepare: operand image of n rows of emb (row stride ld floats),
+ *       scaled by `scale` (a power of two keeping |scale * emb| well inside
+ *       FP16's range); is_db = 1: database image (tiles of 256 rows) and
+ *       norms float32 [n]; 0: query image (tiles of 128 rows).  img: device
+ *       memory of tsm_scan_image_bytes(n, is_db) bytes, 16-byte aligned.
+ *   tsm_scan: either dense (thresholds NULL): dense[q * ld_dense + j] = d;
+ *       or candidate lists (dense NULL): for each pair with d <= thresholds[q]
+ *       a slot of counts[q] (zeroed by the caller) is taken and, below cap,
+ *       cand_idx[q * cap + slot] = j, cand_d[q * cap + slot] = d (any order;
+ *       counts[q] > cap means the list overflowed).  The same d in both modes.
+ *       status: device int, OR-ed with 1/2/8 when a bounded wait inside the
+ *       kernel ran out (results then incomplete), 4 when tensor memory was
+ *       left allocated because MMAs were still pending (reset the device).
+ */
+int32_t tsm_scan_dim(void);
+int64_t tsm_scan_image_bytes(int64_t n_rows, int32_t is_db);
+int tsm_scan_prepare(const float* emb, int64_t n, int64_t ld, float scale, int32_t is_db, void* img, float* norms,
+                     void* stream);
+int tsm_scan(const void* q_img, int64_t nq, const void* db_img, const float* db_norms, int64_t nd, float scale,
+             const float* thresholds, int32_t cap, int32_t* cand_idx, float* cand_d, int32_t* counts, float* dense,
+             int64_t ld_dense, int32_t* status, void* stream);
+/* tsm_scan with its wait limit in SM clocks (tsm_scan uses about 1 s). */
+int tsm_scan_opts(const void* q_img, int64_t nq, const void* db_img, const float* db_norms, int64_t nd, float scale,
+                  const float* thresholds, int32_t cap, int32_t* cand_idx, float* cand_d, int32_t* counts,
+                  float* dense, int64_t ld_dense, int32_t* status, int64_t wait_cycles, void* stream);
+
+/*
  * Learned candidate filter (trajectory encoder).  The reference's learned
  * measures embed trajectories and train on heuristic distances normalised by
  * their maximum with an MSE loss (nn/MLP_trajsimi_train.py:74-84,197-200); this
  * encoder (conv 2->64 k=5 + GRU 64->128 + linear 128->128, BF16 weights, FP32
- * accumulation) is trained the same way on DTW labels from tsm_pairs and
- * serves as a kNN filter.
+ * accumulation, plus a geometric skip: the trajectory's 16 points at indices
+ * round(k (n-1) / 15), normalised, times one learned scale, appended as 32
+ * more embedding values) is trained the same way on DTW labels from
+ * tsm_pairs and serves as a kNN filter.  Embeddings are 160 floats.
  *   params  float32 [tsm_enc_param_count()] master weights (layout: conv W
  *           [64][2][5], b [64]; W_ih [384][64], b_ih [384]; W_hh [384][128],
- *           b_hh [384]; W_o [128][128], b_o [128]; gate order r, z, n)
+ *           b_hh [384]; W_o [128][128], b_o [128]; skip scale [1]; gate order
+ *           r, z, n)
  *   pts/off/len  a packed batch of B trajectories, T = max length in it
  *   nrm     HOST float[4] = (mean_x, mean_y, 1/std_x, 1/std_y) input scaling
  *   workspace  device memory of tsm_enc_workspace_bytes(B, T, P) bytes
  */
 int tsm_enc_param_count(void);
 int64_t tsm_enc_workspace_bytes(int32_t B, int32_t T, int32_t P);
-/* emb float32 [B][128] (device) */
+/* emb float32 [B][160] (device) */
 int tsm_enc_forward(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
                     int32_t T, const float* nrm, void* workspace, float* emb, void* stream);
 /* Inference-only forward on the tensor cores (tcgen05): 128 trajectories per
@@ -247,7 +284,7 @@ int tsm_enc_forward(const float* params, const float* pts, const int64_t* off, c
  * with a_t and h_t entering the products as BF16 (the training forward above
  * keeps them FP32), and no training caches.  Used to embed the kNN database
  * and the queries: the test-time embedding of the reference's learned
- * measures (nn/MLP_trajsimi_train.py).  emb float32 [B][128] (device);
+ * measures (nn/MLP_trajsimi_train.py).  emb float32 [B][160] (device);
  * workspace of tsm_enc_embed_workspace_bytes(B, T) bytes.  Batches of similar
  * lengths waste fewer steps (a CTA runs its longest trajectory's length). */
 int64_t tsm_enc_embed_workspace_bytes(int32_t B, int32_t T);
@@ -276,6 +313,14 @@ int tsm_enc_embed_opts(const float* params, const float* pts, const int64_t* off
 int tsm_enc_loss_grad(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
                       int32_t T, const float* nrm, const int32_t* ia, const int32_t* ib, const float* y, int32_t P,
                       void* workspace, float* grad, float* loss, float* pred, void* stream);
+/* The same with per-pair weights (device float32 [P], nullable = all 1):
+ * loss = mean_p w_p (||e_ia - e_ib|| - y_p)^2.  Weights 1 / y_p^2 give the
+ * relative error, which keeps the near pairs (the ones a kNN filter must
+ * order) from vanishing next to the far ones. */
+int tsm_enc_loss_grad_w(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
+                        int32_t T, const float* nrm, const int32_t* ia, const int32_t* ib, const float* y,
+                        const float* weights, int32_t P, void* workspace, float* grad, float* loss, float* pred,
+                        void* stream);
 /* One Adam step on params with moments m, v (device, param_count each). */
 int tsm_enc_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr, float beta1,
                  float beta2, float eps, void* stream);

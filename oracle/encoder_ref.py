@@ -5,7 +5,8 @@ PyTorch float64 ops on the CPU so that autograd gives the gradients the
 kernels must reproduce:
   conv   relu(conv1d(x, W1, b1, padding=2))        64 channels, k=5
   GRU    r, z, n gates (order r, z, n), hidden 128, one step per point
-  head   e = Wo h_last + bo
+  head   e = [Wo h_last + bo | sc * r], r = the 16 points at indices
+         round(k (n - 1) / 15) (halves up), normalised, 0 for an empty trajectory
   loss   mean_p (||e_a - e_b||_2 - y_p)^2
 Conv and GRU weights are taken at their BF16-rounded values (as the kernels
 use them); the head is FP32.  Gradients are with respect to those values.
@@ -17,7 +18,8 @@ import numpy as np
 import torch
 
 SIZES = [("conv_w", (64, 2, 5)), ("conv_b", (64,)), ("w_ih", (384, 64)), ("b_ih", (384,)),
-         ("w_hh", (384, 128)), ("b_hh", (384,)), ("w_o", (128, 128)), ("b_o", (128,))]
+         ("w_hh", (384, 128)), ("b_hh", (384,)), ("w_o", (128, 128)), ("b_o", (128,)), ("skip_scale", (1,))]
+NS = 16
 BF16 = {"conv_w", "w_ih", "w_hh"}
 
 
@@ -61,17 +63,26 @@ def embed(W, trajs, nrm, bf16_operands=False):
                 z = torch.sigmoid(gi[128:256] + gh[128:256])
                 nn_ = torch.tanh(gi[256:] + r * gh[256:])
                 h = (1 - z) * nn_ + z * h
-        embs.append(W["w_o"] @ h + W["b_o"])
+        if n > 0:
+            idx = [(2 * k * (n - 1) + NS - 1) // (2 * (NS - 1)) for k in range(NS)]
+            r = x[idx].reshape(-1)
+        else:
+            r = torch.zeros(2 * NS, dtype=torch.float64)
+        embs.append(torch.cat([W["w_o"] @ h + W["b_o"], W["skip_scale"] * r]))
     return torch.stack(embs)
 
 
-def loss_grad(params, trajs, nrm, ia, ib, y):
-    """-> (loss float, grad float64 [n_params] in the flat layout, pred [P])."""
+def loss_grad(params, trajs, nrm, ia, ib, y, w=None):
+    """-> (loss float, grad float64 [n_params] in the flat layout, pred [P]);
+    w: per-pair loss weights (None = 1)."""
     W = unpack(params)
     e = embed(W, trajs, nrm)
     d = e[torch.as_tensor(ia)] - e[torch.as_tensor(ib)]
     pred = torch.linalg.vector_norm(d, dim=1)
-    loss = ((pred - torch.as_tensor(np.asarray(y), dtype=torch.float64)) ** 2).mean()
+    sq = (pred - torch.as_tensor(np.asarray(y), dtype=torch.float64)) ** 2
+    if w is not None:
+        sq = sq * torch.as_tensor(np.asarray(w, dtype=np.float32), dtype=torch.float64)
+    loss = sq.mean()
     loss.backward()
     g = torch.cat([W[name].grad.reshape(-1) for name, _ in SIZES])
     return float(loss.item()), g.numpy(), pred.detach().numpy()

@@ -25,9 +25,10 @@ def test_encoder_gradients_match_fp64_autograd():
     # larger weights than the init so that the gates leave their linear range
     enc.params.mul_(3.0)
     ia, ib, y = np.array([0, 1, 2, 4, 5]), np.array([1, 2, 4, 5, 3]), np.array([0.1, 0.5, 0.2, 0.9, 0.3])
-    loss, grad, pred = enc.loss_grad(s, np.arange(6), ia, ib, y)
+    w = np.array([1.0, 4.0, 25.0, 1.2, 11.1], dtype=np.float32)  # relative-error weights 1 / y^2
+    loss, grad, pred = enc.loss_grad(s, np.arange(6), ia, ib, y, w)
     torch.cuda.synchronize()
-    l_ref, g_ref, p_ref = R.loss_grad(enc.params.cpu().numpy(), trajs, enc.nrm, ia, ib, y)
+    l_ref, g_ref, p_ref = R.loss_grad(enc.params.cpu().numpy(), trajs, enc.nrm, ia, ib, y, w)
     np.testing.assert_allclose(pred.cpu().numpy(), p_ref, rtol=2e-5, atol=1e-6)
     assert abs(loss.item() - l_ref) <= 1e-4 * abs(l_ref) + 1e-7
     g = grad.cpu().numpy().astype(np.float64)
@@ -100,20 +101,23 @@ def test_training_learns_dtw_order():
     before = spearman(enc.predict_pairs(s, pa[hold], pb[hold]), y[hold])
     hist = enc.fit(s, pa[:27000], pb[:27000], y[:27000], epochs=6, batch_pairs=1024, lr=3e-3)
     after = spearman(enc.predict_pairs(s, pa[hold], pb[hold]), y[hold])
-    assert hist[-1] < hist[0]
-    assert after > 0.8 and after > before + 0.1, (before, after)
+    assert hist[-1] < 0.5 * hist[0], hist
+    assert after > 0.8 and after > before, (before, after)
 
 
-def test_trained_filter_gains_over_exhaustive_and_falls_back():
-    """What the learned part buys over the method without it (exhaustive exact
-    DP): the trained encoder's candidates plus exact rerank reach recall@10 >=
-    0.99 while evaluating at most 2 % of the database per query (counted in DP
-    evaluations, not timed).  A filter that cannot reach the target inside its
-    budget hands the queries to the exhaustive search (exact results)."""
+def test_trained_filter_gains_over_untrained_and_exhaustive_and_falls_back():
+    """What the learned part buys.  Over the same network untrained (same
+    architecture, same initial weights, same candidate count): a higher
+    recall@10 of the candidate sets.  Over the method without it
+    (exhaustive exact DP): the trained encoder's candidates plus exact rerank
+    reach recall@10 >= 0.99 while evaluating at most 2 % of the database per
+    query (counted in DP evaluations, not timed).  A filter that cannot reach
+    the target inside its budget hands the queries to the exhaustive search
+    (exact results)."""
     from trajsimimeasures_b200 import datagen as D
     from trajsimimeasures_b200.engine import TrajSet
     from trajsimimeasures_b200.knn import SurrogateIndex, knn_exhaustive, recall_at_k
-    from trajsimimeasures_b200.surrogate import Encoder, dtw_labels
+    from trajsimimeasures_b200.surrogate import Encoder, dtw_labels, neighbour_pairs
     N = 20000
     p, o, l = D.trajectory_set(N, seed=12)
     Dset = TrajSet.from_packed(p, o, l)
@@ -121,10 +125,19 @@ def test_trained_filter_gains_over_exhaustive_and_falls_back():
     _, exact = knn_exhaustive(Q, Dset, 10)
     rng = np.random.default_rng(14)
     pa, pb = rng.integers(0, N, 40000), rng.integers(0, N, 40000)
+    na, nb = neighbour_pairs(Dset, 2000, k=10, seed=15)
+    pa, pb = np.concatenate([pa, na]), np.concatenate([pb, nb])
     lab = dtw_labels(Dset, pa, pb)
+    untrained = SurrogateIndex(Encoder.init(Dset, seed=2), Dset)
     enc = Encoder.init(Dset, seed=2)
-    enc.fit(Dset, pa, pb, lab / lab.max(), epochs=6, batch_pairs=1024, lr=3e-3)
+    enc.fit(Dset, pa, pb, lab / lab.max(), epochs=6, batch_pairs=1024, lr=3e-3, relative=True)
     idx = SurrogateIndex(enc, Dset)
+    # below saturation (a count where the untrained filter still misses
+    # answers): trained strictly better at 20 candidates and on average
+    rec = {c: (recall_at_k(idx.query(Q, 10, c=c)[1], exact), recall_at_k(untrained.query(Q, 10, c=c)[1], exact))
+           for c in (10, 20, 40)}
+    assert rec[20][0] > rec[20][1], rec
+    assert sum(t - u for t, u in rec.values()) > 0.02, rec
     idx.LADDER = (40, 80, 160, 320, 400)
     cal = TrajSet.from_packed(*D.trajectory_set(64, seed=15))
     c, rec = idx.calibrate(cal, 10, target=0.99, max_fraction=0.02)

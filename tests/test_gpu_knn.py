@@ -135,3 +135,101 @@ def test_matrix_gather_equals_matrix_entries(measure):
     if measure_id(measure) in (1, 2):
         np.testing.assert_array_equal(k[:, :301][ok], fc[qi[ok], cand[ok]])
         assert k[3, 5] == -1 and k[4, 7] == -1
+
+
+def _scan_case(n=20000, nq=300, seed=21):
+    """Embeddings like the filter's: 160 values, centred; queries are noisy
+    copies of database rows, so the nearest distances are tiny next to |e|^2."""
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    E = (torch.randn(n, 160, generator=g) * 0.3).cuda()
+    E -= E.double().mean(0).float()
+    rows = torch.randint(0, n, (nq,), generator=g).cuda()
+    Qe = E[rows] + (torch.randn(nq, 160, generator=g) * 1e-3).cuda()
+    return E, Qe
+
+
+def _scan_images(E, Qe, scale):
+    from trajsimimeasures_b200 import _lib
+    from trajsimimeasures_b200.engine import _ptr
+    lib = _lib.load()
+
+    def img(X, db):
+        b = torch.empty(lib.tsm_scan_image_bytes(X.shape[0], int(db)), dtype=torch.uint8, device="cuda")
+        nrm = torch.empty(X.shape[0], device="cuda") if db else None
+        assert lib.tsm_scan_prepare(_ptr(X), X.shape[0], X.stride(0), scale, int(db), _ptr(b), _ptr(nrm), None) == 0
+        return b, nrm
+    (dimg, norms), (qimg, _) = img(E, True), img(Qe, False)
+    return lib, dimg, norms, qimg
+
+
+def test_scan_dense_matches_fp64_and_lists_match_dense():
+    """tsm_scan (tcgen05, FP16 hi/lo split products, FP32 accumulation):
+    dense d = |e_j|^2 - 2 e_q.e_j within 1e-5 of |e_q||e_j| of the FP64 value
+    (a TF32 product is off by ~1e-3 of it) and the same top-50 up to near
+    ties; in list mode exactly the pairs whose dense value is <= the
+    threshold, with the dense values, over 3 query tiles (the last one
+    partial) and a partial last database tile."""
+    from trajsimimeasures_b200.engine import _ptr
+    E, Qe = _scan_case()
+    n, nq = E.shape[0], Qe.shape[0]
+    scale = float(2.0 ** np.floor(np.log2(16384.0 / float(torch.cat([E, Qe]).abs().max()))))
+    lib, dimg, norms, qimg = _scan_images(E, Qe, scale)
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    dense = torch.full((nq, n + 3), -7.0, device="cuda")
+    assert lib.tsm_scan(_ptr(qimg), nq, _ptr(dimg), _ptr(norms), n, scale, None, 0, None, None, None, _ptr(dense),
+                        n + 3, _ptr(st), None) == 0
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    d = dense[:, :n].double()
+    assert bool((dense[:, n:] == -7.0).all())  # nothing written past nd
+    E64, Q64 = E.double(), Qe.double()
+    ref = (E64 * E64).sum(1)[None, :] - 2.0 * Q64 @ E64.T
+    bound = Q64.norm(dim=1)[:, None] * E64.norm(dim=1)[None, :]
+    err = ((d - ref).abs() / bound).max().item()
+    assert err <= 1e-5, err
+    top_k = torch.topk(d, 50, dim=1, largest=False).indices.cpu().numpy()
+    top_r = torch.topk(ref, 50, dim=1, largest=False).indices.cpu().numpy()
+    overlap = np.mean([len(np.intersect1d(a, b)) / 50 for a, b in zip(top_k, top_r)])
+    assert overlap >= 0.98, overlap
+    # list mode: threshold at each query's 100th smallest dense value
+    thr = torch.kthvalue(dense[:, :n], 100, dim=1).values.contiguous()
+    cap = 160
+    idx = torch.full((nq, cap), -1, dtype=torch.int32, device="cuda")
+    dd = torch.full((nq, cap), float("inf"), device="cuda")
+    cnt = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    assert lib.tsm_scan(_ptr(qimg), nq, _ptr(dimg), _ptr(norms), n, scale, _ptr(thr), cap, _ptr(idx), _ptr(dd),
+                        _ptr(cnt), None, 0, _ptr(st), None) == 0
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    want = (dense[:, :n] <= thr[:, None])
+    np.testing.assert_array_equal(cnt.cpu().numpy(), want.sum(1).cpu().numpy())
+    dn = dense.cpu().numpy()
+    for q in range(nq):
+        c = int(cnt[q])
+        got = np.sort(idx[q, :c].cpu().numpy())
+        np.testing.assert_array_equal(got, np.nonzero(want[q].cpu().numpy())[0])
+        np.testing.assert_array_equal(np.sort(dd[q, :c].cpu().numpy()), np.sort(dn[q, got]))
+
+
+def test_scan_candidates_match_fp64_ranking():
+    """SurrogateIndex-style candidates (sampled threshold, lists, exact
+    selection) equal the FP64 top-c up to near ties, for several counts; a
+    count that makes the list the whole database falls back to a dense scan."""
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.engine import TrajSet
+    from trajsimimeasures_b200.knn import SurrogateIndex
+    from trajsimimeasures_b200.surrogate import Encoder
+    p, o, l = D.trajectory_set(30000, seed=31)
+    Dset = TrajSet.from_packed(p, o, l)
+    Q = TrajSet.from_packed(*D.trajectory_set(200, seed=32))
+    idx = SurrogateIndex(Encoder.init(Dset, seed=3), Dset)
+    eq = idx.enc.embed(Q)
+    X = (idx.E * idx.wt).double()
+    Y = ((eq - idx.mu) * idx.wt).double()
+    ref = (X * X).sum(1)[None, :] - 2.0 * Y @ X.T
+    for c in (50, 300, 5000):
+        got = idx.candidates(Q, c).cpu().numpy()
+        want = torch.topk(ref, c, dim=1, largest=False).indices.cpu().numpy()
+        overlap = np.mean([len(np.intersect1d(a, b)) / c for a, b in zip(got, want)])
+        assert overlap >= 0.995, (c, overlap)
+        assert all(len(np.unique(r)) == c for r in got)

@@ -4,10 +4,15 @@
 //   conv   a_t = relu(b1 + sum_{k<5, i<2} W1[c][i][k] x_{t+k-2,i})   64 channels, zero padding
 //   GRU    r = s(Wir a + bir + Whr h + bhr),  z = s(Wiz a + biz + Whz h + bhz),
 //          n = tanh(Win a + bin + r * (Whn h + bhn)),  h' = (1-z) n + z h      hidden 128
-//   head   e = Wo h_n + bo                                                      128-d embedding
+//   head   e = [Wo h_n + bo | sc * r]                                           160-d embedding
+//          r = the 16 points at indices round(k (n - 1) / 15), normalised (32 values): a
+//          geometric skip around the recurrent branch, with one learned scale sc
 //   pair   d(a, b) = ||e_a - e_b||_2, trained with MSE against DTW / max DTW.
 // Conv and GRU weights are used as BF16 values (rounded from FP32 master
-// weights before each forward), all accumulation is FP32; the head is FP32.
+// weights before each forward), all accumulation is FP32; the head and the
+// skip are FP32 (a BF16 path cannot hold positions to the ~1e-4 of the box
+// that separates DTW neighbours among a million trajectories; the skip
+// carries them exactly).
 // The reference trains its learned measures the same way (MSE on
 // distance / max distance, nn/MLP_trajsimi_train.py:74-84,197-200).
 //
@@ -22,9 +27,9 @@
 //   enc_round_bf16    FP32 master -> BF16 weights
 //   enc_conv_fwd      conv + relu -> A [B][T][64]
 //   enc_gru_fwd       persistent GRU over T steps -> H [B][T+1][128] and gate caches
-//   enc_head_fwd      e = Wo h_last + bo
+//   enc_head_fwd      e = [Wo h_last + bo | sc r]
 //   enc_pair_loss     distances, MSE loss, dL/de (atomic)
-//   enc_head_bwd      dWo, dbo, dh_last
+//   enc_head_bwd      dWo, dbo, dh_last; enc_skip_bwd: d sc
 //   enc_gru_bwd       BPTT: gate gradients G [B][T][384] (input side), dA [B][T][64]
 //   enc_gemm_tn       split-K reduction dW[m][n] += sum_k A[k][m] B[k][n]  (weight gradients)
 //   enc_conv_bwd      dW1, db1
@@ -47,7 +52,10 @@ constexpr int C1 = 64;    // conv channels
 constexpr int KW = 5;     // conv width
 constexpr int HD = 128;   // hidden
 constexpr int G3 = 384;   // 3 gates
-constexpr int ED = 128;   // embedding
+constexpr int EO = 128;   // learned head outputs
+constexpr int NS = 16;    // resampled points of the geometric skip
+constexpr int SK = 2 * NS;  // skip features (x, y of each resampled point)
+constexpr int ED = EO + SK; // embedding: [head outputs | skip scale * resampled points]
 constexpr int S = 16;     // trajectories per GRU CTA
 constexpr int GRU_THREADS = 384;
 
@@ -59,8 +67,9 @@ constexpr int OFF_BIH = OFF_WIH + G3 * C1;   // [384]
 constexpr int OFF_WHH = OFF_BIH + G3;        // [384][128]
 constexpr int OFF_BHH = OFF_WHH + G3 * HD;   // [384]
 constexpr int OFF_WO = OFF_BHH + G3;         // [128][128]
-constexpr int OFF_BO = OFF_WO + ED * HD;     // [128]
-constexpr int N_PARAMS = OFF_BO + ED;
+constexpr int OFF_BO = OFF_WO + EO * HD;     // [128]
+constexpr int OFF_SC = OFF_BO + EO;          // [1] scale of the resampled-point skip
+constexpr int N_PARAMS = OFF_SC + 1;
 
 __device__ __forceinline__ float sigm(float x) { return 1.f / (1.f + expf(-x)); }
 
@@ -207,16 +216,37 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
     }
 }
 
-// E[b][o] = bo[o] + sum_k Wo[o][k] hl[b][k] (bias first, k ascending).  One
-// thread per output o, HEAD_B trajectories per CTA, their hidden states
-// staged in shared memory; each W_o row is read once per CTA.
+// Point index of resampled point k (0 <= k < NS) of a trajectory of n >= 1
+// points: round(k (n - 1) / (NS - 1)), halves rounded up, in integers.
+__device__ __forceinline__ int skip_index(int k, int n) { return (2 * k * (n - 1) + (NS - 1)) / (2 * (NS - 1)); }
+
+// E[b][o] = bo[o] + sum_k Wo[o][k] hl[b][k] (bias first, k ascending) for
+// o < EO; E[b][EO + 2 k + i] = sc * coordinate i of resampled point k (the
+// normalised input at skip_index(k, n); 0 for an empty trajectory), the
+// geometric skip, written unscaled to X[b][2 k + i] too when X is given (the
+// training forward keeps it for the gradient of sc).  One thread per head
+// output o, HEAD_B trajectories per CTA, their hidden states staged in
+// shared memory; each W_o row is read once per CTA.
 constexpr int HEAD_B = 32;
-__global__ void __launch_bounds__(ED) enc_head_fwd(const float* __restrict__ hl, int B, const float* __restrict__ p,
-                                                   float* __restrict__ E) {
+__global__ void __launch_bounds__(EO) enc_head_fwd(const float* __restrict__ hl, int B, const float* __restrict__ p,
+                                                   float* __restrict__ E, const float2* __restrict__ pts,
+                                                   const int64_t* __restrict__ off, const int32_t* __restrict__ len,
+                                                   float4 nrm, float* __restrict__ X) {
     __shared__ __align__(16) float hs[HEAD_B][HD];
     const int o = threadIdx.x;
     const int64_t b0 = (int64_t)blockIdx.x * HEAD_B;
-    for (int e = o; e < HEAD_B * HD; e += ED) {
+    const float sc = p[OFF_SC];
+    for (int e = o; e < HEAD_B * SK; e += EO) {
+        const int64_t b = b0 + e / SK;
+        const int q = e % SK;
+        if (b < B) {
+            const int n = len[b];
+            const float x = n > 0 ? xin(pts, off[b], n, skip_index(q >> 1, n), q & 1, nrm) : 0.f;
+            E[b * ED + EO + q] = sc * x;
+            if (X) X[b * SK + q] = x;
+        }
+    }
+    for (int e = o; e < HEAD_B * HD; e += EO) {
         const int64_t b = b0 + e / HD;
         hs[e / HD][e % HD] = b < B ? hl[b * HD + e % HD] : 0.f;
     }
@@ -239,11 +269,12 @@ __global__ void __launch_bounds__(ED) enc_head_fwd(const float* __restrict__ hl,
         if (b0 + j < B) E[(b0 + j) * ED + o] = acc[j];
 }
 
-// One warp per pair: pred = ||E[ia]-E[ib]||, loss += (pred-y)^2 / P,
-// dE[ia] += 2 (pred-y)/P * (E[ia]-E[ib])/pred, dE[ib] -= the same.
+// One warp per pair: pred = ||E[ia]-E[ib]|| (all ED embedding values), loss += w (pred-y)^2 / P,
+// dE[ia] += 2 w (pred-y)/P * (E[ia]-E[ib])/pred, dE[ib] -= the same; w = wt[p] (1 without weights).
 __global__ void enc_pair_loss(const float* __restrict__ E, const int32_t* __restrict__ ia,
-                              const int32_t* __restrict__ ib, const float* __restrict__ y, int P,
-                              float* __restrict__ pred, float* __restrict__ loss, float* __restrict__ dE) {
+                              const int32_t* __restrict__ ib, const float* __restrict__ y,
+                              const float* __restrict__ wt, int P, float* __restrict__ pred,
+                              float* __restrict__ loss, float* __restrict__ dE) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= P) return;
@@ -260,12 +291,13 @@ __global__ void enc_pair_loss(const float* __restrict__ E, const int32_t* __rest
     for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
     const float pr = sqrtf(ss);
     const float err = pr - y[w];
+    const float wp = wt ? wt[w] : 1.f;
     if (lane == 0) {
         pred[w] = pr;
-        if (loss) atomicAdd(loss, err * err / P);
+        if (loss) atomicAdd(loss, wp * err * err / P);
     }
     if (dE && pr > 0.f) {
-        const float g = 2.f * err / (P * pr);
+        const float g = 2.f * wp * err / (P * pr);
 #pragma unroll
         for (int q = 0; q < ED / 32; ++q) {
             atomicAdd(dE + (int64_t)ia[w] * ED + lane + 32 * q, g * d[q]);
@@ -278,7 +310,7 @@ __global__ void enc_pair_loss(const float* __restrict__ E, const int32_t* __rest
 // dhl[b][k] = sum_o Wo[o][k] dE[b][o].
 __global__ void enc_head_bwd_w(const float* __restrict__ dE, const float* __restrict__ hl, int B,
                                float* __restrict__ grad) {
-    const int o = blockIdx.x;  // 128 blocks
+    const int o = blockIdx.x;  // EO blocks
     const int k = threadIdx.x; // 128 threads
     float acc = 0.f, accb = 0.f;
     for (int b = 0; b < B; ++b) {
@@ -296,8 +328,20 @@ __global__ void enc_head_bwd_h(const float* __restrict__ dE, int B, const float*
     const int k = gid % HD;
     const int64_t b = gid / HD;
     float acc = 0.f;
-    for (int o = 0; o < ED; ++o) acc = fmaf(p[OFF_WO + o * HD + k], dE[b * ED + o], acc);
+    for (int o = 0; o < EO; ++o) acc = fmaf(p[OFF_WO + o * HD + k], dE[b * ED + o], acc);
     dhl[gid] = acc;
+}
+
+// d sc += sum_b sum_q dE[b][EO + q] X[b][q] (the skip scale's gradient).
+__global__ void enc_skip_bwd(const float* __restrict__ dE, const float* __restrict__ X, int B,
+                             float* __restrict__ grad) {
+    float acc = 0.f;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)B * SK;
+         e += (int64_t)gridDim.x * blockDim.x)
+        acc = fmaf(dE[(e / SK) * ED + EO + e % SK], X[e], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(grad + OFF_SC, acc);
 }
 
 // BPTT.  CTA = S trajectories, 384 threads.  Shared memory: Whh [384][128]
@@ -824,7 +868,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfl
 namespace {
 
 struct EncWs {  // views into the caller's workspace
-    float *A, *H, *R, *Z, *N, *GHN, *G, *GH, *dA, *hl, *E, *dE, *dhl, *pred, *loss;
+    float *A, *H, *R, *Z, *N, *GHN, *G, *GH, *dA, *hl, *E, *dE, *dhl, *pred, *loss, *X;
     __nv_bfloat16* wq;
 };
 
@@ -853,6 +897,7 @@ int64_t ws_layout(int B, int T, int P, float* base, EncWs* w) {
     take(&x->E, (int64_t)B * enc::ED);
     take(&x->dE, (int64_t)B * enc::ED);
     take(&x->dhl, (int64_t)B * enc::HD);
+    take(&x->X, (int64_t)B * enc::SK);
     take(&x->pred, P > 0 ? P : 1);
     take(&x->loss, 1);
     float* wqf = nullptr;
@@ -894,7 +939,9 @@ int enc_forward(const float* params, const float* pts, const int64_t* off, const
     if (rc) return rc;
     enc_gru_fwd<<<(B + S - 1) / S, GRU_THREADS, kGruFwdSmem, s>>>(w.A, len, B, T, w.wq, params, w.H, w.R, w.Z, w.N,
                                                                    w.GHN, w.hl);
-    enc_head_fwd<<<(unsigned)((B + HEAD_B - 1) / HEAD_B), ED, 0, s>>>(w.hl, B, params, w.E);
+    enc_head_fwd<<<(unsigned)((B + HEAD_B - 1) / HEAD_B), EO, 0, s>>>(w.hl, B, params, w.E,
+                                                                      reinterpret_cast<const float2*>(pts), off, len,
+                                                                      n4, w.X);
     return enc_check(cudaGetLastError(), "encoder forward launch");
 }
 
@@ -902,7 +949,9 @@ int enc_backward(const float* params, const float* pts, const int64_t* off, cons
                  const float* nrm, EncWs& w, float* grad, cudaStream_t s) {
     using namespace enc;
     const float4 n4 = make_float4(nrm[0], nrm[1], nrm[2], nrm[3]);
-    enc_head_bwd_w<<<ED, HD, 0, s>>>(w.dE, w.hl, B, grad);
+    enc_head_bwd_w<<<EO, HD, 0, s>>>(w.dE, w.hl, B, grad);
+    enc_skip_bwd<<<(unsigned)(((int64_t)B * SK + 255) / 256 < 256 ? ((int64_t)B * SK + 255) / 256 : 256), 256, 0, s>>>(
+        w.dE, w.X, B, grad);
     enc_head_bwd_h<<<(unsigned)(((int64_t)B * HD + 255) / 256), 256, 0, s>>>(w.dE, B, params, w.dhl);
     int rc = enc_check(cudaFuncSetAttribute(enc_gru_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, kGruBwdSmem),
                        "cudaFuncSetAttribute(enc_gru_bwd)");
@@ -982,9 +1031,10 @@ int tsm_enc_forward(const float* params, const float* pts, const int64_t* off, c
     return rc;
 }
 
-int tsm_enc_loss_grad(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
-                      int32_t T, const float* nrm, const int32_t* ia, const int32_t* ib, const float* y, int32_t P,
-                      void* workspace, float* grad, float* loss, float* pred, void* stream) {
+int tsm_enc_loss_grad_w(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
+                        int32_t T, const float* nrm, const int32_t* ia, const int32_t* ib, const float* y,
+                        const float* weights, int32_t P, void* workspace, float* grad, float* loss, float* pred,
+                        void* stream) {
     int rc = enc_args(params, pts, off, len, B, T, nrm, workspace);
     if (rc) return rc;
     if (P < 1 || !ia || !ib || !y || !grad) return tsm_internal_fail(TSM_EINVAL, "tsm_enc_loss_grad: bad pairs");
@@ -996,12 +1046,19 @@ int tsm_enc_loss_grad(const float* params, const float* pts, const int64_t* off,
     if ((rc = enc_check(cudaMemsetAsync(w.dE, 0, (size_t)B * enc::ED * 4, s), "memset dE"))) return rc;
     if ((rc = enc_check(cudaMemsetAsync(w.loss, 0, 4, s), "memset loss"))) return rc;
     if ((rc = enc_check(cudaMemsetAsync(grad, 0, (size_t)enc::N_PARAMS * 4, s), "memset grad"))) return rc;
-    enc::enc_pair_loss<<<(P * 32 + 255) / 256, 256, 0, s>>>(w.E, ia, ib, y, P, w.pred, w.loss, w.dE);
+    enc::enc_pair_loss<<<(P * 32 + 255) / 256, 256, 0, s>>>(w.E, ia, ib, y, weights, P, w.pred, w.loss, w.dE);
     rc = enc_backward(params, pts, off, len, B, T, nrm, w, grad, s);
     if (rc) return rc;
     if (loss) rc = enc_check(cudaMemcpyAsync(loss, w.loss, 4, cudaMemcpyDeviceToDevice, s), "copy loss");
     if (!rc && pred) rc = enc_check(cudaMemcpyAsync(pred, w.pred, (size_t)P * 4, cudaMemcpyDeviceToDevice, s), "copy pred");
     return rc;
+}
+
+int tsm_enc_loss_grad(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
+                      int32_t T, const float* nrm, const int32_t* ia, const int32_t* ib, const float* y, int32_t P,
+                      void* workspace, float* grad, float* loss, float* pred, void* stream) {
+    return tsm_enc_loss_grad_w(params, pts, off, len, B, T, nrm, ia, ib, y, nullptr, P, workspace, grad, loss, pred,
+                               stream);
 }
 
 int tsm_enc_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr, float beta1,
@@ -1041,7 +1098,9 @@ int tsm_enc_embed_opts(const float* params, const float* pts, const int64_t* off
     if (rc) return rc;
     enc_gru_embed_tc<<<Bp / TC_M, TC_THREADS, TC_SMEM, s>>>(w.Ab, len, B, T, w.wq, params, w.hl, w.status,
                                                             wait_cycles, stall_step);
-    enc_head_fwd<<<(unsigned)((B + HEAD_B - 1) / HEAD_B), ED, 0, s>>>(w.hl, B, params, emb);
+    enc_head_fwd<<<(unsigned)((B + HEAD_B - 1) / HEAD_B), EO, 0, s>>>(w.hl, B, params, emb,
+                                                                      reinterpret_cast<const float2*>(pts), off, len,
+                                                                      n4, nullptr);
     return enc_check(cudaGetLastError(), "tsm_enc_embed launch");
 }
 

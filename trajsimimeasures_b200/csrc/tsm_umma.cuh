@@ -34,6 +34,12 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo_bytes
     return d;
 }
 
+// Instruction descriptor of kind::f16 with FP16 A and B (both K-major) and an
+// FP32 accumulator: the BF16 form below with A and B format 0 (F16).
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int m, int n) {
+    return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
 // Instruction descriptor of kind::f16 with BF16 A and B (both K-major) and an
 // FP32 accumulator: D format bits 4-5 = 1 (F32), A format bits 7-9 = 1 (BF16),
 // B format bits 10-12 = 1 (BF16), N / 8 in bits 17-22, M / 16 in bits 24-28.
@@ -87,6 +93,11 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar_saddr, uint32_t parity, l
         if (done) return true;
         if (clock64() - t0 > max_cycles) return false;
     }
+}
+
+// One plain arrival on the mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint32_t bar_saddr) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar_saddr) : "memory");
 }
 
 // Arrival on the mbarrier that also expects `bytes` of asynchronous copies

@@ -18,6 +18,7 @@ its GPU refinement bridge Traj::TrajSimiGPU is broken as shipped).  Here:
 from __future__ import annotations
 
 import ctypes
+import math
 
 import numpy as np
 import torch
@@ -144,73 +145,137 @@ def select_rows(d: torch.Tensor, k: int, stream=None) -> torch.Tensor:
 
 class SurrogateIndex:
     """Database embeddings of a trained encoder, used to pick kNN candidates:
-    the c database trajectories nearest to a query in embedding space
-    (squared L2 via one TF32 matrix product on mean-centred embeddings with
-    the squared norms folded in, then the sampled-threshold selection kernel),
-    then reranked by exact DP.
+    the c database trajectories nearest to a query in embedding space, then
+    reranked by exact DP.
 
-    The candidate count is calibrated, not guessed: ``calibrate`` runs the
-    exhaustive search on a sample of queries and takes the smallest count of
-    a ladder whose recall@k reaches the target; if none does within the
-    speed budget, queries fall back to the exhaustive search."""
+    Candidate scan (tsm_scan, tensor cores): embeddings centred on the
+    database mean, split into FP16 hi/lo pairs, |e_j|^2 - 2 e_q.e_j from one
+    split product in FP32 accumulation (about 2^-21 relative per product: a
+    TF32 product, at 2^-11, cannot separate the nearest of a million
+    trajectories).  A threshold per query comes from a dense scan of a fixed
+    sample of SAMPLE database rows (the order statistic whose expected count
+    in the full database is 1.25 c plus four standard deviations); the full
+    scan keeps only the pairs under it, in per-query lists, and the exact c
+    smallest are selected from those.  A query whose list holds fewer than c
+    or overflowed is scanned densely instead.
 
-    LADDER = (200, 500, 1000, 1500, 2000, 2500, 3000, 4000, 5000, 7000, 10000, 20000, 50000)
+    Two things are calibrated, not guessed: the weight of the recurrent
+    branch against the geometric skip in the scan's distance (BRANCH_WEIGHTS;
+    the training objective, a regression on distances, does not set the
+    balance that ranks the nearest few best) and the candidate count (LADDER).
+    ``calibrate`` runs the exhaustive search on a sample of queries and takes
+    the smallest count, over the weights, whose recall@k reaches the target;
+    if none does within the speed budget, queries fall back to the
+    exhaustive search."""
 
-    # embedding width + 1 (the squared norm), padded to a multiple of 4 floats
-    AUG = 132
+    LADDER = (100, 200, 300, 500, 700, 1000, 1500, 2000, 3000, 5000, 7000, 10000, 20000, 50000)
+    BRANCH_WEIGHTS = (1.0, 0.5, 0.3, 0.1)
+    SAMPLE = 16384
+    FP16_TOP = 16384.0  # largest scaled magnitude (FP16 holds 65504)
 
-    def __init__(self, encoder, D: TrajSet, batch=None):
+    def __init__(self, encoder, D: TrajSet, batch=None, branch_weight=1.0):
         self.enc = encoder
         self.D = D
         emb = encoder.embed(D, batch=batch)
-        w = emb.shape[1]
-        # Embeddings are centred on the database mean mu (distances do not
-        # change): a TF32 product rounds its inputs to 11 significant bits,
-        # relative to their size, and a trained network's embeddings share a
-        # large common offset.  Measured on the trained encoder (1,000 queries
-        # x 1M, recall@10 at 200 / 5,000 candidates): FP32 0.463 / 0.9998,
-        # TF32 0.202 / 0.998, centred TF32 0.437 / 0.9998.
-        self.mu = emb.mean(0)
-        emb = emb - self.mu
-        # augmented rows [e_j, |e_j|^2, 0...]: one product with [-2 e_q, 1, 0...]
-        # gives |e_j|^2 - 2 e_q.e_j, the squared distance less the query's own
-        # |e_q|^2, which does not change a query's ranking
-        self.aug = torch.zeros((emb.shape[0], max(self.AUG, (w + 4) // 4 * 4)), dtype=torch.float32,
-                               device=emb.device)
-        self.aug[:, :w] = emb
-        self.aug[:, w] = (emb * emb).sum(1)
-        self.width = w
+        self.width = emb.shape[1]
+        if self.width != _lib.load().tsm_scan_dim():
+            raise ValueError(f"the scan takes {_lib.load().tsm_scan_dim()}-value embeddings, got {self.width}")
+        self.mu = emb.double().mean(0).float()
+        self.E = emb - self.mu  # centred (distances do not change)
+        n = self.E.shape[0]
+        self.sample = torch.arange(0, n, max(1, n // self.SAMPLE), device=emb.device)[:self.SAMPLE]
+        self.status = torch.zeros(1, dtype=torch.int32, device=emb.device)
         self.c = None
+        self.set_branch_weight(branch_weight)
+
+    # -- operand images ------------------------------------------------------
+    def set_branch_weight(self, beta: float):
+        """Re-weights the recurrent branch (the first width - 32 values) in the
+        scan's distance and rebuilds the database operand images."""
+        self.beta = float(beta)
+        self.wt = torch.ones(self.width, dtype=torch.float32, device=self.E.device)
+        self.wt[:self.width - 32] = self.beta
+        X = self.E * self.wt
+        top = float(X.abs().max()) if X.numel() else 1.0
+        self.scale = float(2.0 ** math.floor(math.log2(self.FP16_TOP / max(top, 1e-30))))
+        self.img, self.norms = self._image(X, True)
+        self.s_img, self.s_norms = self._image(X[self.sample].contiguous(), True)
+
+    def _image(self, X, is_db):
+        lib = _lib.load()
+        n = X.shape[0]
+        img = torch.empty(max(lib.tsm_scan_image_bytes(n, int(is_db)), 16), dtype=torch.uint8, device=X.device)
+        norms = torch.empty(n, dtype=torch.float32, device=X.device) if is_db else None
+        rc = lib.tsm_scan_prepare(_ptr(X), n, X.stride(0), self.scale, int(is_db), _ptr(img), _ptr(norms),
+                                  _stream_ptr(None))
+        _lib.check(rc, "tsm_scan_prepare")
+        return img, norms
+
+    def _query_image(self, e):
+        X = ((e - self.mu) * self.wt).contiguous()
+        return self._image(X, False)[0]
 
     @property
     def emb(self) -> torch.Tensor:
         """Database embeddings [n, width]."""
-        return self.aug[:, :self.width] + self.mu
+        return self.E + self.mu
+
+    # -- scans ------------------------------------------------------------------
+    def _dense(self, qimg, nq, img, norms, nd):
+        out = torch.empty((nq, nd), dtype=torch.float32, device=self.E.device)
+        rc = _lib.load().tsm_scan(_ptr(qimg), nq, _ptr(img), _ptr(norms), nd, self.scale, None, 0, None, None, None,
+                                  _ptr(out), nd, _ptr(self.status), _stream_ptr(None))
+        _lib.check(rc, "tsm_scan")
+        return out
 
     def scan(self, e: torch.Tensor) -> torch.Tensor:
-        """Embedding-space distances (less |e_q - mu|^2) of queries e [b, width]
-        to every database trajectory: one TF32 tensor-core product, FP32
-        accumulation and output ([b, n] float32)."""
-        q = torch.zeros((e.shape[0], self.aug.shape[1]), dtype=torch.float32, device=e.device)
-        q[:, :self.width] = -2.0 * (e - self.mu)
-        q[:, self.width] = 1.0
-        mm = torch.backends.cuda.matmul
-        prev = mm.allow_tf32
-        mm.allow_tf32 = True
-        try:
-            return q @ self.aug.T
-        finally:
-            mm.allow_tf32 = prev
+        """Embedding-space distances (less |e_q - mu|^2 in the weighted
+        space) of queries e [b, width] to every database trajectory
+        ([b, n] float32, dense)."""
+        return self._dense(self._query_image(e), e.shape[0], self.img, self.norms, self.E.shape[0])
 
-    def candidates(self, Q: TrajSet, c: int, chunk=1024) -> torch.Tensor:
-        """Candidate indices [nq, c] (int64, any order).  chunk queries per
-        scan: one [chunk, n] float32 distance block (4 GB at 1024 x 1M); 1,000
-        queries x 1M on B200, ms: 4.76 at 256, 4.56 at 512, 4.23 at 1024."""
+    def _check_status(self):
+        st = int(self.status.item())
+        if st:
+            self.status.zero_()
+            raise _lib.TsmError(f"tsm_scan: a tensor-core wait ran out (status {st})")
+
+    def candidates(self, Q: TrajSet, c: int, chunk=4096) -> torch.Tensor:
+        """Candidate indices [nq, c] (int64, any order)."""
+        lib = _lib.load()
+        n = self.E.shape[0]
+        c = min(int(c), n)
         eq = self.enc.embed(Q)
         out = torch.empty((Q.n, c), dtype=torch.int64, device=Q.device)
+        S = int(self.sample.shape[0])
+        exp = c * S / n
+        ks = int(min(S, max(1, math.ceil(1.25 * exp + 4.0 * math.sqrt(exp)))))
+        expect = ks * n / S  # expected list length at the threshold
+        cap = int(min(n, math.ceil(expect + 6.0 * expect / math.sqrt(ks)) + 64))
         for q0 in range(0, Q.n, chunk):
-            d = self.scan(eq[q0:q0 + chunk])
-            out[q0:q0 + d.shape[0]] = select_rows(d, c).long()
+            e = eq[q0:q0 + chunk]
+            b = e.shape[0]
+            qimg = self._query_image(e)
+            if ks >= S or cap >= n:  # the list would hold most of the database: dense
+                out[q0:q0 + b] = select_rows(self._dense(qimg, b, self.img, self.norms, n), c).long()
+                continue
+            ds = self._dense(qimg, b, self.s_img, self.s_norms, S)
+            thr = torch.kthvalue(ds, ks, dim=1).values.contiguous()
+            idx = torch.empty((b, cap), dtype=torch.int32, device=Q.device)
+            dd = torch.full((b, cap), float("inf"), dtype=torch.float32, device=Q.device)
+            cnt = torch.zeros(b, dtype=torch.int32, device=Q.device)
+            rc = lib.tsm_scan(_ptr(qimg), b, _ptr(self.img), _ptr(self.norms), n, self.scale, _ptr(thr), cap,
+                              _ptr(idx), _ptr(dd), _ptr(cnt), None, 0, _ptr(self.status), _stream_ptr(None))
+            _lib.check(rc, "tsm_scan")
+            pos = select_rows(dd, c).long()
+            res = torch.gather(idx, 1, pos).long()
+            bad = torch.nonzero((cnt < c) | (cnt > cap)).flatten()
+            if bad.numel():  # threshold too tight or list overflowed: those queries densely
+                eb = e[bad]
+                res[bad] = select_rows(self._dense(self._query_image(eb), eb.shape[0], self.img, self.norms, n),
+                                       c).long()
+            out[q0:q0 + b] = res
+        self._check_status()
         return out
 
     def query(self, Q: TrajSet, k=10, c=None, measure="dtw", **kw):
@@ -221,27 +286,42 @@ class SurrogateIndex:
         return knn_rerank(Q, self.D, cand, k, measure, **kw)
 
     def calibrate(self, Q_sample: TrajSet, k=10, target=0.99, max_fraction=0.05, margin=None, measure="dtw",
-                  **kw):
-        """-> (chosen count or None, {count: recall}) on the sample.
+                  weights=None, **kw):
+        """-> (chosen count or None, {count: recall} at the chosen branch
+        weight) on the sample; sets self.c and the branch weight.
 
-        A count is chosen only if its sample recall clears the target by a
-        margin of two standard errors of a recall measured on n*k answers
-        (default), so that the recall on the full query set does not fall
-        below the target by sampling noise."""
+        For each branch weight (``weights``, default BRANCH_WEIGHTS) the
+        smallest count of the ladder whose sample recall clears the target by
+        a margin of two standard errors of a recall measured on n*k answers
+        (default) -- so that the recall on the full query set does not fall
+        below the target by sampling noise -- and the weight with the
+        smallest such count.  Recalls are judged on the candidate sets (the
+        exact rerank keeps every true answer a set contains)."""
         _, exact = knn_exhaustive(Q_sample, self.D, k, measure, **kw)
+        ex = exact.cpu().numpy()
         if margin is None:
             margin = 2.0 * float(np.sqrt(target * (1.0 - target) / (Q_sample.n * k)))
-        rec = {}
-        self.c = None
-        for c in self.LADDER:
-            if c > max_fraction * self.D.n and c > self.LADDER[0]:
-                break
-            _, got = self.query(Q_sample, k, c=c, measure=measure, **kw)
-            rec[c] = recall_at_k(got, exact)
-            if rec[c] >= min(target + margin, 1.0):
-                self.c = c
-                break
-        return self.c, rec
+        best, table = None, {}
+        for beta in (self.BRANCH_WEIGHTS if weights is None else weights):
+            self.set_branch_weight(beta)
+            rec = {}
+            for c in self.LADDER:
+                if (c > max_fraction * self.D.n and c > self.LADDER[0]) or (best is not None and c >= best[1]):
+                    break
+                got = self.candidates(Q_sample, c).cpu().numpy()
+                rec[c] = float(np.mean([len(np.intersect1d(got[i], ex[i])) / k for i in range(ex.shape[0])]))
+                if rec[c] >= min(target + margin, 1.0):
+                    best = (beta, c)
+                    break
+            table[beta] = rec
+        if best is None:
+            self.c = None
+            self.set_branch_weight(self.BRANCH_WEIGHTS[0] if weights is None else weights[0])
+            return None, table[next(iter(table))]
+        self.set_branch_weight(best[0])
+        self.c = best[1]
+        self.calibration = table
+        return self.c, table[best[0]]
 
 
 def merge_topk(dists: torch.Tensor, idx: torch.Tensor, k: int):

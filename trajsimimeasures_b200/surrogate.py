@@ -9,7 +9,7 @@ kernel (tsm_pairs) on the GPU.
 
     enc = Encoder.init(pool)                       # normalisation from the pool
     hist = enc.fit(pool, pa, pb, labels, epochs=…)  # labels already normalised
-    emb = enc.embed(pool)                          # [n, 128] float32 on the device
+    emb = enc.embed(pool)                          # [n, 160] float32 on the device
 """
 from __future__ import annotations
 
@@ -24,12 +24,13 @@ import torch
 from . import _lib
 from .engine import TrajSet, _ptr, _stream_ptr, pairs_in_set
 
-EMB = 128
+EMB = 160  # 128 head outputs + the geometric skip (16 resampled points x 2)
 # (fan_in, count) of the parameter blocks in layout order; PyTorch-style
 # uniform(-1/sqrt(k), 1/sqrt(k)) init with k = fan_in (conv: 2*5, GRU: 128,
-# head: 128)
+# head: 128); the skip scale starts at 1/sqrt(32) (fan-in of the 32 skip values)
 _BLOCKS = [("conv_w", 10, 64 * 2 * 5), ("conv_b", 10, 64), ("w_ih", 128, 384 * 64), ("b_ih", 128, 384),
-           ("w_hh", 128, 384 * 128), ("b_hh", 128, 384), ("w_o", 128, 128 * 128), ("b_o", 128, 128)]
+           ("w_hh", 128, 384 * 128), ("b_hh", 128, 384), ("w_o", 128, 128 * 128), ("b_o", 128, 128),
+           ("skip_scale", 32, 1)]
 
 
 def spearman(a, b) -> float:
@@ -70,6 +71,7 @@ class Encoder:
         dev = device or pool.device
         g = np.random.Generator(np.random.PCG64(seed))
         chunks = [g.uniform(-1 / math.sqrt(k), 1 / math.sqrt(k), n).astype(np.float32) for _, k, n in _BLOCKS]
+        chunks[-1][:] = 1 / math.sqrt(32)
         p = np.concatenate(chunks)
         assert p.size == cls.n_params()
         pts = pool.pts.double()
@@ -77,7 +79,26 @@ class Encoder:
         std = pts.std(0).cpu().numpy()
         nrm = np.array([mean[0], mean[1], 1.0 / max(std[0], 1e-12), 1.0 / max(std[1], 1e-12)], dtype=np.float32)
         t = torch.from_numpy(p).to(dev)
-        return cls(t, nrm, torch.zeros_like(t), torch.zeros_like(t))
+        enc = cls(t, nrm, torch.zeros_like(t), torch.zeros_like(t))
+        enc._balance_skip(pool, seed)
+        return enc
+
+    def _balance_skip(self, pool: TrajSet, seed=0, n=4096):
+        """Data-dependent initial skip scale: the embedding's two paths (the
+        recurrent branch's 128 outputs and the 32 resampled-point values)
+        contribute equal mean squared distances over random pairs of the pool,
+        the way weight-normalised networks set their scales from data at
+        initialisation (Salimans and Kingma, NeurIPS 2016).  Training then
+        decides how much of each path the distances use."""
+        g = np.random.Generator(np.random.PCG64(seed + 1))
+        idx = g.choice(pool.n, size=min(n, pool.n), replace=False)
+        self.params[-1] = 1.0
+        e = self.embed(pool, idx).double()
+        a, b = torch.from_numpy(g.permutation(len(idx))).to(e.device), torch.from_numpy(g.permutation(len(idx))).to(e.device)
+        d = e[a] - e[b]
+        fb = float((d[:, :EMB - 32] ** 2).sum(1).mean())
+        fs = float((d[:, EMB - 32:] ** 2).sum(1).mean())
+        self.params[-1] = math.sqrt(fb / fs) if fs > 0 and fb > 0 else 1.0 / math.sqrt(32)
 
     # -- device buffers ---------------------------------------------------------
     def _workspace(self, B, T, P):
@@ -98,7 +119,7 @@ class Encoder:
     TC_BATCH = 296 * 128
 
     def embed(self, s: TrajSet, idx=None, batch=None, stream=None, tensor_cores=True) -> torch.Tensor:
-        """Embeddings [n, 128] of trajectories idx (default all) of s.
+        """Embeddings [n, 160] of trajectories idx (default all) of s.
 
         tensor_cores=True: the tcgen05 inference kernel (tsm_enc_embed; a_t
         and h_t enter the gate products as BF16), over batches of similar
@@ -154,9 +175,10 @@ class Encoder:
         return out
 
     # -- training -----------------------------------------------------------------
-    def loss_grad(self, s: TrajSet, tidx, ia, ib, y, stream=None):
+    def loss_grad(self, s: TrajSet, tidx, ia, ib, y, w=None, stream=None):
         """Loss, gradient and predictions for pairs (ia, ib) over the batch of
-        trajectories tidx of s.  -> (loss tensor [1], grad [n_params], pred [P])."""
+        trajectories tidx of s; w: per-pair loss weights (None = 1).
+        -> (loss tensor [1], grad [n_params], pred [P])."""
         lib = _lib.load()
         tidx = torch.as_tensor(tidx, device=s.device).long()
         B = int(tidx.shape[0])
@@ -171,9 +193,10 @@ class Encoder:
         loss = torch.empty(1, dtype=torch.float32, device=s.device)
         pred = torch.empty(P, dtype=torch.float32, device=s.device)
         ws = self._workspace(B, T, P)
-        rc = lib.tsm_enc_loss_grad(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T, self._nrm_ptr(),
-                                   _ptr(ia), _ptr(ib), _ptr(y), P, _ptr(ws), _ptr(grad), _ptr(loss), _ptr(pred),
-                                   _stream_ptr(stream))
+        w = None if w is None else torch.as_tensor(w, device=s.device).float().contiguous()
+        rc = lib.tsm_enc_loss_grad_w(_ptr(self.params), _ptr(s.pts), _ptr(off), _ptr(ln), B, T, self._nrm_ptr(),
+                                     _ptr(ia), _ptr(ib), _ptr(y), _ptr(w), P, _ptr(ws), _ptr(grad), _ptr(loss),
+                                     _ptr(pred), _stream_ptr(stream))
         _lib.check(rc, "tsm_enc_loss_grad")
         return loss, grad, pred
 
@@ -183,25 +206,31 @@ class Encoder:
                                       float(lr), float(betas[0]), float(betas[1]), float(eps), _stream_ptr(stream))
         _lib.check(rc, "tsm_enc_adam")
 
-    def fit(self, s: TrajSet, pa, pb, y, *, epochs=5, batch_pairs=1024, lr=1e-3, seed=0, log=None):
+    def fit(self, s: TrajSet, pa, pb, y, *, epochs=5, batch_pairs=1024, lr=1e-3, seed=0, log=None,
+            relative=False, floor=1e-3):
         """Trains on pairs (pa[i], pb[i]) of s with targets y (normalised
-        distances).  Every step encodes the 2*batch_pairs endpoints."""
+        distances).  relative=True weights each pair by 1 / max(y, floor)^2
+        (relative squared error: near pairs count as much as far ones).
+        Every step encodes the 2*batch_pairs endpoints.  The loss is summed
+        on the device and read once per epoch (the host does not wait for
+        each step).  -> mean loss per epoch."""
         pa, pb, y = np.asarray(pa), np.asarray(pb), np.asarray(y, dtype=np.float32)
+        wts = (1.0 / np.maximum(y, floor) ** 2).astype(np.float32) if relative else None
         rng = np.random.Generator(np.random.PCG64(seed))
         hist = []
         n = len(pa)
         for ep in range(epochs):
             perm = rng.permutation(n)
-            tot, cnt = 0.0, 0
+            tot = torch.zeros(1, dtype=torch.float64, device=s.device)
             for b0 in range(0, n, batch_pairs):
                 sel = perm[b0:b0 + batch_pairs]
                 P = len(sel)
                 tidx = np.concatenate([pa[sel], pb[sel]])
-                loss, grad, _ = self.loss_grad(s, tidx, np.arange(P), P + np.arange(P), y[sel])
+                loss, grad, _ = self.loss_grad(s, tidx, np.arange(P), P + np.arange(P), y[sel],
+                                               None if wts is None else wts[sel])
                 self.adam(grad, lr=lr * 0.5 * (1 + math.cos(math.pi * (ep + b0 / n) / epochs)))
-                tot += float(loss.item()) * P
-                cnt += P
-            hist.append(tot / cnt)
+                tot += loss.double() * P
+            hist.append(float(tot.item()) / n)
             if log:
                 log(f"epoch {ep}: mse {hist[-1]:.3e}")
         return hist
@@ -215,6 +244,28 @@ class Encoder:
         ea = e[torch.from_numpy(inv[:len(pa)]).to(e.device)]
         eb = e[torch.from_numpy(inv[len(pa):]).to(e.device)]
         return torch.linalg.vector_norm(ea - eb, dim=1).cpu().numpy()
+
+
+def neighbour_pairs(s: TrajSet, n_anchors, k=20, seed=0, chunk=4096):
+    """Training pairs from the neighbourhoods that a kNN filter must order:
+    n_anchors trajectories of s drawn at random, each paired with its k
+    nearest trajectories of s by exact GPU DTW (itself excluded).  The
+    reference's learned baselines sample training pairs by distance for the
+    same reason (nn/NEUTRAJ_trajsimi_train.py:59,282-319).
+    -> (anchors int64 [n_anchors * k], neighbours int64 [n_anchors * k])."""
+    from .knn import _subset, knn_exhaustive
+    rng = np.random.Generator(np.random.PCG64(seed))
+    anc = np.sort(rng.choice(s.n, size=min(n_anchors, s.n), replace=False))
+    pa, pb = [], []
+    for a0 in range(0, len(anc), chunk):
+        a = anc[a0:a0 + chunk]
+        _, nb = knn_exhaustive(_subset(s, torch.as_tensor(a, device=s.device)), s, k + 1)
+        nb = nb.cpu().numpy()
+        for i, ai in enumerate(a):
+            row = nb[i][nb[i] != ai][:k]
+            pa.append(np.full(row.shape[0], ai, dtype=np.int64))
+            pb.append(row.astype(np.int64))
+    return np.concatenate(pa), np.concatenate(pb)
 
 
 def dtw_labels(s: TrajSet, pa, pb, batch=1 << 20):
