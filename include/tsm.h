@@ -76,8 +76,18 @@ int tsm_version(void);
 /* Last error message of the calling thread ("" if none). */
 const char* tsm_last_error(void);
 
-/* Largest trajectory length the kernels accept (points). */
+/* Largest trajectory length the paired kernels accept (points): 32768.
+ * Longer inputs are rejected with TSM_ETOOLONG (the reference's datasets are
+ * cut to 20..200 points, config.py:51-52, and its timing sweep reaches 1,600,
+ * test_trajsimi_time.py:109). */
 int32_t tsm_max_supported_len(void);
+
+/* Longest query of the matrix forms (tsm_matrix, tsm_matrix_gather,
+ * tsm_allpairs_sym; Hausdorff excepted): 1400 points, whose boundary rows and
+ * staged columns fill a CTA's shared memory.  Longer queries get
+ * TSM_ETOOLONG; the Python layer (core.matrix, core.allpairs,
+ * core.matrix_many) computes their rows with tsm_pairs instead. */
+int32_t tsm_matrix_query_max(void);
 
 /*
  * Paired batch: out[k] = measure(traj a_k, traj b_k) for k < n_pairs.
@@ -234,8 +244,9 @@ int tsm_select_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, 
  *   tsm_scan_prepare: operand image of n rows of emb (row stride ld floats),
  *       scaled by `scale` (a power of two keeping |scale * emb| well inside
  *       FP16's range); is_db = 1: database image (tiles of 256 rows) and
- *       norms float32 [n]; 0: query image (tiles of 128 rows).  img: device
- *       memory of tsm_scan_image_bytes(n, is_db) bytes, 16-byte aligned.
+ *       norms float32 [tsm_scan_norms_count(n)] (the padding rows get +inf);
+ *       0: query image (tiles of 128 rows).  img: device memory of
+ *       tsm_scan_image_bytes(n, is_db) bytes; img and norms 16-byte aligned.
  *   tsm_scan: either dense (thresholds NULL): dense[q * ld_dense + j] = d;
  *       or candidate lists (dense NULL): for each pair with d <= thresholds[q]
  *       a slot of counts[q] (zeroed by the caller) is taken and, below cap,
@@ -247,6 +258,7 @@ int tsm_select_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, 
  */
 int32_t tsm_scan_dim(void);
 int64_t tsm_scan_image_bytes(int64_t n_rows, int32_t is_db);
+int64_t tsm_scan_norms_count(int64_t n_rows);
 int tsm_scan_prepare(const float* emb, int64_t n, int64_t ld, float scale, int32_t is_db, void* img, float* norms,
                      void* stream);
 int tsm_scan(const void* q_img, int64_t nq, const void* db_img, const float* db_norms, int64_t nd, float scale,

@@ -44,7 +44,9 @@ def test_library_is_sm100a_only():
 
 def test_version_and_limits(lib):
     assert lib.tsm_version() >= 100
-    assert lib.tsm_max_supported_len() >= 200
+    assert lib.tsm_max_supported_len() == 32768
+    from trajsimimeasures_b200.engine import MATRIX_QUERY_MAX
+    assert lib.tsm_matrix_query_max() == MATRIX_QUERY_MAX
     assert lib.tsm_last_error() == b""
 
 
@@ -72,6 +74,8 @@ def test_invalid_arguments_fail_before_cuda(lib):
     rc = lib.tsm_allpairs_sym(7, dummy, dummy, dummy, dummy, 3, 10, ctypes.byref(p), dummy, 3, nul, nul)
     assert rc == -1 and b"unknown measure" in lib.tsm_last_error()
     assert lib.tsm_allpairs_sym(0, nul, nul, nul, nul, 0, 10, ctypes.byref(p), nul, 0, nul, nul) == 0
+    rc = lib.tsm_pairs(0, dummy, dummy, dummy, dummy, dummy, nul, 4, 40000, ctypes.byref(p), dummy, nul, nul)
+    assert rc == -3 and b"max_len 40000 > 32768" in lib.tsm_last_error()
     st = ctypes.c_int32(0)
     assert lib.tsm_enc_embed_status(nul, ctypes.byref(st), nul) == -1
     rc = lib.tsm_enc_embed_opts(dummy, dummy, dummy, dummy, 4, 8, (ctypes.c_float * 4)(0, 0, 1, 1), dummy, dummy, 0,

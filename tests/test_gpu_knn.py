@@ -155,7 +155,7 @@ def _scan_images(E, Qe, scale):
 
     def img(X, db):
         b = torch.empty(lib.tsm_scan_image_bytes(X.shape[0], int(db)), dtype=torch.uint8, device="cuda")
-        nrm = torch.empty(X.shape[0], device="cuda") if db else None
+        nrm = torch.empty(lib.tsm_scan_norms_count(X.shape[0]), device="cuda") if db else None
         assert lib.tsm_scan_prepare(_ptr(X), X.shape[0], X.stride(0), scale, int(db), _ptr(b), _ptr(nrm), None) == 0
         return b, nrm
     (dimg, norms), (qimg, _) = img(E, True), img(Qe, False)

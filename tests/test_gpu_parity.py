@@ -428,3 +428,50 @@ def test_allpairs_sym_reference_signature_full_size(full_set):
         b = core.matrix(name, P, l, P, l, eps=EPS, gpoint=G)
         assert a.dtype == np.float64 and a.shape == (2000, 2000)
         np.testing.assert_array_equal(a, b, err_msg=name)
+
+
+@pytest.mark.parametrize("m", [0, 1, 3])
+def test_long_lengths_through_matrix_allpairs_and_pairs(oracle_mod, m):
+    """Lengths 801..1,600 (the reference's timing sweep, test_trajsimi_time.py:109)
+    with some short ones: core.matrix (the rows of queries longer than the
+    matrix forms' 1,400-point limit computed by tsm_pairs), core.allpairs and
+    core.pairs, exact mode, bit-identical to the FP32 twin (float32 inputs)."""
+    from trajsimimeasures_b200 import core, datagen as D
+    O = oracle_mod
+    rng = np.random.default_rng(70 + m)
+    lens = np.concatenate([rng.integers(801, 1601, 14), rng.integers(20, 201, 6), [1400, 1401]])
+    pts, off, lens = D._walks(rng, lens, D.STEP_SIGMA)
+    t = D.unpack(pts, off, lens)
+    P = D.pad(t, dtype=np.float32)
+    kw = dict(eps=EPS, gpoint=G, exact=True)
+    got, cnt = core.matrix(m, P, lens, P, lens, counts=True, **kw)
+    want, wcnt = O.matrix_idx(O.pairs_f32, m, pts, off, lens, pts, off, lens, eps=EPS, gpoint=G)
+    if m in (1, 2):
+        np.testing.assert_array_equal(cnt, wcnt)
+    else:
+        np.testing.assert_array_equal(got.astype(np.float32), want)
+    sym = core.allpairs(m, P, lens, **kw)
+    np.testing.assert_array_equal(sym, got)
+    ia, ib = np.arange(0, 21), np.arange(1, 22)
+    pr = core.pairs(m, P[ia], lens[ia], P[ib], lens[ib], **kw)
+    np.testing.assert_array_equal(pr, got[ia, ib])
+
+
+def test_pairs_beyond_8192_points(oracle_mod):
+    """Pairs longer than 8,192 points (the wave kernel with fewer warps per
+    CTA) up to 12,000: exact mode bit-identical to the twin; above
+    tsm_max_supported_len (32,768) the call is refused with TSM_ETOOLONG."""
+    from trajsimimeasures_b200 import _lib, datagen as D
+    O = oracle_mod
+    rng = np.random.default_rng(81)
+    lens = np.array([12000, 9000, 8193, 300, 10000, 16])
+    pts, off, lens = D._walks(rng, lens, D.STEP_SIGMA)
+    ia, ib = np.array([0, 1, 2, 4]), np.array([1, 3, 4, 5])
+    for m in (0, 1):
+        got, cnt = run_pairs(m, pts, off, lens, ia, ib, exact=True)
+        want, wcnt = O.pairs_idx(O.pairs_f32, m, pts, off, lens, ia, ib, eps=EPS, gpoint=G)
+        np.testing.assert_array_equal(got, want)
+        if m == 1:
+            np.testing.assert_array_equal(cnt, wcnt)
+    with pytest.raises(_lib.TsmError, match="TSM_ETOOLONG|-3"):
+        run_pairs(0, np.zeros((33000, 2), np.float32), np.array([0]), np.array([33000]), np.array([0]), np.array([0]))

@@ -19,12 +19,12 @@ MEASURE_NAMES = {DTW: "dtw", EDR: "edr", LCSS: "lcss", ERP: "erp", DFRECHET: "df
 FLAG_EXACT = 1
 
 # Every symbol include/tsm.h declares (checked by the test suite).
-EXPORTS = ("tsm_version", "tsm_last_error", "tsm_max_supported_len", "tsm_pairs", "tsm_matrix",
+EXPORTS = ("tsm_version", "tsm_last_error", "tsm_max_supported_len", "tsm_matrix_query_max", "tsm_pairs", "tsm_matrix",
            "tsm_sched_workspace_bytes", "tsm_pairs_sched", "tsm_topk_rows", "tsm_pairs_sched_noalloc",
            "tsm_enc_param_count", "tsm_enc_workspace_bytes", "tsm_enc_forward", "tsm_enc_loss_grad", "tsm_enc_adam",
            "tsm_select_rows", "tsm_allpairs_sym", "tsm_matrix_gather", "tsm_enc_embed_workspace_bytes",
            "tsm_enc_embed", "tsm_enc_embed_status", "tsm_enc_embed_opts", "tsm_enc_loss_grad_w", "tsm_scan_dim",
-           "tsm_scan_image_bytes", "tsm_scan_prepare", "tsm_scan", "tsm_scan_opts")
+           "tsm_scan_image_bytes", "tsm_scan_norms_count", "tsm_scan_prepare", "tsm_scan", "tsm_scan_opts")
 
 
 class TsmParams(ctypes.Structure):
@@ -57,6 +57,7 @@ def load():
         lib.tsm_version.restype = ctypes.c_int
         lib.tsm_last_error.restype = ctypes.c_char_p
         lib.tsm_max_supported_len.restype = _i32
+        lib.tsm_matrix_query_max.restype = _i32
         lib.tsm_pairs.restype = ctypes.c_int
         lib.tsm_pairs.argtypes = [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i32,
                                   ctypes.POINTER(TsmParams), _vp, _vp, _vp]
@@ -102,6 +103,8 @@ def load():
         lib.tsm_scan_dim.restype = _i32
         lib.tsm_scan_image_bytes.restype = _i64
         lib.tsm_scan_image_bytes.argtypes = [_i64, _i32]
+        lib.tsm_scan_norms_count.restype = _i64
+        lib.tsm_scan_norms_count.argtypes = [_i64]
         lib.tsm_scan_prepare.restype = ctypes.c_int
         lib.tsm_scan_prepare.argtypes = [_vp, _i64, _i64, ctypes.c_float, _i32, _vp, _vp, _vp]
         lib.tsm_scan.restype = ctypes.c_int

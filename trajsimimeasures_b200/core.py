@@ -38,8 +38,8 @@ import threading
 import numpy as np
 import torch
 
-from . import _lib
-from .engine import (TrajSet, allpairs_sym_raw, first_points_lists, matrix_raw, measure_id, needs_origin,
+from . import _lib, engine
+from .engine import (MATRIX_QUERY_MAX, TrajSet, allpairs_sym_raw, first_points_lists, matrix_raw, measure_id, needs_origin,
                      origin_of_points, pack_lists, pair_order, pairs_raw, shift_gpoint, sub_origin_f32)
 
 __all__ = ["dtw", "edr", "lcss", "erp", "dfrechet", "hausdorff", "matrix", "dtw_matrix", "edr_matrix",
@@ -396,6 +396,46 @@ def _set_of(t, lens, device, origin=None):
     return TrajSet.from_padded(a, la, device=device, origin=o)
 
 
+def _matrix_into(m, qs, ds, out, cnt, *, eps, gpoint, exact, rows, stream=None):
+    """out (and cnt) [qs.n, ds.n] = measure over Q x D.  Queries up to the
+    matrix forms' limit (MATRIX_QUERY_MAX points; Hausdorff: any) in one
+    tsm_matrix launch; the rows of longer queries with tsm_pairs over
+    (query, every database trajectory) pairs, whose kernels take any length
+    up to tsm_max_supported_len.  Both give the same values bit for bit."""
+    lq = qs.lens_host if qs.lens_host is not None else qs.lens.cpu().numpy()
+    if m == _lib.HAUSDORFF or qs.max_len <= MATRIX_QUERY_MAX:
+        matrix_raw(m, qs, ds, out=out, counts=cnt, eps=eps, gpoint=gpoint, exact=exact, rows=rows, stream=stream)
+        return
+    dev = qs.device
+    long_i = np.nonzero(np.asarray(lq) > MATRIX_QUERY_MAX)[0]
+    short_i = np.nonzero(np.asarray(lq) <= MATRIX_QUERY_MAX)[0]
+    if short_i.size:
+        si = torch.as_tensor(short_i, device=dev)
+        sub = TrajSet(qs.pts, qs.off[si], qs.lens[si], int(np.asarray(lq)[short_i].max()),
+                      np.asarray(lq)[short_i].astype(np.int32), origin=qs.origin)
+        o = torch.empty((sub.n, ds.n), dtype=torch.float32, device=dev)
+        c = torch.empty((sub.n, ds.n), dtype=torch.int32, device=dev) if cnt is not None else None
+        matrix_raw(m, sub, ds, out=o, counts=c, eps=eps, gpoint=gpoint, exact=exact, rows=rows, stream=stream)
+        out[si] = o
+        if cnt is not None:
+            cnt[si] = c
+    origin = engine.same_origin(qs, ds)
+    shift = ds.pts.shape[0]
+    pool = torch.cat([ds.pts, qs.pts])  # one point pool for the paired kernels
+    nd = ds.n
+    for i in long_i:
+        ia = torch.full((nd,), int(i), dtype=torch.int64, device=dev)
+        off_a, len_a = qs.off[ia] + shift, qs.lens[ia]
+        o = torch.empty(nd, dtype=torch.float32, device=dev)
+        c = torch.empty(nd, dtype=torch.int32, device=dev) if cnt is not None else None
+        pairs_raw(m, pool, off_a, len_a, ds.off, ds.lens, max(qs.max_len, ds.max_len), out=o, counts=c,
+                  order=engine.pair_order_dev(len_a, ds.lens), eps=eps, gpoint=shift_gpoint(gpoint, origin),
+                  exact=exact, rows=rows, stream=stream)
+        out[int(i)] = o
+        if cnt is not None:
+            cnt[int(i)] = c
+
+
 def matrix(measure, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False, rows=0, counts=False):
     """result[i, j] = measure(Q_i, D_j) for all pairs, one launch.
 
@@ -410,7 +450,7 @@ def matrix(measure, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False, rows
     ds = _set_of(D, lenD, qs.device, origin)
     out = torch.empty((qs.n, ds.n), dtype=torch.float32, device=qs.device)
     cnt = torch.empty((qs.n, ds.n), dtype=torch.int32, device=qs.device) if m in (_lib.EDR, _lib.LCSS) else None
-    matrix_raw(m, qs, ds, out=out, counts=cnt, eps=eps, gpoint=_gpoint(gpoint), exact=exact, rows=rows)
+    _matrix_into(m, qs, ds, out, cnt, eps=eps, gpoint=_gpoint(gpoint), exact=exact, rows=rows)
     return _finish_matrix(m, out, cnt, qs, ds, on_device, counts)
 
 
@@ -447,7 +487,10 @@ def allpairs(measure, S, lenS=None, *, eps=0.0, gpoint=None, exact=False, rows=0
     ss = _set_of(S, lenS, dev, set_origin((S, lenS)))
     out = torch.empty((ss.n, ss.n), dtype=torch.float32, device=ss.device)
     cnt = torch.empty((ss.n, ss.n), dtype=torch.int32, device=ss.device) if m in (_lib.EDR, _lib.LCSS) else None
-    allpairs_sym_raw(m, ss, out=out, counts=cnt, eps=eps, gpoint=_gpoint(gpoint), exact=exact, rows=rows)
+    if m != _lib.HAUSDORFF and ss.max_len > MATRIX_QUERY_MAX:  # the full matrix, long rows by tsm_pairs
+        _matrix_into(m, ss, ss, out, cnt, eps=eps, gpoint=_gpoint(gpoint), exact=exact, rows=rows)
+    else:
+        allpairs_sym_raw(m, ss, out=out, counts=cnt, eps=eps, gpoint=_gpoint(gpoint), exact=exact, rows=rows)
     return _finish_matrix(m, out, cnt, ss, ss, on_device, counts)
 
 
@@ -475,7 +518,7 @@ def matrix_many(measures, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=False
         m = measure_id(meas)
         out = torch.empty((qs.n, ds.n), dtype=torch.float32, device=dev)
         cnt = torch.empty((qs.n, ds.n), dtype=torch.int32, device=dev) if m in (_lib.EDR, _lib.LCSS) else None
-        matrix_raw(m, qs, ds, out=out, counts=cnt, eps=eps, gpoint=g, exact=exact, rows=rows, stream=s)
+        _matrix_into(m, qs, ds, out, cnt, eps=eps, gpoint=g, exact=exact, rows=rows, stream=s)
         with torch.cuda.stream(s):
             if m == _lib.EDR:
                 res = cnt.double() / torch.maximum(lq, ld)
@@ -548,7 +591,7 @@ def matrix_sharded(measures, Q, lenQ, D, lenD, *, eps=0.0, gpoint=None, exact=Fa
             out = torch.empty((qs.n, ds.n), dtype=torch.float32, device=dev)
             cnt = torch.empty((qs.n, ds.n), dtype=torch.int32, device=dev) if m in (_lib.EDR, _lib.LCSS) else None
             if qs.n:
-                matrix_raw(m, qs, ds, out=out, counts=cnt, eps=eps, gpoint=g, exact=exact, rows=rows)
+                _matrix_into(m, qs, ds, out, cnt, eps=eps, gpoint=g, exact=exact, rows=rows)
             blocks[m] = (out, cnt)
         ld_all = ds.lens_host if ds.lens_host is not None else ds.lens.cpu().numpy()
     else:

@@ -43,9 +43,10 @@ static_assert(tsm::kHeavyRows >= kTileCap, "a tile-heavy pair must have a side l
 // Matrix mode keeps the query as the tile kernel's columns: its boundary
 // rows (32 per warp) and staged columns must fit one CTA's shared memory.
 constexpr int kMatrixQueryMax = 1400;
-// Longest trajectory accepted (wave kernel: 20 bytes of shared memory per
-// column point and warp).
-constexpr int kMaxLen = 8192;
+// Longest trajectory accepted by the paired kernels: the wave kernel keeps 4
+// bytes of shared memory per point of a pair's shorter side for each of its W
+// warps (W = 4 up to 8192 points, 2 up to 16384, 1 up to 32768: 128 KB).
+constexpr int kMaxLen = 32768;
 // A paired batch of at most kSmallBatchPerSm pairs per SM is too small to
 // fill the GPU one thread per pair (the tile and Hausdorff pairs kernels
 // would then run one pair's whole DP serially on a few warps per SM): every
@@ -195,6 +196,8 @@ const char* tsm_last_error(void) { return g_err.c_str(); }
 
 int32_t tsm_max_supported_len(void) { return kMaxLen; }
 
+int32_t tsm_matrix_query_max(void) { return kMatrixQueryMax; }
+
 int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t* len_a,
               const int64_t* off_b, const int32_t* len_b, const int32_t* order, int64_t n_pairs,
               int32_t max_len, const tsm_params* params, float* out, int32_t* out_counts, void* stream) {
@@ -204,6 +207,8 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
     if (n_pairs == 0) return TSM_OK;
     if (!pts || !off_a || !len_a || !off_b || !len_b || !out) return fail(TSM_EINVAL, "tsm_pairs: null pointer");
     if (max_len < 0) return fail(TSM_EINVAL, "tsm_pairs: max_len < 0");
+    if (measure != TSM_HAUSDORFF && max_len > kMaxLen)
+        return fail(TSM_ETOOLONG, "tsm_pairs: max_len %d > %d (tsm_max_supported_len)", max_len, kMaxLen);
     const bool exact = exact_of(params);
     cudaStream_t s = (cudaStream_t)stream;
     const tsm::KParams kp = make_kparams(params);
@@ -239,7 +244,6 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
         return launch_with_side([&](cudaStream_t st) { return launch(fn, grid, dim3(threads), 0, args, st); }, wfn,
                                 w_grid, dim3(threads), 0, w_args, s, dev);
     }
-    if (max_len > kMaxLen) return fail(TSM_ETOOLONG, "tsm_pairs: max_len %d > %d", max_len, kMaxLen);
     const void* fn = tsm_k::dp_pairs(measure, R, exact);
     if (!fn) return fail(TSM_EINVAL, "tsm_pairs: rows_per_thread must be 4, 8 or 16");
     // small batch: tile capacity 0, so the tile kernel keeps only empty and
@@ -256,7 +260,7 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
     // long: the persistent wave kernel, one warp per pair
     const void* wfn = tsm_k::dp_wave(measure, R, exact);
     int wcap = (max_len + 3) & ~3;
-    const int W = 4;
+    const int W = wcap <= 8192 ? 4 : (wcap <= 16384 ? 2 : 1);
     const int w_smem = W * tsm::wave_warp_floats(wcap) * 4;
     if (w_smem > kSmemMax) return fail(TSM_ETOOLONG, "tsm_pairs: wave kernel needs %d bytes", w_smem);
     dim3 w_grid;

@@ -65,10 +65,12 @@ constexpr int B_TILE_BYTES = DN * K * 2;   // 245,760
 constexpr int B_STAGE_BYTES = DN * SK * 2; // 24,576
 constexpr int THREADS = 192;               // warp 0 copies, warp 1 MMAs, warps 2-5 epilogue
 constexpr uint32_t TMEM_COLS = 2 * DN;     // two accumulators
+constexpr int NNORM = 4;                   // squared-norm ring: one database tile's norms per slot
 constexpr int OFF_A = 0;
 constexpr int OFF_B = A_BYTES;
-constexpr int OFF_BAR = OFF_B + NSTAGE * B_STAGE_BYTES;
-constexpr int SMEM = OFF_BAR + 128;        // 221,312 bytes
+constexpr int OFF_N = OFF_B + NSTAGE * B_STAGE_BYTES;
+constexpr int OFF_BAR = OFF_N + NNORM * DN * 4;
+constexpr int SMEM = OFF_BAR + 256;        // 225,536 bytes
 constexpr long long WAIT_CYCLES = 2000000000LL;
 static_assert(K % SK == 0 && SK % 16 == 0 && D % 8 == 0, "stage and chunk sizes");
 static_assert(SMEM <= 227 * 1024, "shared memory");
@@ -81,9 +83,11 @@ constexpr int ERR_EPI = 8;    // the epilogue gave up waiting for an accumulator
 
 // Operand image of rows [0, n) of emb (row stride ld floats, D values each,
 // times s), padded with zero rows to whole tiles of R rows.  DB: rows
-// [hi | hi | lo] (and FP32 squared norms |emb_j|^2 of the unscaled rows);
-// queries: [hi | lo | hi].  One thread per (row, 16-byte chunk), consecutive
-// threads on consecutive rows of one chunk (coalesced 16-byte stores).
+// [hi | hi | lo] and FP32 squared norms |emb_j|^2 of the unscaled rows, +inf
+// for the padding rows of the last tile (their d is then +inf, below no
+// threshold); queries: [hi | lo | hi].  One thread per (row, 16-byte chunk),
+// consecutive threads on consecutive rows of one chunk (coalesced 16-byte
+// stores).
 template <bool DB>
 __global__ void scan_prepare(const float* __restrict__ emb, int64_t n, int64_t ld, float s, int64_t n_tiles,
                              __half* __restrict__ img, float* __restrict__ norms) {
@@ -107,16 +111,20 @@ __global__ void scan_prepare(const float* __restrict__ emb, int64_t n, int64_t l
     unsigned char* dst = reinterpret_cast<unsigned char*>(img) + t * ((int64_t)R * K * 2) +
                          (int64_t)c * (R * 16) + (r >> 3) * 128 + (r & 7) * 16;
     *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(v);
-    if (DB && norms && c == 0 && row < n) {
-        float ss = 0.f;
-        for (int k = 0; k < D; ++k) {
-            const float x = emb[row * ld + k];
-            ss = fmaf(x, x, ss);
+    if (DB && norms && c == 0) {
+        float ss = __int_as_float(0x7f800000);  // +inf
+        if (row < n) {
+            ss = 0.f;
+            for (int k = 0; k < D; ++k) {
+                const float x = emb[row * ld + k];
+                ss = fmaf(x, x, ss);
+            }
         }
         norms[row] = ss;
     }
 }
 
+template <bool DENSE>
 __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
     const __half* __restrict__ qimg, int64_t nq, const __half* __restrict__ dimg, const float* __restrict__ norms,
     int64_t nd, float inv_s2, const float* __restrict__ thr, int cap, int32_t* __restrict__ cand_idx,
@@ -127,14 +135,17 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
     const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
     const uint32_t bar = sbase + OFF_BAR;
     // mbarriers: full[4] (copies landed), empty[4] (stage read by the MMAs),
-    // tfull[2] (accumulator ready), tempty[2] (accumulator read), A landed, all MMAs done
+    // tfull[2] (accumulator ready), tempty[2] (accumulator read), A landed, all
+    // MMAs done, nfull[4] (a tile's norms landed), nempty[4] (norms read)
     auto full = [&](int i) { return bar + 8 * i; };
     auto empty = [&](int i) { return bar + 32 + 8 * i; };
     auto tfull = [&](int b) { return bar + 64 + 8 * b; };
     auto tempty = [&](int b) { return bar + 80 + 8 * b; };
     const uint32_t abar = bar + 96, donebar = bar + 104;
-    volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(sm + OFF_BAR + 112);
-    volatile int* tmem_busy = reinterpret_cast<volatile int*>(sm + OFF_BAR + 116);
+    auto nfull = [&](int i) { return bar + 112 + 8 * i; };
+    auto nempty = [&](int i) { return bar + 144 + 8 * i; };
+    volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(sm + OFF_BAR + 176);
+    volatile int* tmem_busy = reinterpret_cast<volatile int*>(sm + OFF_BAR + 180);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int qt = blockIdx.x % nqt;
     const int64_t sl = blockIdx.x / nqt;
@@ -154,10 +165,14 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
         }
         U::mbar_init(abar, 1);
         U::mbar_init(donebar, 1);
+        for (int i = 0; i < NNORM; ++i) {
+            U::mbar_init(nfull(i), 1);
+            U::mbar_init(nempty(i), 4);  // one arrival per epilogue warp
+        }
         *tmem_busy = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) U::tmem_alloc(sbase + OFF_BAR + 112, TMEM_COLS);
+    if (warp == 0) U::tmem_alloc(sbase + OFF_BAR + 176, TMEM_COLS);
     U::fence_before_sync();
     __syncthreads();
     U::fence_after_sync();
@@ -170,9 +185,21 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
             for (int c = 0; c < 4; ++c)
                 U::bulk_load(sbase + OFF_A + c * (A_BYTES / 4), asrc + c * (A_BYTES / 4), A_BYTES / 4, abar);
             int64_t g = 0;  // stages issued
+            int64_t nt = 0;  // tiles whose norms were issued
             bool ok = true;
             for (int64_t t = t0; t < t1 && ok; ++t) {
                 const unsigned char* bsrc = reinterpret_cast<const unsigned char*>(dimg) + t * B_TILE_BYTES;
+                {  // the tile's squared norms into the norm ring
+                    const int slot = (int)(nt % NNORM);
+                    const uint32_t u = (uint32_t)(nt / NNORM);
+                    if (!U::mbar_wait(nempty(slot), (u & 1) ^ 1, wait_cycles)) {
+                        atomicOr(status, ERR_COPY);
+                        break;
+                    }
+                    U::mbar_arrive_expect_tx(nfull(slot), DN * 4);
+                    U::bulk_load(sbase + OFF_N + slot * (DN * 4), norms + t * DN, DN * 4, nfull(slot));
+                    ++nt;
+                }
                 for (int k = 0; k < STAGES_PER_TILE; ++k) {
                     const int slot = (int)(g % NSTAGE);
                     const uint32_t u = (uint32_t)(g / NSTAGE);
@@ -190,6 +217,8 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
             // every copy this CTA issued lands before it exits: the last use of each slot, and A
             for (int slot = 0; slot < NSTAGE; ++slot)
                 if (slot < g) U::mbar_wait(full(slot), (uint32_t)((g - 1 - slot) / NSTAGE) & 1, wait_cycles);
+            for (int slot = 0; slot < NNORM; ++slot)
+                if (slot < nt) U::mbar_wait(nfull(slot), (uint32_t)((nt - 1 - slot) / NNORM) & 1, wait_cycles);
             U::mbar_wait(abar, 0, wait_cycles);
         }
     } else if (warp == 1) {
@@ -242,35 +271,58 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
         const int quarter = warp & 3;
         const int64_t q = (int64_t)qt * QM + 32 * quarter + lane;
         const bool qv = q < nq;
-        const float th = (thr && qv) ? thr[q] : 0.f;
+        // padding queries get -inf: no d (>= finite or +inf) is at or below it
+        const float th = DENSE ? 0.f : (qv ? thr[q] : __int_as_float(0xff800000));
         const float m2 = -2.f * inv_s2;
         for (int64_t t = 0; t < ntl; ++t) {
             const int b = (int)(t & 1);
             const uint32_t v = (uint32_t)(t >> 1);
-            if (!U::mbar_wait(tfull(b), v & 1, wait_cycles)) {
+            const int ns = (int)(t % NNORM);
+            if (!U::mbar_wait(tfull(b), v & 1, wait_cycles) ||
+                !U::mbar_wait(nfull(ns), (uint32_t)(t / NNORM) & 1, wait_cycles)) {
                 atomicOr(status, ERR_EPI);
                 break;
             }
             U::fence_after_sync();
             const int64_t j0 = (t0 + t) * DN;
             const uint32_t ta = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(b * DN);
+            const float4* nr = reinterpret_cast<const float4*>(sm + OFF_N + ns * (DN * 4));
 #pragma unroll 1
             for (int cg = 0; cg < DN / 16; ++cg) {
                 uint32_t r[16];
                 U::ld16(ta + cg * 16, r);
                 U::wait_ld(r);
+                float d[16];
+                float mn = __int_as_float(0x7f800000);
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const int64_t j = j0 + cg * 16 + i;
-                    if (qv && j < nd) {
-                        const float dd = fmaf(m2, __uint_as_float(r[i]), __ldg(norms + j));
-                        if (dense) {
-                            dense[q * ld + j] = dd;
-                        } else if (dd <= th) {
-                            const int pos = atomicAdd(counts + q, 1);
-                            if (pos < cap) {
-                                cand_idx[q * cap + pos] = (int32_t)j;
-                                cand_d[q * cap + pos] = dd;
+                for (int i4 = 0; i4 < 4; ++i4) {
+                    const float4 nv = nr[cg * 4 + i4];  // same address in every lane: a broadcast
+                    d[4 * i4 + 0] = fmaf(m2, __uint_as_float(r[4 * i4 + 0]), nv.x);
+                    d[4 * i4 + 1] = fmaf(m2, __uint_as_float(r[4 * i4 + 1]), nv.y);
+                    d[4 * i4 + 2] = fmaf(m2, __uint_as_float(r[4 * i4 + 2]), nv.z);
+                    d[4 * i4 + 3] = fmaf(m2, __uint_as_float(r[4 * i4 + 3]), nv.w);
+                }
+                if (DENSE) {
+                    if (qv) {
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) {
+                            const int64_t j = j0 + cg * 16 + i;
+                            if (j < nd) dense[q * ld + j] = d[i];
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) mn = fminf(mn, d[i]);
+                    if (mn <= th) {  // rare: at least one of the 16 survives
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) {
+                            const int64_t j = j0 + cg * 16 + i;
+                            if (d[i] <= th && j < nd) {
+                                const int pos = atomicAdd(counts + q, 1);
+                                if (pos < cap) {
+                                    cand_idx[q * cap + pos] = (int32_t)j;
+                                    cand_d[q * cap + pos] = d[i];
+                                }
                             }
                         }
                     }
@@ -278,7 +330,10 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
             }
             U::fence_before_sync();
             __syncwarp();
-            if (lane == 0) U::mbar_arrive(tempty(b));
+            if (lane == 0) {
+                U::mbar_arrive(tempty(b));
+                U::mbar_arrive(nempty(ns));
+            }
         }
     }
     U::fence_before_sync();
@@ -309,6 +364,11 @@ extern "C" {
 
 int32_t tsm_scan_dim(void) { return tsm::scan::D; }
 
+int64_t tsm_scan_norms_count(int64_t n_rows) {
+    if (n_rows < 0) return -1;
+    return (n_rows + tsm::scan::DN - 1) / tsm::scan::DN * tsm::scan::DN;
+}
+
 int64_t tsm_scan_image_bytes(int64_t n_rows, int32_t is_db) {
     if (n_rows < 0) return -1;
     const int64_t R = is_db ? tsm::scan::DN : tsm::scan::QM;
@@ -327,6 +387,8 @@ int tsm_scan_prepare(const float* emb, int64_t n, int64_t ld, float scale, int32
     const int64_t threads = tiles * KCH * R;
     const unsigned grid = (unsigned)((threads + 255) / 256);
     cudaStream_t s = (cudaStream_t)stream;
+    if (is_db && reinterpret_cast<uintptr_t>(norms) % 16)
+        return scan_fail(TSM_EINVAL, "tsm_scan_prepare: norms not 16-byte aligned");
     if (is_db)
         scan_prepare<true><<<grid, 256, 0, s>>>(emb, n, ld, scale, tiles, static_cast<__half*>(img), norms);
     else
@@ -349,8 +411,9 @@ int tsm_scan_opts(const void* q_img, int64_t nq, const void* db_img, const float
     if (dense_mode && ld_dense < nd) return scan_fail(TSM_EINVAL, "tsm_scan: ld_dense < nd");
     if (!dense_mode && (cap < 1 || !cand_idx || !cand_d || !counts))
         return scan_fail(TSM_EINVAL, "tsm_scan: candidate lists need cap >= 1 and their three arrays");
-    if ((reinterpret_cast<uintptr_t>(q_img) | reinterpret_cast<uintptr_t>(db_img)) % 16)
-        return scan_fail(TSM_EINVAL, "tsm_scan: images not 16-byte aligned");
+    if ((reinterpret_cast<uintptr_t>(q_img) | reinterpret_cast<uintptr_t>(db_img) |
+         reinterpret_cast<uintptr_t>(db_norms)) % 16)
+        return scan_fail(TSM_EINVAL, "tsm_scan: images or norms not 16-byte aligned");
     const float inv_s2 = 1.f / (scale * scale);
     int dev = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -366,13 +429,17 @@ int tsm_scan_opts(const void* q_img, int64_t nq, const void* db_img, const float
     const int64_t per = (ntiles + slices - 1) / slices;
     slices = (ntiles + per - 1) / per;
     if (nqt * slices > 0x7fffffffLL) return scan_fail(TSM_EINVAL, "tsm_scan: grid too large");
-    if ((e = cudaFuncSetAttribute(scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM)) != cudaSuccess)
+    const void* fn = dense_mode ? (const void*)&scan_kernel<true> : (const void*)&scan_kernel<false>;
+    if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM)) != cudaSuccess)
         return scan_cuda(e, "cudaFuncSetAttribute(scan_kernel)");
     int inqt = (int)nqt;
-    scan_kernel<<<(unsigned)(nqt * slices), THREADS, SMEM, (cudaStream_t)stream>>>(
-        static_cast<const __half*>(q_img), nq, static_cast<const __half*>(db_img), db_norms, nd, inv_s2, thresholds,
-        cap, cand_idx, cand_d, counts, dense, ld_dense, inqt, per, status, (long long)wait_cycles);
-    return scan_cuda(cudaGetLastError(), "tsm_scan launch");
+    const __half* qi = static_cast<const __half*>(q_img);
+    const __half* di = static_cast<const __half*>(db_img);
+    long long wc = (long long)wait_cycles;
+    void* args[] = {&qi, &nq, &di, &db_norms, &nd, (void*)&inv_s2, &thresholds, &cap, &cand_idx, &cand_d, &counts,
+                    &dense, &ld_dense, &inqt, (void*)&per, &status, &wc};
+    e = cudaLaunchKernel(fn, dim3((unsigned)(nqt * slices)), dim3(THREADS), args, (size_t)SMEM, (cudaStream_t)stream);
+    return scan_cuda(e, "tsm_scan launch");
 }
 
 int tsm_scan(const void* q_img, int64_t nq, const void* db_img, const float* db_norms, int64_t nd, float scale,

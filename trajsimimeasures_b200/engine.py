@@ -302,7 +302,15 @@ def matrix_raw(measure, q: TrajSet, d: TrajSet, *, out, counts=None, d_order=Non
     return out
 
 
-MATRIX_QUERY_MAX = 1400  # longest query of the matrix forms (kMatrixQueryMax in the library)
+MATRIX_QUERY_MAX = 1400  # longest query of the matrix forms (tsm_matrix_query_max() of the library)
+
+
+def pair_order_dev(len_a: torch.Tensor, len_b: torch.Tensor, rows=DEFAULT_ROWS) -> torch.Tensor:
+    """pair_order on the device (int32 processing order for tsm_pairs)."""
+    la, lb = len_a.long(), len_b.long()
+    nr, nc = torch.maximum(la, lb), torch.minimum(la, lb)
+    key = ((nr + rows - 1) // rows) * 65536 + nc
+    return torch.argsort(-key, stable=True).to(torch.int32)
 
 
 def matrix_gather_raw(measure, q: TrajSet, d: TrajSet, cand: torch.Tensor, *, out, counts=None, eps=0.0,

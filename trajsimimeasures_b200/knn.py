@@ -25,7 +25,7 @@ import torch
 
 from . import _lib
 from .engine import (DEFAULT_ROWS, MATRIX_QUERY_MAX, TrajSet, _ptr, _stream_ptr, matrix_gather_raw, matrix_raw,
-                     measure_id, pairs_raw, same_origin, shift_gpoint)
+                     measure_id, pair_order_dev, pairs_raw, same_origin, shift_gpoint)
 
 
 def topk_rows(d: torch.Tensor, k: int, stream=None):
@@ -117,10 +117,7 @@ def shape_order(len_a: torch.Tensor, len_b: torch.Tensor, rows=DEFAULT_ROWS) -> 
     """engine.pair_order on the device: the pairs ordered by (row blocks,
     columns) of their DP, the largest first, so a warp's 32 lanes run loops of
     equal trip counts (int32 processing order for tsm_pairs)."""
-    la, lb = len_a.long(), len_b.long()
-    nr, nc = torch.maximum(la, lb), torch.minimum(la, lb)
-    key = ((nr + rows - 1) // rows) * 65536 + nc
-    return torch.argsort(-key, stable=True).to(torch.int32)
+    return pair_order_dev(len_a, len_b, rows)
 
 
 def recall_at_k(approx_idx, exact_idx) -> float:
@@ -205,7 +202,8 @@ class SurrogateIndex:
         lib = _lib.load()
         n = X.shape[0]
         img = torch.empty(max(lib.tsm_scan_image_bytes(n, int(is_db)), 16), dtype=torch.uint8, device=X.device)
-        norms = torch.empty(n, dtype=torch.float32, device=X.device) if is_db else None
+        norms = torch.empty(max(lib.tsm_scan_norms_count(n), 1), dtype=torch.float32, device=X.device) if is_db \
+            else None
         rc = lib.tsm_scan_prepare(_ptr(X), n, X.stride(0), self.scale, int(is_db), _ptr(img), _ptr(norms),
                                   _stream_ptr(None))
         _lib.check(rc, "tsm_scan_prepare")
@@ -260,7 +258,7 @@ class SurrogateIndex:
                 out[q0:q0 + b] = select_rows(self._dense(qimg, b, self.img, self.norms, n), c).long()
                 continue
             ds = self._dense(qimg, b, self.s_img, self.s_norms, S)
-            thr = torch.kthvalue(ds, ks, dim=1).values.contiguous()
+            thr = torch.topk(ds, ks, dim=1, largest=False, sorted=True).values[:, -1].contiguous()
             idx = torch.empty((b, cap), dtype=torch.int32, device=Q.device)
             dd = torch.full((b, cap), float("inf"), dtype=torch.float32, device=Q.device)
             cnt = torch.zeros(b, dtype=torch.int32, device=Q.device)
