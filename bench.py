@@ -25,6 +25,10 @@ cfg1     = the 1,000-pair paired call, core.<measure>(t1, len1, t2, len2), per
 cfg3     = the 500k-pair uneven batch (lognormal lengths), DTW + Frechet + EDR
            in one autotuned persistent launch replayed as a CUDA graph, next to
            three plain tsm_pairs launches.
+cfg5     = kNN, 1,000 queries x 1M trajectories, DTW top-10: exhaustive exact
+           GPU DP against the learned filter (an encoder trained here on a
+           reduced budget, stated in the line) + tensor-core candidate scan +
+           exact rerank; queries/s and recall@10.
 roofline = the dominant kernel's FP32-issue rate (algorithmic ops per unit x
            units / its event time) against SMs x 128 lanes x max SM clock.
 cpu_baseline = the reference's C++ measures (oracle/_ref: DTW, ERP, Frechet,
@@ -61,7 +65,9 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--impl", choices=["ours", "reference", "numba"], default="ours",
+                    help="reference: the reference's CPU measures (the reference arm); numba: the reference's "
+                         "Numba-CUDA measures (baseline/_ref/core) on this GPU, 1,000 paired trajectories")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU work of the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -468,6 +474,15 @@ def run_ours(args, ws, rank, local):
     if ws == 1 and not args.no_extra:
         line["cfg1"] = cfg1_pairs(args)
         line["cfg3"] = uneven_result(args.n_pairs, 10, 3)
+        t0 = time.perf_counter()
+        enc = train_quick(100_000, 4, D.SEED_DB)
+        train_s = time.perf_counter() - t0
+        k = run_knn(args, enc=enc, emit=False)
+        k["encoder_training"] = {"pool": 100_000, "pairs": "100k random + 5k anchors x 10 neighbours",
+                                 "epochs": 4, "seconds": train_s,
+                                 "note": "reduced from the full surrogate configuration (200k pairs, 20 epochs) "
+                                         "to keep the default bench within minutes"}
+        line["cfg5"] = k
     print(json.dumps(line), flush=True)
 
 
@@ -730,14 +745,34 @@ def run_surrogate(args):
         "label_max_rel_err_vs_fp64": label_err, "checkpoint": args.checkpoint or None}), flush=True)
 
 
-def run_knn(args):
+def train_quick(pool_n, epochs, seed):
+    """A filter encoder trained on a reduced budget for the default bench line:
+    pool of pool_n walks, pool_n random pairs plus pool_n / 20 anchors x 10
+    neighbour pairs, MSE on normalised DTW, `epochs` epochs."""
+    import torch
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.engine import TrajSet
+    from trajsimimeasures_b200.surrogate import Encoder, dtw_labels, neighbour_pairs
+    dev = torch.device("cuda", torch.cuda.current_device())
+    s = TrajSet.from_packed(*D.trajectory_set(pool_n, seed=seed), device=dev)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pa, pb = rng.integers(0, pool_n, pool_n), rng.integers(0, pool_n, pool_n)
+    na, nb = neighbour_pairs(s, pool_n // 20, k=10, seed=seed)
+    pa, pb = np.concatenate([pa, na]), np.concatenate([pb, nb])
+    lab = dtw_labels(s, pa, pb)
+    enc = Encoder.init(s, seed=0)
+    enc.fit(s, pa, pb, lab / lab.max(), epochs=epochs, batch_pairs=1024, lr=2e-3)
+    return enc
+
+
+def run_knn(args, enc=None, emit=True):
     """1k queries against a 1M database (random walks, U{20..200}): exhaustive
     exact GPU DTW top-10 vs the calibrated learned filter + exact rerank."""
     import torch
     from trajsimimeasures_b200 import datagen as D
     from trajsimimeasures_b200.engine import TrajSet
     from trajsimimeasures_b200.knn import SurrogateIndex, knn_exhaustive, recall_at_k
-    dev = torch.device("cuda", 0)
+    dev = torch.device("cuda", torch.cuda.current_device())
     t0 = time.perf_counter()
     dp, do, dl = D.trajectory_set(args.n_db, seed=D.SEED_DB)
     qp, qo, ql = D.trajectory_set(args.n_queries, seed=D.SEED_QUERY)
@@ -755,8 +790,10 @@ def run_knn(args):
     out = {"workload": f"knn_{args.n_queries}q_x_{args.n_db}db_dtw_top10",
            "exhaustive_queries_per_s": args.n_queries / ex_s, "exhaustive_s": ex_s,
            "exhaustive_cells_per_s": float(ql.astype(np.float64).sum() * dl.astype(np.float64).sum()) / ex_s}
-    if args.checkpoint and os.path.exists(args.checkpoint):
-        enc, ck = _load_encoder(args.checkpoint, dev)
+    if enc is not None or (args.checkpoint and os.path.exists(args.checkpoint)):
+        ck = {"rho": None}
+        if enc is None:
+            enc, ck = _load_encoder(args.checkpoint, dev)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         index = SurrogateIndex(enc, Dset)
@@ -810,7 +847,9 @@ def run_knn(args):
         out["hit_ratio"] = hit_ratios(Q, Dset, enc, ex50)
         out["hit_ratio_untrained"] = hit_ratios(Q, Dset, raw.enc, ex50)
     out["host_generate_s"] = gen_s
-    print(json.dumps(out), flush=True)
+    if emit:
+        print(json.dumps(out), flush=True)
+    return out
 
 
 def run_sym(args):
@@ -852,9 +891,87 @@ def run_sym(args):
                       "total_sym_ms": sum(v["sym_ms"] for v in res.values())}), flush=True)
 
 
+def run_numba_arm(args, ws, rank):
+    """The reference's own GPU path on this GPU: core.dtw / erp / dfrechet /
+    hausdorff / edr / lcss of the reference (Numba-CUDA, FP64, one 64-thread
+    block per pair; core/dtw.py:56-77 etc.), installed unmodified in
+    baseline/_ref by baseline/install_reference.py, called as the reference's
+    paired driver calls them (test_trajsimi_time.py:222-276): 1,000 pairs,
+    batches of 512 (config.py:45), padded float64 host arrays in, float64 out.
+    ERP gets one trailing dummy pair whose second trajectory is as long as the
+    padding, which keeps the reference kernel's gap-distance buffer (sized by
+    the longest second trajectory, core/erp.py:106,112) in bounds.  Hausdorff
+    is timed only: its host maximum reads uninitialised padded slots
+    (core/hausdorff.py:114,121)."""
+    if rank != 0:
+        return
+    ref = os.path.join(ROOT, "baseline", "_ref")
+    line = {"impl": "numba", "metric": "pairs/s per measure (1,000 pairs, U{20..200}, reference Numba-CUDA)"}
+    if not os.path.isdir(os.path.join(ref, "core")):
+        line["unavailable"] = "baseline/_ref/core missing: run baseline/install_reference.py where the reference exists"
+        print(json.dumps(line), flush=True)
+        return
+    try:
+        sys.path.insert(0, ref)
+        import core as rcore  # the reference's package
+        from numba import cuda
+        if not cuda.is_available():
+            raise RuntimeError("numba.cuda reports no usable GPU")
+        cc = cuda.get_current_device().compute_capability
+    except Exception as e:  # noqa: BLE001 - reported, not hidden
+        line["unavailable"] = f"{type(e).__name__}: {e}"[:300]
+        print(json.dumps(line), flush=True)
+        return
+    from trajsimimeasures_b200 import datagen as D
+    pts, off, lens, ia, ib = D.pairs_uniform(1000)
+    la, lb = lens[ia].astype(np.int64), lens[ib].astype(np.int64)
+    t1, t2 = D.pad(D.unpack(pts, off, lens, ia)), D.pad(D.unpack(pts, off, lens, ib))
+    w = t1.shape[1]
+    B = 512
+
+    def batches(fn):
+        for b0 in range(0, 1000, B):
+            fn(slice(b0, min(b0 + B, 1000)))
+
+    def erp_call(s):
+        a = np.concatenate([t1[s], np.zeros((1, w, 2))])
+        b = np.concatenate([t2[s], np.zeros((1, w, 2))])
+        return rcore.erp(a, np.append(la[s], 1), b, np.append(lb[s], w), list(D.BOX_CENTRE), threads_per_traj=64)
+    calls = {"dtw": lambda s: rcore.dtw(t1[s], la[s], t2[s], lb[s], threads_per_traj=64),
+             "edr": lambda s: rcore.edr(t1[s], la[s], t2[s], lb[s], EPS, threads_per_traj=64),
+             "lcss": lambda s: rcore.lcss(t1[s], la[s], t2[s], lb[s], EPS, threads_per_traj=64),
+             "erp": erp_call,
+             "dfrechet": lambda s: rcore.dfrechet(t1[s], la[s], t2[s], lb[s], threads_per_traj=64),
+             "hausdorff": lambda s: rcore.hausdorff(t1[s], la[s], t2[s], lb[s], threads_per_traj=64)}
+    per = {}
+    try:
+        for name, fn in calls.items():
+            for _ in range(max(1, args.warmup)):
+                batches(fn)  # the first call JIT-compiles the kernel
+            cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                batches(fn)
+            cuda.synchronize()
+            dt = (time.perf_counter() - t0) / args.steps
+            per[name] = {"pairs_per_s": 1000 / dt, "ms_per_1000_pairs": 1e3 * dt}
+    except Exception as e:  # noqa: BLE001
+        line["unavailable"] = f"{type(e).__name__}: {e}"[:300]
+        line["per_measure"] = per
+        print(json.dumps(line), flush=True)
+        return
+    line.update({"compute_capability": list(cc), "steps": args.steps, "warmup": args.warmup,
+                 "batch": B, "threads_per_traj": 64, "per_measure": per,
+                 "config": {"workload": "pairs_1000_uniform_20_200", "eps_deg": EPS, "erp_gpoint": list(D.BOX_CENTRE)}})
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
+    if args.impl == "numba":
+        run_numba_arm(args, ws, rank)
+        return
     if args.workload != "allpairs":
         {"uneven": run_uneven, "surrogate": run_surrogate, "knn": run_knn, "sym": run_sym}[args.workload](args)
         return

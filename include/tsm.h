@@ -148,6 +148,20 @@ int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int3
                float* out, int64_t ld_out, int32_t* out_counts, void* stream);
 
 /*
+ * Selected rows of the Q x D matrix: for r < n_rows, with i = q_rows[r],
+ *   out[i*ld_out + j] = measure(Q_i, D_j),  j < nd
+ * (the other rows of out are not touched).  rows_max_len bounds the lengths
+ * of the selected queries only: launched for a group of queries of similar
+ * length, the kernel's shared memory (boundary rows and staged columns of
+ * rows_max_len points) admits more CTAs per SM than one launch sized for the
+ * longest query of Q.  Same reference call as tsm_matrix.
+ */
+int tsm_matrix_rows(int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len,
+                    const int32_t* q_rows, int64_t n_rows, int32_t rows_max_len, const float* d_pts,
+                    const int64_t* d_off, const int32_t* d_len, const int32_t* d_order, int64_t nd, int32_t d_max_len,
+                    const tsm_params* params, float* out, int64_t ld_out, int32_t* out_counts, void* stream);
+
+/*
  * Symmetric all pairs of one set S (the clustering shape):
  *   out[i*ld_out + j] = out[j*ld_out + i] = measure(S_i, S_j),  i, j < n,
  * computing each unordered pair once (every measure here is symmetric, and

@@ -475,3 +475,40 @@ def test_pairs_beyond_8192_points(oracle_mod):
             np.testing.assert_array_equal(cnt, wcnt)
     with pytest.raises(_lib.TsmError, match="TSM_ETOOLONG|-3"):
         run_pairs(0, np.zeros((33000, 2), np.float32), np.array([0]), np.array([33000]), np.array([0]), np.array([0]))
+
+
+@pytest.mark.parametrize("m", MEAS)
+def test_matrix_rows_and_length_buckets(m):
+    """tsm_matrix_rows writes exactly the selected rows, with tsm_matrix's
+    values; matrix_raw's length-bucketed launches (one per query-length
+    group) give the one-launch matrix bit for bit, counts included."""
+    import ctypes
+    from trajsimimeasures_b200 import _lib, datagen as D
+    from trajsimimeasures_b200.engine import TrajSet, _ptr, matrix_raw
+    rng = np.random.default_rng(90 + m)
+    pts, off, lens = D._walks(rng, rng.integers(1, 260, 400), D.STEP_SIGMA)
+    s = TrajSet.from_packed(pts, off, lens)
+    n = s.n
+    ref = torch.empty((n, n), device="cuda")
+    rc = torch.empty((n, n), dtype=torch.int32, device="cuda") if m in (1, 2) else None
+    matrix_raw(m, s, s, out=ref, counts=rc, eps=EPS, gpoint=G, buckets=1)
+    got = torch.full((n, n), -7.0, device="cuda")
+    gc = torch.full((n, n), -7, dtype=torch.int32, device="cuda") if m in (1, 2) else None
+    matrix_raw(m, s, s, out=got, counts=gc, eps=EPS, gpoint=G, buckets=4)
+    torch.cuda.synchronize()
+    assert torch.equal(got, ref)
+    if rc is not None:
+        assert torch.equal(gc, rc)
+    rows = torch.as_tensor(np.sort(rng.choice(n, 37, replace=False)).astype(np.int32)).cuda()
+    sel = torch.full((n, n), -7.0, device="cuda")
+    lib = _lib.load()
+    p = _lib.params(EPS, G, False, 0)
+    assert lib.tsm_matrix_rows(m, _ptr(s.pts), _ptr(s.off), _ptr(s.lens), _ptr(rows), 37,
+                               int(s.lens[rows.long()].max()), _ptr(s.pts), _ptr(s.off), _ptr(s.lens),
+                               _ptr(s.order_by_length()), n, s.max_len, ctypes.byref(p), _ptr(sel), n, None,
+                               None) == 0
+    torch.cuda.synchronize()
+    mask = torch.zeros(n, dtype=torch.bool, device="cuda")
+    mask[rows.long()] = True
+    assert torch.equal(sel[mask], ref[mask])
+    assert bool((sel[~mask] == -7.0).all())

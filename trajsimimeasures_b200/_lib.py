@@ -20,6 +20,7 @@ FLAG_EXACT = 1
 
 # Every symbol include/tsm.h declares (checked by the test suite).
 EXPORTS = ("tsm_version", "tsm_last_error", "tsm_max_supported_len", "tsm_matrix_query_max", "tsm_pairs", "tsm_matrix",
+           "tsm_matrix_rows",
            "tsm_sched_workspace_bytes", "tsm_pairs_sched", "tsm_topk_rows", "tsm_pairs_sched_noalloc",
            "tsm_enc_param_count", "tsm_enc_workspace_bytes", "tsm_enc_forward", "tsm_enc_loss_grad", "tsm_enc_adam",
            "tsm_select_rows", "tsm_allpairs_sym", "tsm_matrix_gather", "tsm_enc_embed_workspace_bytes",
@@ -64,6 +65,9 @@ def load():
         lib.tsm_matrix.restype = ctypes.c_int
         lib.tsm_matrix.argtypes = [ctypes.c_int, _vp, _vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _i64, _i32,
                                    ctypes.POINTER(TsmParams), _vp, _i64, _vp, _vp]
+        lib.tsm_matrix_rows.restype = ctypes.c_int
+        lib.tsm_matrix_rows.argtypes = [ctypes.c_int, _vp, _vp, _vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _i64, _i32,
+                                        ctypes.POINTER(TsmParams), _vp, _i64, _vp, _vp]
         lib.tsm_matrix_gather.restype = ctypes.c_int
         lib.tsm_matrix_gather.argtypes = [ctypes.c_int, _vp, _vp, _vp, _i64, _i32, _vp, _vp, _vp, _i64, _i32, _vp, _i64,
                                           ctypes.POINTER(TsmParams), _vp, _i64, _vp, _vp]

@@ -344,6 +344,22 @@ int tsm_matrix(int measure, const float* q_pts, const int64_t* q_off, const int3
                          d_order, nd, nd, d_max_len, 0, params, out, ld_out, out_counts, stream);
 }
 
+int tsm_matrix_rows(int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len,
+                    const int32_t* q_rows, int64_t n_rows, int32_t rows_max_len, const float* d_pts,
+                    const int64_t* d_off, const int32_t* d_len, const int32_t* d_order, int64_t nd, int32_t d_max_len,
+                    const tsm_params* params, float* out, int64_t ld_out, int32_t* out_counts, void* stream) {
+    g_err.clear();
+    if (measure < TSM_DTW || measure > TSM_HAUSDORFF) return fail(TSM_EINVAL, "tsm_matrix_rows: unknown measure %d", measure);
+    if (n_rows < 0 || nd < 0) return fail(TSM_EINVAL, "tsm_matrix_rows: negative set size");
+    if (n_rows == 0 || nd == 0) return TSM_OK;
+    if (!q_pts || !q_off || !q_len || !q_rows || !d_pts || !d_off || !d_len || !out)
+        return fail(TSM_EINVAL, "tsm_matrix_rows: null pointer");
+    if (ld_out < nd) return fail(TSM_EINVAL, "tsm_matrix_rows: ld_out < nd");
+    if (rows_max_len < 0 || d_max_len < 0) return fail(TSM_EINVAL, "tsm_matrix_rows: max_len < 0");
+    return matrix_launch("tsm_matrix_rows", measure, q_pts, q_off, q_len, q_rows, n_rows, rows_max_len, d_pts, d_off,
+                         d_len, d_order, nd, nd, d_max_len, 0, params, out, ld_out, out_counts, stream);
+}
+
 int tsm_matrix_gather(int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len, int64_t nq,
                       int32_t q_max_len, const float* d_pts, const int64_t* d_off, const int32_t* d_len, int64_t nd,
                       int32_t d_max_len, const int32_t* cand, int64_t ncand, const tsm_params* params, float* out,

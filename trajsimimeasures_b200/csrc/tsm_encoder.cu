@@ -567,7 +567,8 @@ __global__ void enc_adam(float* __restrict__ p, const float* __restrict__ g, flo
 // (n needs Whn h apart from Win a: r multiplies only the hidden part.)  One
 // thread issues the 24 MMAs and commits them to an mbarrier; then warp w reads
 // lanes 32 (w % 4) .. +31 (its 32 trajectories) and hidden units
-// 64 (w / 4) .. +63, applies the gates with the biases in FP32, keeps h in FP32
+// 64 (w / 4) .. +63 (sixteen warps, 32 units each, measured no faster: 1.31 vs
+// 1.39 ms for 1,000 queries), applies the gates with the biases in FP32, keeps h in FP32
 // registers and writes it back to shared memory as BF16 for the next step.
 // The a_t part comes from enc_conv_fwd_tc as one 16 KB BF16 image per step
 // already in the operand layout; thread 0 bulk-copies step t+1's image into
@@ -577,7 +578,8 @@ __global__ void enc_adam(float* __restrict__ p, const float* __restrict__ g, flo
 // hardware tanh, so the embeddings agree with the training forward to BF16
 // rounding of the activations.
 constexpr int TC_M = 128;
-constexpr int TC_THREADS = 256;
+constexpr int TC_THREADS = 256;  // 8 warps: two per 32-lane quarter of tensor memory
+constexpr int TC_HU = HD / (TC_THREADS / 128);  // hidden units per thread (32)
 constexpr int TC_K = C1 + HD;                               // 192
 constexpr int TC_A_BYTES = TC_M * C1 * 2;                   // one a_t image: 16 KB
 constexpr int TC_OFF_A0 = 0;                                // a-buffers [128][64] BF16
@@ -699,7 +701,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfl
     volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(sm + TC_OFF_BAR + 24);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int row = 32 * (warp & 3) + lane;  // this thread's trajectory (TMEM lane)
-    const int hc = warp >> 2;                // hidden units 64 hc .. +63
+    const int hc = warp >> 2;                // hidden units TC_HU hc .. +TC_HU-1
     const int b = blockIdx.x * TC_M + row;
     const int n = b < B ? len[b] : 0;
     const __nv_bfloat16* img = Ab + (int64_t)blockIdx.x * T * (TC_M * C1);  // this block's a_t images
@@ -725,7 +727,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfl
     {  // h_0 = 0: this thread's 64 hidden units
         const float z8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-        for (int c = 0; c < 8; ++c) *reinterpret_cast<uint4*>(XH + U::core_offset(row, 64 * hc + 8 * c, TC_M)) = pack8_bf16(z8);
+        for (int c = 0; c < TC_HU / 8; ++c)
+            *reinterpret_cast<uint4*>(XH + U::core_offset(row, TC_HU * hc + 8 * c, TC_M)) = pack8_bf16(z8);
     }
     if (tid == 0) {
         U::mbar_init(mbar, 1);
@@ -754,9 +757,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfl
         if (stall_step != 0) U::bulk_load(sbase + TC_OFF_A0, img, TC_A_BYTES, abar0);
         pend = 0;
     }
-    float h[64];
+    float h[TC_HU];
 #pragma unroll
-    for (int i = 0; i < 64; ++i) h[i] = 0.f;
+    for (int i = 0; i < TC_HU; ++i) h[i] = 0.f;
     bool failed = false;
     int fail_t = -1;
     for (int t = 0; t < tmax; ++t) {
@@ -802,8 +805,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfl
         U::fence_after_sync();
         const bool live = t < n;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {  // 16 hidden units at a time
-            const int k0 = 64 * hc + 16 * c;
+        for (int c = 0; c < TC_HU / 16; ++c) {  // 16 hidden units at a time
+            const int k0 = TC_HU * hc + 16 * c;
             uint32_t rr[16], zz[16], ii[16], hh[16];
             U::ld16(tl + k0, rr);
             U::ld16(tl + HD + k0, zz);
@@ -848,9 +851,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfl
         }
     }
     if (b < B) {
-        float* dst = hl + (int64_t)b * HD + 64 * hc;
+        float* dst = hl + (int64_t)b * HD + TC_HU * hc;
 #pragma unroll
-        for (int i = 0; i < 64; ++i) dst[i] = failed ? __int_as_float(0x7fc00000) : h[i];
+        for (int i = 0; i < TC_HU; ++i) dst[i] = failed ? __int_as_float(0x7fc00000) : h[i];
     }
     U::fence_before_sync();
     __syncthreads();

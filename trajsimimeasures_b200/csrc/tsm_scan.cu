@@ -22,15 +22,19 @@
 // squared norms |e_j|^2 are FP32 and enter in the epilogue.
 //
 // Kernel.  One CTA per (query tile of 128, slice of database tiles of 256
-// rows).  The query tile's operand image (120 KB) stays in shared memory;
-// the database rows stream through a four-stage ring of 24 KB stages
-// (cp.async.bulk of pre-formatted operand images, completion on mbarrier
-// transaction counts).  Warp 0 issues the copies, one thread of warp 1 issues
+// rows).  Both operands stream through a six-stage ring in shared memory,
+// each stage a K slice of 48 of the query tile (12 KB, re-read from L2 for
+// every database tile) and of the database tile (24 KB): cp.async.bulk of
+// pre-formatted operand images, completion on mbarrier transaction counts.
+// (Keeping the query tile resident instead left room for four stages only,
+// and the copies' latency held the tensor pipe to a third of its time.)  Warp 0 issues the copies, one thread of warp 1 issues
 // the MMAs (M = 128 queries, N = 256 rows, K = 16 per instruction, 30 per
 // database tile) into one of two FP32 accumulators of 256 tensor-memory
-// columns, and warps 2-5 (one per 32-lane quarter of tensor memory) read the
-// other accumulator with tcgen05.ld, form d and apply the threshold while the
-// next tile's MMAs run.  Every wait is bounded (about 1 s of SM clocks); one
+// columns, and warps 2-9 (two per 32-lane quarter of tensor memory, each
+// reading half of the columns, 64 per tensor-memory load batch) read the
+// other accumulator with tcgen05.ld, form d and apply the threshold (one
+// compare per 64 values against their tree minimum) while the next tile's
+// MMAs run.  Every wait is bounded (about 1 s of SM clocks); one
 // that runs out sets a bit of *status and ends that role's loop, the CTA
 // waits (bounded) for its own copies and MMAs in flight, and frees tensor
 // memory only when no MMA can still write it.
@@ -58,17 +62,20 @@ constexpr int KCH = K / 8;                 // 16-byte K chunks of a row
 constexpr int QM = 128;                    // queries per tile (MMA M, tensor-memory lanes)
 constexpr int DN = 256;                    // database rows per tile (MMA N)
 constexpr int SK = 48;                     // K per pipeline stage: three MMAs of K = 16
-constexpr int NSTAGE = 4;
+constexpr int NSTAGE = 6;
 constexpr int STAGES_PER_TILE = K / SK;    // 10
-constexpr int A_BYTES = QM * K * 2;        // 122,880
-constexpr int B_TILE_BYTES = DN * K * 2;   // 245,760
+constexpr int A_BYTES = QM * K * 2;        // 122,880: one query tile's image
+constexpr int B_TILE_BYTES = DN * K * 2;   // 245,760: one database tile's image
+constexpr int A_STAGE_BYTES = QM * SK * 2; // 12,288
 constexpr int B_STAGE_BYTES = DN * SK * 2; // 24,576
-constexpr int THREADS = 192;               // warp 0 copies, warp 1 MMAs, warps 2-5 epilogue
+constexpr int STAGE_BYTES = A_STAGE_BYTES + B_STAGE_BYTES;
+constexpr int EPI_WARPS = 8;               // two per 32-lane quarter of tensor memory, each half the columns
+constexpr int THREADS = 64 + 32 * EPI_WARPS;  // warp 0 copies, warp 1 MMAs, warps 2-9 epilogue
+constexpr int EPI_COLS = 64;               // accumulator columns per tensor-memory load batch
 constexpr uint32_t TMEM_COLS = 2 * DN;     // two accumulators
 constexpr int NNORM = 4;                   // squared-norm ring: one database tile's norms per slot
-constexpr int OFF_A = 0;
-constexpr int OFF_B = A_BYTES;
-constexpr int OFF_N = OFF_B + NSTAGE * B_STAGE_BYTES;
+constexpr int OFF_S = 0;                   // NSTAGE stages of [A part | B part]
+constexpr int OFF_N = OFF_S + NSTAGE * STAGE_BYTES;
 constexpr int OFF_BAR = OFF_N + NNORM * DN * 4;
 constexpr int SMEM = OFF_BAR + 256;        // 225,536 bytes
 constexpr long long WAIT_CYCLES = 2000000000LL;
@@ -135,13 +142,13 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
     const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
     const uint32_t bar = sbase + OFF_BAR;
     // mbarriers: full[4] (copies landed), empty[4] (stage read by the MMAs),
-    // tfull[2] (accumulator ready), tempty[2] (accumulator read), A landed, all
-    // MMAs done, nfull[4] (a tile's norms landed), nempty[4] (norms read)
-    auto full = [&](int i) { return bar + 8 * i; };
-    auto empty = [&](int i) { return bar + 32 + 8 * i; };
-    auto tfull = [&](int b) { return bar + 64 + 8 * b; };
-    auto tempty = [&](int b) { return bar + 80 + 8 * b; };
-    const uint32_t abar = bar + 96, donebar = bar + 104;
+    // tfull[2] (accumulator ready), tempty[2] (accumulator read), all MMAs
+    // done, nfull[4] (a tile's norms landed), nempty[4] (norms read)
+    auto full = [&](int i) { return bar + 8 * i; };         // i < NSTAGE (6): bytes 0..47
+    auto empty = [&](int i) { return bar + 48 + 8 * i; };   // 48..95
+    auto tfull = [&](int b) { return bar + 184 + 8 * b; };
+    auto tempty = [&](int b) { return bar + 200 + 8 * b; };
+    const uint32_t donebar = bar + 104;
     auto nfull = [&](int i) { return bar + 112 + 8 * i; };
     auto nempty = [&](int i) { return bar + 144 + 8 * i; };
     volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(sm + OFF_BAR + 176);
@@ -161,13 +168,12 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
         }
         for (int b = 0; b < 2; ++b) {
             U::mbar_init(tfull(b), 1);
-            U::mbar_init(tempty(b), 4);  // one arrival per epilogue warp
+            U::mbar_init(tempty(b), EPI_WARPS);  // one arrival per epilogue warp
         }
-        U::mbar_init(abar, 1);
         U::mbar_init(donebar, 1);
         for (int i = 0; i < NNORM; ++i) {
             U::mbar_init(nfull(i), 1);
-            U::mbar_init(nempty(i), 4);  // one arrival per epilogue warp
+            U::mbar_init(nempty(i), EPI_WARPS);
         }
         *tmem_busy = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -180,10 +186,7 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
 
     if (warp == 0) {
         if (lane == 0 && ntl > 0) {  // copies
-            U::mbar_arrive_expect_tx(abar, A_BYTES);
             const unsigned char* asrc = reinterpret_cast<const unsigned char*>(qimg) + (int64_t)qt * A_BYTES;
-            for (int c = 0; c < 4; ++c)
-                U::bulk_load(sbase + OFF_A + c * (A_BYTES / 4), asrc + c * (A_BYTES / 4), A_BYTES / 4, abar);
             int64_t g = 0;  // stages issued
             int64_t nt = 0;  // tiles whose norms were issued
             bool ok = true;
@@ -208,9 +211,10 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
                         ok = false;
                         break;
                     }
-                    U::mbar_arrive_expect_tx(full(slot), B_STAGE_BYTES);
-                    U::bulk_load(sbase + OFF_B + slot * B_STAGE_BYTES, bsrc + k * B_STAGE_BYTES, B_STAGE_BYTES,
-                                 full(slot));
+                    const uint32_t st = sbase + OFF_S + slot * STAGE_BYTES;
+                    U::mbar_arrive_expect_tx(full(slot), STAGE_BYTES);
+                    U::bulk_load(st, asrc + k * A_STAGE_BYTES, A_STAGE_BYTES, full(slot));
+                    U::bulk_load(st + A_STAGE_BYTES, bsrc + k * B_STAGE_BYTES, B_STAGE_BYTES, full(slot));
                     ++g;
                 }
             }
@@ -219,13 +223,10 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
                 if (slot < g) U::mbar_wait(full(slot), (uint32_t)((g - 1 - slot) / NSTAGE) & 1, wait_cycles);
             for (int slot = 0; slot < NNORM; ++slot)
                 if (slot < nt) U::mbar_wait(nfull(slot), (uint32_t)((nt - 1 - slot) / NNORM) & 1, wait_cycles);
-            U::mbar_wait(abar, 0, wait_cycles);
         }
     } else if (warp == 1) {
         if (lane == 0 && ntl > 0) {  // MMAs
-            bool ok = U::mbar_wait(abar, 0, wait_cycles);
-            if (!ok) atomicOr(status, ERR_COPY);
-            U::fence_after_sync();
+            bool ok = true;
             constexpr uint32_t idesc = U::idesc_f16_f32(QM, DN);
             int64_t g = 0;
             for (int64_t t = 0; t < ntl && ok; ++t) {
@@ -246,12 +247,12 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
                         break;
                     }
                     U::fence_after_sync();
+                    const uint32_t st = sbase + OFF_S + slot * STAGE_BYTES;
 #pragma unroll
                     for (int kk = 0; kk < SK / 16; ++kk) {
                         const int ks = k * (SK / 16) + kk;
-                        const uint64_t ad = U::smem_desc(sbase + OFF_A + ks * 2 * (QM * 16), QM * 16, 128);
-                        const uint64_t bd =
-                            U::smem_desc(sbase + OFF_B + slot * B_STAGE_BYTES + kk * 2 * (DN * 16), DN * 16, 128);
+                        const uint64_t ad = U::smem_desc(st + kk * 2 * (QM * 16), QM * 16, 128);
+                        const uint64_t bd = U::smem_desc(st + A_STAGE_BYTES + kk * 2 * (DN * 16), DN * 16, 128);
                         U::mma_bf16(dt, ad, bd, idesc, ks > 0 ? 1u : 0u);  // kind::f16 issue (FP16 idesc)
                     }
                     U::commit(empty(slot));
@@ -267,8 +268,9 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
                 *tmem_busy = 1;
             }
         }
-    } else {  // epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. +31
+    } else {  // epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. +31, columns half * 128 .. +127
         const int quarter = warp & 3;
+        const int half = (warp - 2) >> 2;
         const int64_t q = (int64_t)qt * QM + 32 * quarter + lane;
         const bool qv = q < nq;
         // padding queries get -inf: no d (>= finite or +inf) is at or below it
@@ -284,39 +286,50 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
                 break;
             }
             U::fence_after_sync();
-            const int64_t j0 = (t0 + t) * DN;
-            const uint32_t ta = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(b * DN);
-            const float4* nr = reinterpret_cast<const float4*>(sm + OFF_N + ns * (DN * 4));
+            const uint32_t ta = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(b * DN + half * (DN / 2));
+            const float4* nr = reinterpret_cast<const float4*>(sm + OFF_N + ns * (DN * 4)) + half * (DN / 8);
+            const int64_t jh = (t0 + t) * DN + half * (DN / 2);
 #pragma unroll 1
-            for (int cg = 0; cg < DN / 16; ++cg) {
-                uint32_t r[16];
-                U::ld16(ta + cg * 16, r);
-                U::wait_ld(r);
-                float d[16];
-                float mn = __int_as_float(0x7f800000);
+            for (int cb = 0; cb < DN / 2; cb += EPI_COLS) {
+                uint32_t r0[16], r1[16], r2[16], r3[16];
+                U::ld16(ta + cb, r0);
+                U::ld16(ta + cb + 16, r1);
+                U::ld16(ta + cb + 32, r2);
+                U::ld16(ta + cb + 48, r3);
+                U::wait_ld(r0);
+                U::wait_ld(r1);
+                U::wait_ld(r2);
+                U::wait_ld(r3);
+                float d[EPI_COLS];
 #pragma unroll
-                for (int i4 = 0; i4 < 4; ++i4) {
-                    const float4 nv = nr[cg * 4 + i4];  // same address in every lane: a broadcast
-                    d[4 * i4 + 0] = fmaf(m2, __uint_as_float(r[4 * i4 + 0]), nv.x);
-                    d[4 * i4 + 1] = fmaf(m2, __uint_as_float(r[4 * i4 + 1]), nv.y);
-                    d[4 * i4 + 2] = fmaf(m2, __uint_as_float(r[4 * i4 + 2]), nv.z);
-                    d[4 * i4 + 3] = fmaf(m2, __uint_as_float(r[4 * i4 + 3]), nv.w);
+                for (int i4 = 0; i4 < EPI_COLS / 4; ++i4) {
+                    const float4 nv = nr[cb / 4 + i4];  // the same address in every lane: a broadcast
+                    const uint32_t* rr = i4 < 4 ? r0 : (i4 < 8 ? r1 : (i4 < 12 ? r2 : r3));
+                    const int o = (4 * i4) & 15;
+                    d[4 * i4 + 0] = fmaf(m2, __uint_as_float(rr[o + 0]), nv.x);
+                    d[4 * i4 + 1] = fmaf(m2, __uint_as_float(rr[o + 1]), nv.y);
+                    d[4 * i4 + 2] = fmaf(m2, __uint_as_float(rr[o + 2]), nv.z);
+                    d[4 * i4 + 3] = fmaf(m2, __uint_as_float(rr[o + 3]), nv.w);
                 }
+                const int64_t jb = jh + cb;
                 if (DENSE) {
                     if (qv) {
 #pragma unroll
-                        for (int i = 0; i < 16; ++i) {
-                            const int64_t j = j0 + cg * 16 + i;
-                            if (j < nd) dense[q * ld + j] = d[i];
-                        }
+                        for (int i = 0; i < EPI_COLS; ++i)
+                            if (jb + i < nd) dense[q * ld + jb + i] = d[i];
                     }
                 } else {
+                    float mn[EPI_COLS / 2];  // tree minimum: depth 6, not a chain of 64
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) mn = fminf(mn, d[i]);
-                    if (mn <= th) {  // rare: at least one of the 16 survives
+                    for (int i = 0; i < EPI_COLS / 2; ++i) mn[i] = fminf(d[2 * i], d[2 * i + 1]);
 #pragma unroll
-                        for (int i = 0; i < 16; ++i) {
-                            const int64_t j = j0 + cg * 16 + i;
+                    for (int w2 = EPI_COLS / 4; w2 >= 1; w2 >>= 1)
+#pragma unroll
+                        for (int i = 0; i < w2; ++i) mn[i] = fminf(mn[i], mn[i + w2]);
+                    if (mn[0] <= th) {  // rare: at least one of the 64 survives (unrolled: d stays in registers)
+#pragma unroll
+                        for (int i = 0; i < EPI_COLS; ++i) {
+                            const int64_t j = jb + i;
                             if (d[i] <= th && j < nd) {
                                 const int pos = atomicAdd(counts + q, 1);
                                 if (pos < cap) {
