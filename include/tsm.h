@@ -254,13 +254,14 @@ int tsm_select_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, 
  * test_knn_time.py:138-202).  For embeddings of tsm_scan_dim() values
  * (centred by the caller), d(q, j) = |e_j|^2 - 2 e_q . e_j, computed as one
  * product of FP16 hi/lo splits, [q_hi | q_lo | q_hi] . [d_hi | d_hi | d_lo],
- * with FP32 accumulation (about 2^-21 relative per product) and FP32 norms.
+ * with the squared norms (three FP16 parts) folded into the same product and
+ * FP32 accumulation (about 2^-21 relative per product).
  *   tsm_scan_prepare: operand image of n rows of emb (row stride ld floats),
- *       scaled by `scale` (a power of two keeping |scale * emb| well inside
- *       FP16's range); is_db = 1: database image (tiles of 256 rows) and
- *       norms float32 [tsm_scan_norms_count(n)] (the padding rows get +inf);
- *       0: query image (tiles of 128 rows).  img: device memory of
- *       tsm_scan_image_bytes(n, is_db) bytes; img and norms 16-byte aligned.
+ *       scaled by `scale`, a power of two keeping |scale * emb| <= 1024;
+ *       is_db = 1: database image (tiles of 256 rows), and norms float32 [n]
+ *       (nullable) receives |emb_j|^2; 0: query image (tiles of 128 rows).
+ *       img: device memory of tsm_scan_image_bytes(n, is_db) bytes, 16-byte
+ *       aligned.
  *   tsm_scan: either dense (thresholds NULL): dense[q * ld_dense + j] = d;
  *       or candidate lists (dense NULL): for each pair with d <= thresholds[q]
  *       a slot of counts[q] (zeroed by the caller) is taken and, below cap,
@@ -272,16 +273,15 @@ int tsm_select_rows(const float* d, int64_t n_rows, int64_t n_cols, int64_t ld, 
  */
 int32_t tsm_scan_dim(void);
 int64_t tsm_scan_image_bytes(int64_t n_rows, int32_t is_db);
-int64_t tsm_scan_norms_count(int64_t n_rows);
 int tsm_scan_prepare(const float* emb, int64_t n, int64_t ld, float scale, int32_t is_db, void* img, float* norms,
                      void* stream);
-int tsm_scan(const void* q_img, int64_t nq, const void* db_img, const float* db_norms, int64_t nd, float scale,
-             const float* thresholds, int32_t cap, int32_t* cand_idx, float* cand_d, int32_t* counts, float* dense,
-             int64_t ld_dense, int32_t* status, void* stream);
+int tsm_scan(const void* q_img, int64_t nq, const void* db_img, int64_t nd, float scale, const float* thresholds,
+             int32_t cap, int32_t* cand_idx, float* cand_d, int32_t* counts, float* dense, int64_t ld_dense,
+             int32_t* status, void* stream);
 /* tsm_scan with its wait limit in SM clocks (tsm_scan uses about 1 s). */
-int tsm_scan_opts(const void* q_img, int64_t nq, const void* db_img, const float* db_norms, int64_t nd, float scale,
-                  const float* thresholds, int32_t cap, int32_t* cand_idx, float* cand_d, int32_t* counts,
-                  float* dense, int64_t ld_dense, int32_t* status, int64_t wait_cycles, void* stream);
+int tsm_scan_opts(const void* q_img, int64_t nq, const void* db_img, int64_t nd, float scale, const float* thresholds,
+                  int32_t cap, int32_t* cand_idx, float* cand_d, int32_t* counts, float* dense, int64_t ld_dense,
+                  int32_t* status, int64_t wait_cycles, void* stream);
 
 /*
  * Learned candidate filter (trajectory encoder).  The reference's learned

@@ -25,7 +25,7 @@ EXPORTS = ("tsm_version", "tsm_last_error", "tsm_max_supported_len", "tsm_matrix
            "tsm_enc_param_count", "tsm_enc_workspace_bytes", "tsm_enc_forward", "tsm_enc_loss_grad", "tsm_enc_adam",
            "tsm_select_rows", "tsm_allpairs_sym", "tsm_matrix_gather", "tsm_enc_embed_workspace_bytes",
            "tsm_enc_embed", "tsm_enc_embed_status", "tsm_enc_embed_opts", "tsm_enc_loss_grad_w", "tsm_scan_dim",
-           "tsm_scan_image_bytes", "tsm_scan_norms_count", "tsm_scan_prepare", "tsm_scan", "tsm_scan_opts")
+           "tsm_scan_image_bytes", "tsm_scan_prepare", "tsm_scan", "tsm_scan_opts")
 
 
 class TsmParams(ctypes.Structure):
@@ -107,16 +107,13 @@ def load():
         lib.tsm_scan_dim.restype = _i32
         lib.tsm_scan_image_bytes.restype = _i64
         lib.tsm_scan_image_bytes.argtypes = [_i64, _i32]
-        lib.tsm_scan_norms_count.restype = _i64
-        lib.tsm_scan_norms_count.argtypes = [_i64]
         lib.tsm_scan_prepare.restype = ctypes.c_int
         lib.tsm_scan_prepare.argtypes = [_vp, _i64, _i64, ctypes.c_float, _i32, _vp, _vp, _vp]
         lib.tsm_scan.restype = ctypes.c_int
-        lib.tsm_scan.argtypes = [_vp, _i64, _vp, _vp, _i64, ctypes.c_float, _vp, _i32, _vp, _vp, _vp, _vp, _i64, _vp,
-                                 _vp]
+        lib.tsm_scan.argtypes = [_vp, _i64, _vp, _i64, ctypes.c_float, _vp, _i32, _vp, _vp, _vp, _vp, _i64, _vp, _vp]
         lib.tsm_scan_opts.restype = ctypes.c_int
-        lib.tsm_scan_opts.argtypes = [_vp, _i64, _vp, _vp, _i64, ctypes.c_float, _vp, _i32, _vp, _vp, _vp, _vp, _i64,
-                                      _vp, _i64, _vp]
+        lib.tsm_scan_opts.argtypes = [_vp, _i64, _vp, _i64, ctypes.c_float, _vp, _i32, _vp, _vp, _vp, _vp, _i64, _vp,
+                                      _i64, _vp]
         lib.tsm_select_rows.restype = ctypes.c_int
         lib.tsm_select_rows.argtypes = [_vp, _i64, _i64, _i64, _i64, _vp, _vp]
         lib.tsm_topk_rows.restype = ctypes.c_int

@@ -17,27 +17,35 @@
 // as ONE product over K = 3 x 160: queries [q_hi | q_lo | q_hi] against rows
 // [d_hi | d_hi | d_lo], accumulated in FP32 -- the split-product method
 // (Markidis et al., "NVIDIA Tensor Core Programmability, Performance &
-// Precision", IPDPSW 2018), about 2^-21 relative per product.  The values are
-// scaled by a power of two s (exact) so that they use FP16's range; the
-// squared norms |e_j|^2 are FP32 and enter in the epilogue.
+// Precision", IPDPSW 2018), about 2^-21 relative per product.  The squared
+// norm enters the same product: three more K columns hold, for the row, the
+// FP32 value n_j = |e_j|^2 s^2 / 2^16 split into three FP16 parts (33
+// significant bits) and, for the query, 2^15 each, so the accumulator is
+//     acc = s^2 (e_q . e_j - |e_j|^2 / 2) = -(s^2 / 2) d(q, j)
+// and the epilogue compares raw accumulators (d <= thr  <=>  acc >= -(s^2/2) thr).
+// The values are scaled by a power of two s (exact) that keeps every scaled
+// value within 2^10 and n_j within FP16's range.  K = 512: the 483 columns
+// used, padded with zeros.
 //
 // Kernel.  One CTA per (query tile of 128, slice of database tiles of 256
-// rows).  Both operands stream through a six-stage ring in shared memory,
-// each stage a K slice of 48 of the query tile (12 KB, re-read from L2 for
-// every database tile) and of the database tile (24 KB): cp.async.bulk of
-// pre-formatted operand images, completion on mbarrier transaction counts.
-// (Keeping the query tile resident instead left room for four stages only,
-// and the copies' latency held the tensor pipe to a third of its time.)  Warp 0 issues the copies, one thread of warp 1 issues
-// the MMAs (M = 128 queries, N = 256 rows, K = 16 per instruction, 30 per
-// database tile) into one of two FP32 accumulators of 256 tensor-memory
-// columns, and warps 2-9 (two per 32-lane quarter of tensor memory, each
-// reading half of the columns, 64 per tensor-memory load batch) read the
-// other accumulator with tcgen05.ld, form d and apply the threshold (one
-// compare per 64 values against their tree minimum) while the next tile's
-// MMAs run.  Every wait is bounded (about 1 s of SM clocks); one
-// that runs out sets a bit of *status and ends that role's loop, the CTA
-// waits (bounded) for its own copies and MMAs in flight, and frees tensor
-// memory only when no MMA can still write it.
+// rows).  The query tile's image (128 KB) is copied into shared memory once and
+// stays there; the database tiles stream through a five-stage ring, each stage
+// a K slice of 32 (16 KB): cp.async.bulk of pre-formatted operand images,
+// completion on mbarrier transaction counts.  Warp 0 issues the copies, one
+// thread of warp 1 issues the MMAs (M = 128 queries, N = 256 rows, K = 16 per
+// instruction, 32 per database tile) into one of two FP32 accumulators of 256
+// tensor-memory columns, and warps 2-9 (two per 32-lane quarter of tensor
+// memory, each reading half of the columns, 64 per tensor-memory load batch)
+// read the other accumulator with tcgen05.ld and apply the threshold -- one
+// compare per 64 values against their tree maximum -- while the next tile's
+// MMAs run.  A survivor is staged in shared memory (four slots per epilogue
+// thread); a warp flushes its staged survivors together (one atomicAdd per
+// thread on its query's count, then the stores) when a thread's slots are
+// full and at the end, so that the round trip of the atomic is paid about once
+// per dozen tiles rather than once per survivor.  Every wait is bounded (about
+// 1 s of SM clocks); one that runs out sets a bit of *status and ends that
+// role's loop, the CTA waits (bounded) for its own copies and MMAs in flight,
+// and frees tensor memory only when no MMA can still write it.
 //
 // Operand images (tsm_scan_prepare): tiles of R rows (128 for queries, 256
 // for the database), each in the K-major core-matrix layout of tsm_umma.cuh
@@ -57,29 +65,37 @@ namespace tsm {
 namespace scan {
 
 constexpr int D = 160;                     // embedding width
-constexpr int K = 3 * D;                   // split-product K
+constexpr int KE = 3 * D;                  // split-product columns
+constexpr int K = 512;                     // + 3 norm columns, zero padding
 constexpr int KCH = K / 8;                 // 16-byte K chunks of a row
 constexpr int QM = 128;                    // queries per tile (MMA M, tensor-memory lanes)
 constexpr int DN = 256;                    // database rows per tile (MMA N)
-constexpr int SK = 48;                     // K per pipeline stage: three MMAs of K = 16
-constexpr int NSTAGE = 6;
-constexpr int STAGES_PER_TILE = K / SK;    // 10
-constexpr int A_BYTES = QM * K * 2;        // 122,880: one query tile's image
-constexpr int B_TILE_BYTES = DN * K * 2;   // 245,760: one database tile's image
-constexpr int A_STAGE_BYTES = QM * SK * 2; // 12,288
-constexpr int B_STAGE_BYTES = DN * SK * 2; // 24,576
-constexpr int STAGE_BYTES = A_STAGE_BYTES + B_STAGE_BYTES;
+constexpr int SK = 32;                     // K per pipeline stage: two MMAs of K = 16
+constexpr int NSTAGE = 5;
+constexpr int STAGES_PER_TILE = K / SK;    // 16
+constexpr int A_BYTES = QM * K * 2;        // 131,072: one query tile's image (resident)
+constexpr int A_COPY = 8192;               // its copies
+constexpr int B_TILE_BYTES = DN * K * 2;   // 262,144: one database tile's image
+constexpr int B_STAGE_BYTES = DN * SK * 2; // 16,384
 constexpr int EPI_WARPS = 8;               // two per 32-lane quarter of tensor memory, each half the columns
-constexpr int THREADS = 64 + 32 * EPI_WARPS;  // warp 0 copies, warp 1 MMAs, warps 2-9 epilogue
+constexpr int EPI_THREADS = 32 * EPI_WARPS;
+constexpr int THREADS = 64 + EPI_THREADS;  // warp 0 copies, warp 1 MMAs, warps 2-9 epilogue
 constexpr int EPI_COLS = 64;               // accumulator columns per tensor-memory load batch
+constexpr int SLOTS = 4;                   // staged survivors per epilogue thread
 constexpr uint32_t TMEM_COLS = 2 * DN;     // two accumulators
-constexpr int NNORM = 4;                   // squared-norm ring: one database tile's norms per slot
-constexpr int OFF_S = 0;                   // NSTAGE stages of [A part | B part]
-constexpr int OFF_N = OFF_S + NSTAGE * STAGE_BYTES;
-constexpr int OFF_BAR = OFF_N + NNORM * DN * 4;
-constexpr int SMEM = OFF_BAR + 256;        // 225,536 bytes
+constexpr int OFF_A = 0;
+constexpr int OFF_S = OFF_A + A_BYTES;     // NSTAGE database stages
+constexpr int OFF_BAR = OFF_S + NSTAGE * B_STAGE_BYTES;
+// mbarriers: full[NSTAGE], empty[NSTAGE], tfull[2], tempty[2], done, a_full; then the tensor-memory slot and flag
+constexpr int BAR_FULL = 0, BAR_EMPTY = 8 * NSTAGE, BAR_TFULL = 16 * NSTAGE, BAR_TEMPTY = BAR_TFULL + 16,
+              BAR_DONE = BAR_TEMPTY + 16, BAR_AFULL = BAR_DONE + 8, TMEM_SLOT = BAR_AFULL + 8, TMEM_BUSY = TMEM_SLOT + 4;
+constexpr int OFF_STG = OFF_BAR + 256;     // SLOTS x EPI_THREADS staged (index, d)
+constexpr int SMEM = OFF_STG + SLOTS * EPI_THREADS * 8;  // 221,440 bytes
 constexpr long long WAIT_CYCLES = 2000000000LL;
-static_assert(K % SK == 0 && SK % 16 == 0 && D % 8 == 0, "stage and chunk sizes");
+constexpr float NORM_A = 32768.f;          // the query's norm columns (2^15)
+constexpr float NORM_SHIFT = 1.f / 65536.f;  // n_j = |e_j|^2 s^2 2^-16
+static_assert(K % SK == 0 && SK % 16 == 0 && D % 8 == 0 && KE + 3 <= K && A_BYTES % A_COPY == 0, "sizes");
+static_assert(TMEM_BUSY + 4 <= 256, "barrier block");
 static_assert(SMEM <= 227 * 1024, "shared memory");
 
 // status bits
@@ -89,12 +105,14 @@ constexpr int ERR_TMEM = 4;   // MMAs still pending at exit: tensor memory left 
 constexpr int ERR_EPI = 8;    // the epilogue gave up waiting for an accumulator
 
 // Operand image of rows [0, n) of emb (row stride ld floats, D values each,
-// times s), padded with zero rows to whole tiles of R rows.  DB: rows
-// [hi | hi | lo] and FP32 squared norms |emb_j|^2 of the unscaled rows, +inf
-// for the padding rows of the last tile (their d is then +inf, below no
-// threshold); queries: [hi | lo | hi].  One thread per (row, 16-byte chunk),
-// consecutive threads on consecutive rows of one chunk (coalesced 16-byte
-// stores).
+// times s), padded with rows to whole tiles of R rows.  K columns: queries
+// [hi | lo | hi | 2^15 x 3 | 0...]; database rows [hi | hi | lo | -n_j
+// as three FP16 parts | 0...] with n_j = |emb_j|^2 s^2 2^-16 (the squared
+// norm of the unscaled row, FP32), and for the padding rows of the last tile
+// n_j parts at FP16's largest value, so that their accumulator is far below
+// any threshold.  norms (nullable): the FP32 |emb_j|^2 of the rows.  One
+// thread per (row, 16-byte chunk), consecutive threads on consecutive rows of
+// one chunk (coalesced 16-byte stores).
 template <bool DB>
 __global__ void scan_prepare(const float* __restrict__ emb, int64_t n, int64_t ld, float s, int64_t n_tiles,
                              __half* __restrict__ img, float* __restrict__ norms) {
@@ -105,54 +123,82 @@ __global__ void scan_prepare(const float* __restrict__ emb, int64_t n, int64_t l
     const int c = (gid / R) % KCH;
     const int64_t t = gid / ((int64_t)R * KCH);
     const int64_t row = t * R + r;
-    const int part = (8 * c) / D;  // which third of K
-    const int k0 = 8 * c - part * D;
     __align__(16) __half v[8];
+    if (8 * c < KE) {
+        const int part = (8 * c) / D;  // which third of the split product
+        const int k0 = 8 * c - part * D;
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-        const float x = row < n ? s * emb[row * ld + k0 + e] : 0.f;
-        const __half h = __float2half_rn(x);
-        const __half l = __float2half_rn(x - __half2float(h));
-        v[e] = DB ? (part < 2 ? h : l) : (part == 1 ? l : h);
+        for (int e = 0; e < 8; ++e) {
+            const float x = row < n ? s * emb[row * ld + k0 + e] : 0.f;
+            const __half h = __float2half_rn(x);
+            const __half l = __float2half_rn(x - __half2float(h));
+            v[e] = DB ? (part < 2 ? h : l) : (part == 1 ? l : h);
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < 8; ++e) v[e] = __float2half_rn(0.f);
+        if (8 * c == KE) {  // the norm columns
+            if (!DB) {
+                v[0] = v[1] = v[2] = __float2half_rn(NORM_A);
+            } else if (row < n) {
+                float ss = 0.f;
+                for (int k = 0; k < D; ++k) {
+                    const float x = emb[row * ld + k];
+                    ss = fmaf(x, x, ss);
+                }
+                if (norms) norms[row] = ss;
+                const float nj = ss * (s * s) * NORM_SHIFT;
+                const __half h = __float2half_rn(nj);
+                const float r1 = nj - __half2float(h);
+                const __half m = __float2half_rn(r1);
+                const __half l = __float2half_rn(r1 - __half2float(m));
+                v[0] = __hneg(h);
+                v[1] = __hneg(m);
+                v[2] = __hneg(l);
+            } else {
+                v[0] = v[1] = v[2] = __float2half_rn(-65504.f);
+            }
+        }
     }
     unsigned char* dst = reinterpret_cast<unsigned char*>(img) + t * ((int64_t)R * K * 2) +
                          (int64_t)c * (R * 16) + (r >> 3) * 128 + (r & 7) * 16;
     *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(v);
-    if (DB && norms && c == 0) {
-        float ss = __int_as_float(0x7f800000);  // +inf
-        if (row < n) {
-            ss = 0.f;
-            for (int k = 0; k < D; ++k) {
-                const float x = emb[row * ld + k];
-                ss = fmaf(x, x, ss);
-            }
+}
+
+// Moves a thread's `n` staged survivors (slots stg[0], stg[EPI_THREADS], ...)
+// to its query's list: one atomicAdd on the count, then the stores below cap.
+// Kept out of line: it runs about once per dozen tiles, and inlined at every
+// staging site it would crowd the instruction cache.
+__device__ __noinline__ void flush_staged(const uint2* stg, int n, int32_t* count, int32_t* idx_row, float* d_row,
+                                          int cap) {
+    const int pos = atomicAdd(count, n);
+    for (int e = 0; e < n; ++e) {
+        const uint2 v = stg[e * EPI_THREADS];
+        if (pos + e < cap) {
+            idx_row[pos + e] = (int32_t)v.x;
+            d_row[pos + e] = __uint_as_float(v.y);
         }
-        norms[row] = ss;
     }
 }
 
 template <bool DENSE>
 __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
-    const __half* __restrict__ qimg, int64_t nq, const __half* __restrict__ dimg, const float* __restrict__ norms,
-    int64_t nd, float inv_s2, const float* __restrict__ thr, int cap, int32_t* __restrict__ cand_idx,
-    float* __restrict__ cand_d, int32_t* __restrict__ counts, float* __restrict__ dense, int64_t ld, int nqt,
-    int64_t tiles_per_slice, int* __restrict__ status, long long wait_cycles) {
+    const __half* __restrict__ qimg, int64_t nq, const __half* __restrict__ dimg, int64_t nd, float inv_s2,
+    const float* __restrict__ thr, int cap, int32_t* __restrict__ cand_idx, float* __restrict__ cand_d,
+    int32_t* __restrict__ counts, float* __restrict__ dense, int64_t ld, int nqt, int64_t tiles_per_slice,
+    int* __restrict__ status, long long wait_cycles) {
     namespace U = tsm::umma;
     extern __shared__ __align__(1024) unsigned char sm[];
     const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
     const uint32_t bar = sbase + OFF_BAR;
-    // mbarriers: full[4] (copies landed), empty[4] (stage read by the MMAs),
-    // tfull[2] (accumulator ready), tempty[2] (accumulator read), all MMAs
-    // done, nfull[4] (a tile's norms landed), nempty[4] (norms read)
-    auto full = [&](int i) { return bar + 8 * i; };         // i < NSTAGE (6): bytes 0..47
-    auto empty = [&](int i) { return bar + 48 + 8 * i; };   // 48..95
-    auto tfull = [&](int b) { return bar + 184 + 8 * b; };
-    auto tempty = [&](int b) { return bar + 200 + 8 * b; };
-    const uint32_t donebar = bar + 104;
-    auto nfull = [&](int i) { return bar + 112 + 8 * i; };
-    auto nempty = [&](int i) { return bar + 144 + 8 * i; };
-    volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(sm + OFF_BAR + 176);
-    volatile int* tmem_busy = reinterpret_cast<volatile int*>(sm + OFF_BAR + 180);
+    auto full = [&](int i) { return bar + BAR_FULL + 8 * i; };    // copies landed
+    auto empty = [&](int i) { return bar + BAR_EMPTY + 8 * i; };  // stage read by the MMAs
+    auto tfull = [&](int b) { return bar + BAR_TFULL + 8 * b; };  // accumulator ready
+    auto tempty = [&](int b) { return bar + BAR_TEMPTY + 8 * b; };  // accumulator read
+    const uint32_t donebar = bar + BAR_DONE;  // all MMAs done
+    const uint32_t afull = bar + BAR_AFULL;   // query tile landed
+    volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(sm + OFF_BAR + TMEM_SLOT);
+    volatile int* tmem_busy = reinterpret_cast<volatile int*>(sm + OFF_BAR + TMEM_BUSY);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int qt = blockIdx.x % nqt;
     const int64_t sl = blockIdx.x / nqt;
@@ -171,14 +217,11 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
             U::mbar_init(tempty(b), EPI_WARPS);  // one arrival per epilogue warp
         }
         U::mbar_init(donebar, 1);
-        for (int i = 0; i < NNORM; ++i) {
-            U::mbar_init(nfull(i), 1);
-            U::mbar_init(nempty(i), EPI_WARPS);
-        }
+        U::mbar_init(afull, 1);
         *tmem_busy = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) U::tmem_alloc(sbase + OFF_BAR + 176, TMEM_COLS);
+    if (warp == 0) U::tmem_alloc(sbase + OFF_BAR + TMEM_SLOT, TMEM_COLS);
     U::fence_before_sync();
     __syncthreads();
     U::fence_after_sync();
@@ -187,22 +230,13 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
     if (warp == 0) {
         if (lane == 0 && ntl > 0) {  // copies
             const unsigned char* asrc = reinterpret_cast<const unsigned char*>(qimg) + (int64_t)qt * A_BYTES;
+            U::mbar_arrive_expect_tx(afull, A_BYTES);
+            for (int i = 0; i < A_BYTES / A_COPY; ++i)
+                U::bulk_load(sbase + OFF_A + i * A_COPY, asrc + i * A_COPY, A_COPY, afull);
             int64_t g = 0;  // stages issued
-            int64_t nt = 0;  // tiles whose norms were issued
             bool ok = true;
             for (int64_t t = t0; t < t1 && ok; ++t) {
                 const unsigned char* bsrc = reinterpret_cast<const unsigned char*>(dimg) + t * B_TILE_BYTES;
-                {  // the tile's squared norms into the norm ring
-                    const int slot = (int)(nt % NNORM);
-                    const uint32_t u = (uint32_t)(nt / NNORM);
-                    if (!U::mbar_wait(nempty(slot), (u & 1) ^ 1, wait_cycles)) {
-                        atomicOr(status, ERR_COPY);
-                        break;
-                    }
-                    U::mbar_arrive_expect_tx(nfull(slot), DN * 4);
-                    U::bulk_load(sbase + OFF_N + slot * (DN * 4), norms + t * DN, DN * 4, nfull(slot));
-                    ++nt;
-                }
                 for (int k = 0; k < STAGES_PER_TILE; ++k) {
                     const int slot = (int)(g % NSTAGE);
                     const uint32_t u = (uint32_t)(g / NSTAGE);
@@ -211,22 +245,22 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
                         ok = false;
                         break;
                     }
-                    const uint32_t st = sbase + OFF_S + slot * STAGE_BYTES;
-                    U::mbar_arrive_expect_tx(full(slot), STAGE_BYTES);
-                    U::bulk_load(st, asrc + k * A_STAGE_BYTES, A_STAGE_BYTES, full(slot));
-                    U::bulk_load(st + A_STAGE_BYTES, bsrc + k * B_STAGE_BYTES, B_STAGE_BYTES, full(slot));
+                    U::mbar_arrive_expect_tx(full(slot), B_STAGE_BYTES);
+                    U::bulk_load(sbase + OFF_S + slot * B_STAGE_BYTES, bsrc + k * B_STAGE_BYTES, B_STAGE_BYTES,
+                                 full(slot));
                     ++g;
                 }
             }
-            // every copy this CTA issued lands before it exits: the last use of each slot, and A
+            // every copy this CTA issued lands before it exits: the query tile and the last use of each slot
+            U::mbar_wait(afull, 0, wait_cycles);
             for (int slot = 0; slot < NSTAGE; ++slot)
                 if (slot < g) U::mbar_wait(full(slot), (uint32_t)((g - 1 - slot) / NSTAGE) & 1, wait_cycles);
-            for (int slot = 0; slot < NNORM; ++slot)
-                if (slot < nt) U::mbar_wait(nfull(slot), (uint32_t)((nt - 1 - slot) / NNORM) & 1, wait_cycles);
         }
     } else if (warp == 1) {
         if (lane == 0 && ntl > 0) {  // MMAs
-            bool ok = true;
+            bool ok = U::mbar_wait(afull, 0, wait_cycles);
+            if (!ok) atomicOr(status, ERR_MMA);
+            U::fence_after_sync();
             constexpr uint32_t idesc = U::idesc_f16_f32(QM, DN);
             int64_t g = 0;
             for (int64_t t = 0; t < ntl && ok; ++t) {
@@ -247,12 +281,12 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
                         break;
                     }
                     U::fence_after_sync();
-                    const uint32_t st = sbase + OFF_S + slot * STAGE_BYTES;
+                    const uint32_t st = sbase + OFF_S + slot * B_STAGE_BYTES;
 #pragma unroll
                     for (int kk = 0; kk < SK / 16; ++kk) {
                         const int ks = k * (SK / 16) + kk;
-                        const uint64_t ad = U::smem_desc(st + kk * 2 * (QM * 16), QM * 16, 128);
-                        const uint64_t bd = U::smem_desc(st + A_STAGE_BYTES + kk * 2 * (DN * 16), DN * 16, 128);
+                        const uint64_t ad = U::smem_desc(sbase + OFF_A + ks * 2 * (QM * 16), QM * 16, 128);
+                        const uint64_t bd = U::smem_desc(st + kk * 2 * (DN * 16), DN * 16, 128);
                         U::mma_bf16(dt, ad, bd, idesc, ks > 0 ? 1u : 0u);  // kind::f16 issue (FP16 idesc)
                     }
                     U::commit(empty(slot));
@@ -271,70 +305,92 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
     } else {  // epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. +31, columns half * 128 .. +127
         const int quarter = warp & 3;
         const int half = (warp - 2) >> 2;
+        const int et = threadIdx.x - 64;  // epilogue thread: its staging slots are et, et + 256, ...
+        uint2* stg = reinterpret_cast<uint2*>(sm + OFF_STG) + et;
         const int64_t q = (int64_t)qt * QM + 32 * quarter + lane;
         const bool qv = q < nq;
-        // padding queries get -inf: no d (>= finite or +inf) is at or below it
-        const float th = DENSE ? 0.f : (qv ? thr[q] : __int_as_float(0xff800000));
-        const float m2 = -2.f * inv_s2;
+        const float to_d = -2.f * inv_s2;  // d = to_d * acc
+        // d <= thr  <=>  acc >= -(s^2 / 2) thr; padding queries get +inf (never)
+        const float at = DENSE ? 0.f : (qv ? -0.5f * thr[q] / inv_s2 : __int_as_float(0x7f800000));
+        int staged = 0;
+        int32_t* const cnt_q = counts + (qv ? q : 0);
+        int32_t* const idx_q = cand_idx + (qv ? q : 0) * cap;
+        float* const d_q = cand_d + (qv ? q : 0) * cap;
+        auto flush = [&]() {
+            flush_staged(stg, staged, cnt_q, idx_q, d_q, cap);
+            staged = 0;
+        };
         for (int64_t t = 0; t < ntl; ++t) {
             const int b = (int)(t & 1);
             const uint32_t v = (uint32_t)(t >> 1);
-            const int ns = (int)(t % NNORM);
-            if (!U::mbar_wait(tfull(b), v & 1, wait_cycles) ||
-                !U::mbar_wait(nfull(ns), (uint32_t)(t / NNORM) & 1, wait_cycles)) {
-                atomicOr(status, ERR_EPI);
+            // warp-uniform outcome: the loads below are .sync.aligned and the flush votes over the warp
+            if (!__all_sync(0xffffffffu, U::mbar_wait(tfull(b), v & 1, wait_cycles))) {
+                if (lane == 0) atomicOr(status, ERR_EPI);
                 break;
             }
             U::fence_after_sync();
             const uint32_t ta = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(b * DN + half * (DN / 2));
-            const float4* nr = reinterpret_cast<const float4*>(sm + OFF_N + ns * (DN * 4)) + half * (DN / 8);
             const int64_t jh = (t0 + t) * DN + half * (DN / 2);
 #pragma unroll 1
             for (int cb = 0; cb < DN / 2; cb += EPI_COLS) {
-                uint32_t r0[16], r1[16], r2[16], r3[16];
-                U::ld16(ta + cb, r0);
-                U::ld16(ta + cb + 16, r1);
-                U::ld16(ta + cb + 32, r2);
-                U::ld16(ta + cb + 48, r3);
-                U::wait_ld(r0);
-                U::wait_ld(r1);
-                U::wait_ld(r2);
-                U::wait_ld(r3);
-                float d[EPI_COLS];
-#pragma unroll
-                for (int i4 = 0; i4 < EPI_COLS / 4; ++i4) {
-                    const float4 nv = nr[cb / 4 + i4];  // the same address in every lane: a broadcast
-                    const uint32_t* rr = i4 < 4 ? r0 : (i4 < 8 ? r1 : (i4 < 12 ? r2 : r3));
-                    const int o = (4 * i4) & 15;
-                    d[4 * i4 + 0] = fmaf(m2, __uint_as_float(rr[o + 0]), nv.x);
-                    d[4 * i4 + 1] = fmaf(m2, __uint_as_float(rr[o + 1]), nv.y);
-                    d[4 * i4 + 2] = fmaf(m2, __uint_as_float(rr[o + 2]), nv.z);
-                    d[4 * i4 + 3] = fmaf(m2, __uint_as_float(rr[o + 3]), nv.w);
-                }
+                uint32_t r[4][16];
+                U::ld16(ta + cb, r[0]);
+                U::ld16(ta + cb + 16, r[1]);
+                U::ld16(ta + cb + 32, r[2]);
+                U::ld16(ta + cb + 48, r[3]);
+                U::wait_ld(r[0]);
+                U::wait_ld(r[1]);
+                U::wait_ld(r[2]);
+                U::wait_ld(r[3]);
                 const int64_t jb = jh + cb;
                 if (DENSE) {
                     if (qv) {
 #pragma unroll
                         for (int i = 0; i < EPI_COLS; ++i)
-                            if (jb + i < nd) dense[q * ld + jb + i] = d[i];
+                            if (jb + i < nd) dense[q * ld + jb + i] = to_d * __uint_as_float(r[i >> 4][i & 15]);
                     }
                 } else {
-                    float mn[EPI_COLS / 2];  // tree minimum: depth 6, not a chain of 64
+                    // tree maximum (depth 6, not a chain of 64); the level of 8 is kept: group g holds
+                    // columns 2g + b + 16a (a = 0..3, b = 0..1), i.e. r[a][2g + b]
+                    float mx[EPI_COLS / 2], grp[8];
 #pragma unroll
-                    for (int i = 0; i < EPI_COLS / 2; ++i) mn[i] = fminf(d[2 * i], d[2 * i + 1]);
+                    for (int i = 0; i < EPI_COLS / 2; ++i)
+                        mx[i] = fmaxf(__uint_as_float(r[(2 * i) >> 4][(2 * i) & 15]),
+                                      __uint_as_float(r[(2 * i + 1) >> 4][(2 * i + 1) & 15]));
 #pragma unroll
-                    for (int w2 = EPI_COLS / 4; w2 >= 1; w2 >>= 1)
+                    for (int w2 = EPI_COLS / 4; w2 >= 1; w2 >>= 1) {
 #pragma unroll
-                        for (int i = 0; i < w2; ++i) mn[i] = fminf(mn[i], mn[i + w2]);
-                    if (mn[0] <= th) {  // rare: at least one of the 64 survives (unrolled: d stays in registers)
+                        for (int i = 0; i < w2; ++i) mx[i] = fmaxf(mx[i], mx[i + w2]);
+                        if (w2 == 8) {
 #pragma unroll
-                        for (int i = 0; i < EPI_COLS; ++i) {
-                            const int64_t j = jb + i;
-                            if (d[i] <= th && j < nd) {
-                                const int pos = atomicAdd(counts + q, 1);
-                                if (pos < cap) {
-                                    cand_idx[q * cap + pos] = (int32_t)j;
-                                    cand_d[q * cap + pos] = d[i];
+                            for (int i = 0; i < 8; ++i) grp[i] = mx[i];
+                        }
+                    }
+                    if (mx[0] >= at) {  // rare: visit the groups that hold a survivor (compact code)
+                        uint32_t gm = 0;
+#pragma unroll
+                        for (int g = 0; g < 8; ++g) gm |= (grp[g] >= at ? 1u : 0u) << g;
+                        const int64_t lim = nd - jb;
+                        while (gm) {
+                            const int g = __ffs(gm) - 1;
+                            gm &= gm - 1;
+                            float vv[8];
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) vv[e] = 0.f;
+#pragma unroll
+                            for (int k = 0; k < 8; ++k)
+                                if (g == k) {
+#pragma unroll
+                                    for (int e = 0; e < 8; ++e) vv[e] = __uint_as_float(r[e >> 1][2 * k + (e & 1)]);
+                                }
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) {
+                                const int col = 2 * g + (e & 1) + 16 * (e >> 1);
+                                if (vv[e] >= at && col < lim) {
+                                    if (staged == SLOTS) flush();
+                                    stg[staged * EPI_THREADS] =
+                                        make_uint2((uint32_t)(jb + col), __float_as_uint(to_d * vv[e]));
+                                    ++staged;
                                 }
                             }
                         }
@@ -343,11 +399,10 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
             }
             U::fence_before_sync();
             __syncwarp();
-            if (lane == 0) {
-                U::mbar_arrive(tempty(b));
-                U::mbar_arrive(nempty(ns));
-            }
+            if (lane == 0) U::mbar_arrive(tempty(b));
+            if (!DENSE && __any_sync(0xffffffffu, staged == SLOTS) && staged > 0) flush();
         }
+        if (!DENSE && staged > 0) flush();
     }
     U::fence_before_sync();
     __syncthreads();
@@ -377,11 +432,6 @@ extern "C" {
 
 int32_t tsm_scan_dim(void) { return tsm::scan::D; }
 
-int64_t tsm_scan_norms_count(int64_t n_rows) {
-    if (n_rows < 0) return -1;
-    return (n_rows + tsm::scan::DN - 1) / tsm::scan::DN * tsm::scan::DN;
-}
-
 int64_t tsm_scan_image_bytes(int64_t n_rows, int32_t is_db) {
     if (n_rows < 0) return -1;
     const int64_t R = is_db ? tsm::scan::DN : tsm::scan::QM;
@@ -393,15 +443,13 @@ int tsm_scan_prepare(const float* emb, int64_t n, int64_t ld, float scale, int32
     using namespace tsm::scan;
     if (n < 0 || ld < D || !(scale > 0.f)) return scan_fail(TSM_EINVAL, "tsm_scan_prepare: bad size or scale");
     if (n == 0) return TSM_OK;
-    if (!emb || !img || (is_db && !norms)) return scan_fail(TSM_EINVAL, "tsm_scan_prepare: null pointer");
+    if (!emb || !img) return scan_fail(TSM_EINVAL, "tsm_scan_prepare: null pointer");
     if (reinterpret_cast<uintptr_t>(img) % 16) return scan_fail(TSM_EINVAL, "tsm_scan_prepare: image not 16-byte aligned");
     const int64_t R = is_db ? DN : QM;
     const int64_t tiles = (n + R - 1) / R;
     const int64_t threads = tiles * KCH * R;
     const unsigned grid = (unsigned)((threads + 255) / 256);
     cudaStream_t s = (cudaStream_t)stream;
-    if (is_db && reinterpret_cast<uintptr_t>(norms) % 16)
-        return scan_fail(TSM_EINVAL, "tsm_scan_prepare: norms not 16-byte aligned");
     if (is_db)
         scan_prepare<true><<<grid, 256, 0, s>>>(emb, n, ld, scale, tiles, static_cast<__half*>(img), norms);
     else
@@ -409,24 +457,24 @@ int tsm_scan_prepare(const float* emb, int64_t n, int64_t ld, float scale, int32
     return scan_cuda(cudaGetLastError(), "tsm_scan_prepare launch");
 }
 
-int tsm_scan_opts(const void* q_img, int64_t nq, const void* db_img, const float* db_norms, int64_t nd, float scale,
-                  const float* thresholds, int32_t cap, int32_t* cand_idx, float* cand_d, int32_t* counts,
-                  float* dense, int64_t ld_dense, int32_t* status, int64_t wait_cycles, void* stream) {
+int tsm_scan_opts(const void* q_img, int64_t nq, const void* db_img, int64_t nd, float scale, const float* thresholds,
+                  int32_t cap, int32_t* cand_idx, float* cand_d, int32_t* counts, float* dense, int64_t ld_dense,
+                  int32_t* status, int64_t wait_cycles, void* stream) {
     using namespace tsm::scan;
     if (nq < 0 || nd < 0) return scan_fail(TSM_EINVAL, "tsm_scan: negative size");
     if (nq == 0 || nd == 0) return TSM_OK;
-    if (!q_img || !db_img || !db_norms || !status) return scan_fail(TSM_EINVAL, "tsm_scan: null pointer");
+    if (!q_img || !db_img || !status) return scan_fail(TSM_EINVAL, "tsm_scan: null pointer");
     if (nd > 0x7fffffffLL) return scan_fail(TSM_EINVAL, "tsm_scan: database index exceeds int32");
     if (wait_cycles < 1) return scan_fail(TSM_EINVAL, "tsm_scan: bad wait limit");
+    if (!(scale > 0.f)) return scan_fail(TSM_EINVAL, "tsm_scan: bad scale");
     const bool dense_mode = dense != nullptr;
     if (dense_mode == (thresholds != nullptr))
         return scan_fail(TSM_EINVAL, "tsm_scan: give either thresholds (candidate lists) or a dense output");
     if (dense_mode && ld_dense < nd) return scan_fail(TSM_EINVAL, "tsm_scan: ld_dense < nd");
     if (!dense_mode && (cap < 1 || !cand_idx || !cand_d || !counts))
         return scan_fail(TSM_EINVAL, "tsm_scan: candidate lists need cap >= 1 and their three arrays");
-    if ((reinterpret_cast<uintptr_t>(q_img) | reinterpret_cast<uintptr_t>(db_img) |
-         reinterpret_cast<uintptr_t>(db_norms)) % 16)
-        return scan_fail(TSM_EINVAL, "tsm_scan: images or norms not 16-byte aligned");
+    if ((reinterpret_cast<uintptr_t>(q_img) | reinterpret_cast<uintptr_t>(db_img)) % 16)
+        return scan_fail(TSM_EINVAL, "tsm_scan: images not 16-byte aligned");
     const float inv_s2 = 1.f / (scale * scale);
     int dev = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -449,17 +497,17 @@ int tsm_scan_opts(const void* q_img, int64_t nq, const void* db_img, const float
     const __half* qi = static_cast<const __half*>(q_img);
     const __half* di = static_cast<const __half*>(db_img);
     long long wc = (long long)wait_cycles;
-    void* args[] = {&qi, &nq, &di, &db_norms, &nd, (void*)&inv_s2, &thresholds, &cap, &cand_idx, &cand_d, &counts,
-                    &dense, &ld_dense, &inqt, (void*)&per, &status, &wc};
+    void* args[] = {&qi, &nq, &di, &nd, (void*)&inv_s2, &thresholds, &cap, &cand_idx, &cand_d, &counts, &dense,
+                    &ld_dense, &inqt, (void*)&per, &status, &wc};
     e = cudaLaunchKernel(fn, dim3((unsigned)(nqt * slices)), dim3(THREADS), args, (size_t)SMEM, (cudaStream_t)stream);
     return scan_cuda(e, "tsm_scan launch");
 }
 
-int tsm_scan(const void* q_img, int64_t nq, const void* db_img, const float* db_norms, int64_t nd, float scale,
-             const float* thresholds, int32_t cap, int32_t* cand_idx, float* cand_d, int32_t* counts, float* dense,
-             int64_t ld_dense, int32_t* status, void* stream) {
-    return tsm_scan_opts(q_img, nq, db_img, db_norms, nd, scale, thresholds, cap, cand_idx, cand_d, counts, dense,
-                         ld_dense, status, tsm::scan::WAIT_CYCLES, stream);
+int tsm_scan(const void* q_img, int64_t nq, const void* db_img, int64_t nd, float scale, const float* thresholds,
+             int32_t cap, int32_t* cand_idx, float* cand_d, int32_t* counts, float* dense, int64_t ld_dense,
+             int32_t* status, void* stream) {
+    return tsm_scan_opts(q_img, nq, db_img, nd, scale, thresholds, cap, cand_idx, cand_d, counts, dense, ld_dense,
+                         status, tsm::scan::WAIT_CYCLES, stream);
 }
 
 }  // extern "C"

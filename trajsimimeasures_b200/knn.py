@@ -168,7 +168,7 @@ class SurrogateIndex:
     LADDER = (100, 200, 300, 500, 700, 1000, 1500, 2000, 3000, 5000, 7000, 10000, 20000, 50000)
     BRANCH_WEIGHTS = (1.0, 0.5, 0.3, 0.1)
     SAMPLE = 16384
-    FP16_TOP = 16384.0  # largest scaled magnitude (FP16 holds 65504)
+    SCALED_TOP = 1024.0  # largest scaled magnitude of an operand value (tsm_scan_prepare)
 
     def __init__(self, encoder, D: TrajSet, batch=None, branch_weight=1.0):
         self.enc = encoder
@@ -194,24 +194,22 @@ class SurrogateIndex:
         self.wt[:self.width - 32] = self.beta
         X = self.E * self.wt
         top = float(X.abs().max()) if X.numel() else 1.0
-        self.scale = float(2.0 ** math.floor(math.log2(self.FP16_TOP / max(top, 1e-30))))
-        self.img, self.norms = self._image(X, True)
-        self.s_img, self.s_norms = self._image(X[self.sample].contiguous(), True)
+        self.scale = float(2.0 ** math.floor(math.log2(self.SCALED_TOP / max(top, 1e-30))))
+        self.img = self._image(X, True)
+        self.s_img = self._image(X[self.sample].contiguous(), True)
 
     def _image(self, X, is_db):
         lib = _lib.load()
         n = X.shape[0]
         img = torch.empty(max(lib.tsm_scan_image_bytes(n, int(is_db)), 16), dtype=torch.uint8, device=X.device)
-        norms = torch.empty(max(lib.tsm_scan_norms_count(n), 1), dtype=torch.float32, device=X.device) if is_db \
-            else None
-        rc = lib.tsm_scan_prepare(_ptr(X), n, X.stride(0), self.scale, int(is_db), _ptr(img), _ptr(norms),
+        rc = lib.tsm_scan_prepare(_ptr(X), n, X.stride(0), self.scale, int(is_db), _ptr(img), None,
                                   _stream_ptr(None))
         _lib.check(rc, "tsm_scan_prepare")
-        return img, norms
+        return img
 
     def _query_image(self, e):
         X = ((e - self.mu) * self.wt).contiguous()
-        return self._image(X, False)[0]
+        return self._image(X, False)
 
     @property
     def emb(self) -> torch.Tensor:
@@ -219,10 +217,10 @@ class SurrogateIndex:
         return self.E + self.mu
 
     # -- scans ------------------------------------------------------------------
-    def _dense(self, qimg, nq, img, norms, nd):
+    def _dense(self, qimg, nq, img, nd):
         out = torch.empty((nq, nd), dtype=torch.float32, device=self.E.device)
-        rc = _lib.load().tsm_scan(_ptr(qimg), nq, _ptr(img), _ptr(norms), nd, self.scale, None, 0, None, None, None,
-                                  _ptr(out), nd, _ptr(self.status), _stream_ptr(None))
+        rc = _lib.load().tsm_scan(_ptr(qimg), nq, _ptr(img), nd, self.scale, None, 0, None, None, None, _ptr(out), nd,
+                                  _ptr(self.status), _stream_ptr(None))
         _lib.check(rc, "tsm_scan")
         return out
 
@@ -230,7 +228,7 @@ class SurrogateIndex:
         """Embedding-space distances (less |e_q - mu|^2 in the weighted
         space) of queries e [b, width] to every database trajectory
         ([b, n] float32, dense)."""
-        return self._dense(self._query_image(e), e.shape[0], self.img, self.norms, self.E.shape[0])
+        return self._dense(self._query_image(e), e.shape[0], self.img, self.E.shape[0])
 
     def _check_status(self):
         st = int(self.status.item())
@@ -255,23 +253,22 @@ class SurrogateIndex:
             b = e.shape[0]
             qimg = self._query_image(e)
             if ks >= S or cap >= n:  # the list would hold most of the database: dense
-                out[q0:q0 + b] = select_rows(self._dense(qimg, b, self.img, self.norms, n), c).long()
+                out[q0:q0 + b] = select_rows(self._dense(qimg, b, self.img, n), c).long()
                 continue
-            ds = self._dense(qimg, b, self.s_img, self.s_norms, S)
+            ds = self._dense(qimg, b, self.s_img, S)
             thr = torch.topk(ds, ks, dim=1, largest=False, sorted=True).values[:, -1].contiguous()
             idx = torch.empty((b, cap), dtype=torch.int32, device=Q.device)
             dd = torch.full((b, cap), float("inf"), dtype=torch.float32, device=Q.device)
             cnt = torch.zeros(b, dtype=torch.int32, device=Q.device)
-            rc = lib.tsm_scan(_ptr(qimg), b, _ptr(self.img), _ptr(self.norms), n, self.scale, _ptr(thr), cap,
-                              _ptr(idx), _ptr(dd), _ptr(cnt), None, 0, _ptr(self.status), _stream_ptr(None))
+            rc = lib.tsm_scan(_ptr(qimg), b, _ptr(self.img), n, self.scale, _ptr(thr), cap, _ptr(idx), _ptr(dd),
+                              _ptr(cnt), None, 0, _ptr(self.status), _stream_ptr(None))
             _lib.check(rc, "tsm_scan")
             pos = select_rows(dd, c).long()
             res = torch.gather(idx, 1, pos).long()
             bad = torch.nonzero((cnt < c) | (cnt > cap)).flatten()
             if bad.numel():  # threshold too tight or list overflowed: those queries densely
                 eb = e[bad]
-                res[bad] = select_rows(self._dense(self._query_image(eb), eb.shape[0], self.img, self.norms, n),
-                                       c).long()
+                res[bad] = select_rows(self._dense(self._query_image(eb), eb.shape[0], self.img, n), c).long()
             out[q0:q0 + b] = res
         self._check_status()
         return out
