@@ -844,6 +844,8 @@ def run_knn(args, enc=None, emit=True):
         out["recall_at_10_trained"] = {str(cc): recall_at_k(index.query(Q, 10, c=cc)[1], ex_i) for cc in counts}
         out["recall_at_10_untrained"] = {str(cc): recall_at_k(raw.query(Q, 10, c=cc)[1], ex_i) for cc in counts}
         _, ex50 = knn_exhaustive(Q, Dset, 50)
+        out["skip_weights"] = {"trained": [round(float(x), 4) for x in enc.params[-16:].tolist()],
+                               "untrained": [round(float(x), 4) for x in raw.enc.params[-16:].tolist()]}
         out["hit_ratio"] = hit_ratios(Q, Dset, enc, ex50)
         out["hit_ratio_untrained"] = hit_ratios(Q, Dset, raw.enc, ex50)
     out["host_generate_s"] = gen_s

@@ -289,15 +289,16 @@ int tsm_scan_opts(const void* q_img, int64_t nq, const void* db_img, int64_t nd,
  * their maximum with an MSE loss (nn/MLP_trajsimi_train.py:74-84,197-200); this
  * encoder (conv 2->64 k=5 + GRU 64->128 + linear 128->128, BF16 weights, FP32
  * accumulation, plus a geometric skip: the trajectory's 16 points at indices
- * round(k (n-1) / 15), normalised, times one learned scale, appended as 32
- * more embedding values) is trained the same way on DTW labels from
+ * round(k (n-1) / 15), normalised, each times its learned weight exp(u_k),
+ * appended as 32 more embedding values) is trained the same way on DTW labels from
  * tsm_pairs and serves as a kNN filter.  Embeddings are 160 floats.
  *   params  float32 [tsm_enc_param_count()] master weights (layout: conv W
  *           [64][2][5], b [64]; W_ih [384][64], b_ih [384]; W_hh [384][128],
- *           b_hh [384]; W_o [128][128], b_o [128]; skip scale [1]; gate order
- *           r, z, n)
+ *           b_hh [384]; W_o [128][128], b_o [128]; skip log-weights u [16];
+ *           gate order r, z, n)
  *   pts/off/len  a packed batch of B trajectories, T = max length in it
- *   nrm     HOST float[4] = (mean_x, mean_y, 1/std_x, 1/std_y) input scaling
+ *   nrm     HOST float[4] = (mean_x, mean_y, 1/s_x, 1/s_y) input scaling (the
+ *           Python encoder uses one scale for both axes, s_x = s_y)
  *   workspace  device memory of tsm_enc_workspace_bytes(B, T, P) bytes
  */
 int tsm_enc_param_count(void);

@@ -5,8 +5,9 @@ PyTorch float64 ops on the CPU so that autograd gives the gradients the
 kernels must reproduce:
   conv   relu(conv1d(x, W1, b1, padding=2))        64 channels, k=5
   GRU    r, z, n gates (order r, z, n), hidden 128, one step per point
-  head   e = [Wo h_last + bo | sc * r], r = the 16 points at indices
-         round(k (n - 1) / 15) (halves up), normalised, 0 for an empty trajectory
+  head   e = [Wo h_last + bo | exp(u_k) * r_k], r_k = point round(k (n - 1) / 15)
+         (halves up, k < 16), normalised, 0 for an empty trajectory; u_k are the
+         stored skip log-weights
   loss   mean_p (||e_a - e_b||_2 - y_p)^2
 Conv and GRU weights are taken at their BF16-rounded values (as the kernels
 use them); the head is FP32.  Gradients are with respect to those values.
@@ -17,9 +18,9 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-SIZES = [("conv_w", (64, 2, 5)), ("conv_b", (64,)), ("w_ih", (384, 64)), ("b_ih", (384,)),
-         ("w_hh", (384, 128)), ("b_hh", (384,)), ("w_o", (128, 128)), ("b_o", (128,)), ("skip_scale", (1,))]
 NS = 16
+SIZES = [("conv_w", (64, 2, 5)), ("conv_b", (64,)), ("w_ih", (384, 64)), ("b_ih", (384,)),
+         ("w_hh", (384, 128)), ("b_hh", (384,)), ("w_o", (128, 128)), ("b_o", (128,)), ("skip_scale", (NS,))]
 BF16 = {"conv_w", "w_ih", "w_hh"}
 
 
@@ -65,10 +66,10 @@ def embed(W, trajs, nrm, bf16_operands=False):
                 h = (1 - z) * nn_ + z * h
         if n > 0:
             idx = [(2 * k * (n - 1) + NS - 1) // (2 * (NS - 1)) for k in range(NS)]
-            r = x[idx].reshape(-1)
+            r = (torch.exp(W["skip_scale"])[:, None] * x[idx]).reshape(-1)
         else:
-            r = torch.zeros(2 * NS, dtype=torch.float64)
-        embs.append(torch.cat([W["w_o"] @ h + W["b_o"], W["skip_scale"] * r]))
+            r = W["skip_scale"].repeat_interleave(2) * 0.0
+        embs.append(torch.cat([W["w_o"] @ h + W["b_o"], r]))
     return torch.stack(embs)
 
 

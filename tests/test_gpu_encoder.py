@@ -24,6 +24,8 @@ def test_encoder_gradients_match_fp64_autograd():
     enc = Encoder.init(s, seed=5)
     # larger weights than the init so that the gates leave their linear range
     enc.params.mul_(3.0)
+    # distinct weights per resampled point of the skip (stored as logarithms)
+    enc.params[-16:] = torch.log(torch.linspace(0.1, 0.4, 16, device=enc.params.device))
     ia, ib, y = np.array([0, 1, 2, 4, 5]), np.array([1, 2, 4, 5, 3]), np.array([0.1, 0.5, 0.2, 0.9, 0.3])
     w = np.array([1.0, 4.0, 25.0, 1.2, 11.1], dtype=np.float32)  # relative-error weights 1 / y^2
     loss, grad, pred = enc.loss_grad(s, np.arange(6), ia, ib, y, w)

@@ -4,9 +4,10 @@
 //   conv   a_t = relu(b1 + sum_{k<5, i<2} W1[c][i][k] x_{t+k-2,i})   64 channels, zero padding
 //   GRU    r = s(Wir a + bir + Whr h + bhr),  z = s(Wiz a + biz + Whz h + bhz),
 //          n = tanh(Win a + bin + r * (Whn h + bhn)),  h' = (1-z) n + z h      hidden 128
-//   head   e = [Wo h_n + bo | sc * r]                                           160-d embedding
-//          r = the 16 points at indices round(k (n - 1) / 15), normalised (32 values): a
-//          geometric skip around the recurrent branch, with one learned scale sc
+//   head   e = [Wo h_n + bo | sc_k * r_k]                                       160-d embedding
+//          r_k = point round(k (n - 1) / 15) of the trajectory, k < 16, normalised (32 values):
+//          a geometric skip around the recurrent branch, with a learned weight sc_k = exp(u_k)
+//          per point (u_k stored: Adam then moves the weights by relative steps)
 //   pair   d(a, b) = ||e_a - e_b||_2, trained with MSE against DTW / max DTW.
 // Conv and GRU weights are used as BF16 values (rounded from FP32 master
 // weights before each forward), all accumulation is FP32; the head and the
@@ -27,9 +28,9 @@
 //   enc_round_bf16    FP32 master -> BF16 weights
 //   enc_conv_fwd      conv + relu -> A [B][T][64]
 //   enc_gru_fwd       persistent GRU over T steps -> H [B][T+1][128] and gate caches
-//   enc_head_fwd      e = [Wo h_last + bo | sc r]
+//   enc_head_fwd      e = [Wo h_last + bo | sc_k r_k]
 //   enc_pair_loss     distances, MSE loss, dL/de (atomic)
-//   enc_head_bwd      dWo, dbo, dh_last; enc_skip_bwd: d sc
+//   enc_head_bwd      dWo, dbo, dh_last; enc_skip_bwd: d sc_k
 //   enc_gru_bwd       BPTT: gate gradients G [B][T][384] (input side), dA [B][T][64]
 //   enc_gemm_tn       split-K reduction dW[m][n] += sum_k A[k][m] B[k][n]  (weight gradients)
 //   enc_conv_bwd      dW1, db1
@@ -55,7 +56,8 @@ constexpr int G3 = 384;   // 3 gates
 constexpr int EO = 128;   // learned head outputs
 constexpr int NS = 16;    // resampled points of the geometric skip
 constexpr int SK = 2 * NS;  // skip features (x, y of each resampled point)
-constexpr int ED = EO + SK; // embedding: [head outputs | skip scale * resampled points]
+constexpr int ED = EO + SK; // embedding: [head outputs | skip weights * resampled points]
+static_assert(SK == 32, "enc_skip_bwd maps one skip value per lane");
 constexpr int S = 16;     // trajectories per GRU CTA
 constexpr int GRU_THREADS = 384;
 
@@ -68,8 +70,8 @@ constexpr int OFF_WHH = OFF_BIH + G3;        // [384][128]
 constexpr int OFF_BHH = OFF_WHH + G3 * HD;   // [384]
 constexpr int OFF_WO = OFF_BHH + G3;         // [128][128]
 constexpr int OFF_BO = OFF_WO + EO * HD;     // [128]
-constexpr int OFF_SC = OFF_BO + EO;          // [1] scale of the resampled-point skip
-constexpr int N_PARAMS = OFF_SC + 1;
+constexpr int OFF_SC = OFF_BO + EO;          // [16] u_k: log-weights of the resampled points of the skip
+constexpr int N_PARAMS = OFF_SC + NS;
 
 __device__ __forceinline__ float sigm(float x) { return 1.f / (1.f + expf(-x)); }
 
@@ -221,10 +223,10 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
 __device__ __forceinline__ int skip_index(int k, int n) { return (2 * k * (n - 1) + (NS - 1)) / (2 * (NS - 1)); }
 
 // E[b][o] = bo[o] + sum_k Wo[o][k] hl[b][k] (bias first, k ascending) for
-// o < EO; E[b][EO + 2 k + i] = sc * coordinate i of resampled point k (the
+// o < EO; E[b][EO + 2 k + i] = sc_k * coordinate i of resampled point k (the
 // normalised input at skip_index(k, n); 0 for an empty trajectory), the
 // geometric skip, written unscaled to X[b][2 k + i] too when X is given (the
-// training forward keeps it for the gradient of sc).  One thread per head
+// training forward keeps it for the gradients of sc_k).  One thread per head
 // output o, HEAD_B trajectories per CTA, their hidden states staged in
 // shared memory; each W_o row is read once per CTA.
 constexpr int HEAD_B = 32;
@@ -235,14 +237,13 @@ __global__ void __launch_bounds__(EO) enc_head_fwd(const float* __restrict__ hl,
     __shared__ __align__(16) float hs[HEAD_B][HD];
     const int o = threadIdx.x;
     const int64_t b0 = (int64_t)blockIdx.x * HEAD_B;
-    const float sc = p[OFF_SC];
     for (int e = o; e < HEAD_B * SK; e += EO) {
         const int64_t b = b0 + e / SK;
         const int q = e % SK;
         if (b < B) {
             const int n = len[b];
             const float x = n > 0 ? xin(pts, off[b], n, skip_index(q >> 1, n), q & 1, nrm) : 0.f;
-            E[b * ED + EO + q] = sc * x;
+            E[b * ED + EO + q] = expf(p[OFF_SC + (q >> 1)]) * x;
             if (X) X[b * SK + q] = x;
         }
     }
@@ -332,16 +333,19 @@ __global__ void enc_head_bwd_h(const float* __restrict__ dE, int B, const float*
     dhl[gid] = acc;
 }
 
-// d sc += sum_b sum_q dE[b][EO + q] X[b][q] (the skip scale's gradient).
+// d u_k += sc_k sum_b sum_i dE[b][EO + 2k + i] X[b][2k + i] (the gradients of
+// the skip's log-weights, sc_k = exp(u_k)).  Lane q of every warp takes skip value q of the warp's
+// trajectories (blockDim a multiple of 32 = SK); lanes 2k and 2k + 1 are summed
+// before one atomic per point and warp.
 __global__ void enc_skip_bwd(const float* __restrict__ dE, const float* __restrict__ X, int B,
-                             float* __restrict__ grad) {
+                             const float* __restrict__ p, float* __restrict__ grad) {
+    const int q = threadIdx.x & (SK - 1);
+    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / SK;
+    const int64_t nw = (int64_t)gridDim.x * blockDim.x / SK;
     float acc = 0.f;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)B * SK;
-         e += (int64_t)gridDim.x * blockDim.x)
-        acc = fmaf(dE[(e / SK) * ED + EO + e % SK], X[e], acc);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(grad + OFF_SC, acc);
+    for (int64_t b = wid; b < B; b += nw) acc = fmaf(dE[b * ED + EO + q], X[b * SK + q], acc);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    if ((q & 1) == 0) atomicAdd(grad + OFF_SC + (q >> 1), expf(p[OFF_SC + (q >> 1)]) * acc);
 }
 
 // BPTT.  CTA = S trajectories, 384 threads.  Shared memory: Whh [384][128]
@@ -954,7 +958,7 @@ int enc_backward(const float* params, const float* pts, const int64_t* off, cons
     const float4 n4 = make_float4(nrm[0], nrm[1], nrm[2], nrm[3]);
     enc_head_bwd_w<<<EO, HD, 0, s>>>(w.dE, w.hl, B, grad);
     enc_skip_bwd<<<(unsigned)(((int64_t)B * SK + 255) / 256 < 256 ? ((int64_t)B * SK + 255) / 256 : 256), 256, 0, s>>>(
-        w.dE, w.X, B, grad);
+        w.dE, w.X, B, params, grad);
     enc_head_bwd_h<<<(unsigned)(((int64_t)B * HD + 255) / 256), 256, 0, s>>>(w.dE, B, params, w.dhl);
     int rc = enc_check(cudaFuncSetAttribute(enc_gru_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, kGruBwdSmem),
                        "cudaFuncSetAttribute(enc_gru_bwd)");

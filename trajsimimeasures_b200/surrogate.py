@@ -27,10 +27,13 @@ from .engine import TrajSet, _ptr, _stream_ptr, pairs_in_set
 EMB = 160  # 128 head outputs + the geometric skip (16 resampled points x 2)
 # (fan_in, count) of the parameter blocks in layout order; PyTorch-style
 # uniform(-1/sqrt(k), 1/sqrt(k)) init with k = fan_in (conv: 2*5, GRU: 128,
-# head: 128); the skip scale starts at 1/sqrt(32) (fan-in of the 32 skip values)
+# head: 128); the 16 skip weights (one per resampled point, stored as their
+# logarithms) start at 1/sqrt(32) (fan-in of the 32 skip values) before the
+# data-dependent balance
 _BLOCKS = [("conv_w", 10, 64 * 2 * 5), ("conv_b", 10, 64), ("w_ih", 128, 384 * 64), ("b_ih", 128, 384),
            ("w_hh", 128, 384 * 128), ("b_hh", 128, 384), ("w_o", 128, 128 * 128), ("b_o", 128, 128),
-           ("skip_scale", 32, 1)]
+           ("skip_scale", 32, 16)]
+NSKIP = 16  # resampled points of the geometric skip (one learned weight each)
 
 
 def spearman(a, b) -> float:
@@ -52,7 +55,7 @@ def spearman(a, b) -> float:
 @dataclass
 class Encoder:
     params: torch.Tensor                  # float32 [n_params] master weights (device)
-    nrm: np.ndarray                       # (mean_x, mean_y, 1/std_x, 1/std_y)
+    nrm: np.ndarray                       # (mean_x, mean_y, 1/s, 1/s), s: RMS of the axes' std
     m: torch.Tensor = None
     v: torch.Tensor = None
     step: int = 0
@@ -71,20 +74,22 @@ class Encoder:
         dev = device or pool.device
         g = np.random.Generator(np.random.PCG64(seed))
         chunks = [g.uniform(-1 / math.sqrt(k), 1 / math.sqrt(k), n).astype(np.float32) for _, k, n in _BLOCKS]
-        chunks[-1][:] = 1 / math.sqrt(32)
+        chunks[-1][:] = math.log(1 / math.sqrt(32))
         p = np.concatenate(chunks)
         assert p.size == cls.n_params()
         pts = pool.pts.double()
         mean = pts.mean(0).cpu().numpy()
-        std = pts.std(0).cpu().numpy()
-        nrm = np.array([mean[0], mean[1], 1.0 / max(std[0], 1e-12), 1.0 / max(std[1], 1e-12)], dtype=np.float32)
+        # one scale for both axes (the RMS of their standard deviations): the
+        # measures are isotropic, and so must the normalised coordinates be
+        sd = float(np.sqrt((pts.var(0).cpu().numpy()).mean()))
+        nrm = np.array([mean[0], mean[1], 1.0 / max(sd, 1e-12), 1.0 / max(sd, 1e-12)], dtype=np.float32)
         t = torch.from_numpy(p).to(dev)
         enc = cls(t, nrm, torch.zeros_like(t), torch.zeros_like(t))
         enc._balance_skip(pool, seed)
         return enc
 
     def _balance_skip(self, pool: TrajSet, seed=0, n=4096):
-        """Data-dependent initial skip scale: the embedding's two paths (the
+        """Data-dependent initial skip weights (all 16 equal): the embedding's two paths (the
         recurrent branch's 128 outputs and the 32 resampled-point values)
         contribute equal mean squared distances over random pairs of the pool,
         the way weight-normalised networks set their scales from data at
@@ -92,13 +97,13 @@ class Encoder:
         decides how much of each path the distances use."""
         g = np.random.Generator(np.random.PCG64(seed + 1))
         idx = g.choice(pool.n, size=min(n, pool.n), replace=False)
-        self.params[-1] = 1.0
+        self.params[-NSKIP:] = 0.0  # weight 1
         e = self.embed(pool, idx).double()
         a, b = torch.from_numpy(g.permutation(len(idx))).to(e.device), torch.from_numpy(g.permutation(len(idx))).to(e.device)
         d = e[a] - e[b]
         fb = float((d[:, :EMB - 32] ** 2).sum(1).mean())
         fs = float((d[:, EMB - 32:] ** 2).sum(1).mean())
-        self.params[-1] = math.sqrt(fb / fs) if fs > 0 and fb > 0 else 1.0 / math.sqrt(32)
+        self.params[-NSKIP:] = 0.5 * math.log(fb / fs) if fs > 0 and fb > 0 else math.log(1.0 / math.sqrt(32))
 
     # -- device buffers ---------------------------------------------------------
     def _workspace(self, B, T, P):
