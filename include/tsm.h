@@ -326,6 +326,14 @@ int tsm_enc_embed(const float* params, const float* pts, const int64_t* off, con
  * context should then be reset), writes NaN for that CTA's trajectories and
  * makes this call return TSM_ETIMEOUT with a message. */
 int tsm_enc_embed_status(const void* workspace, int32_t* status, void* stream);
+/* Status of the training calls (tsm_enc_loss_grad*) made with this
+ * workspace since the last check: synchronises the stream, reads the
+ * workspace's first word into *status and clears it.  The word holds bits
+ * OR-ed in by the tensor-core weight-gradient kernel when one of its bounded
+ * waits ran out (16 copy, 32 MMA, 64 completion, 128 tensor memory left
+ * allocated); the gradients are then incomplete.  Zero the word once when the
+ * workspace is allocated.  Returns TSM_ETIMEOUT when it was nonzero. */
+int tsm_enc_train_status(void* workspace, int32_t* status, void* stream);
 /* tsm_enc_embed with its wait limit (SM clocks, >= 1) and a failure-path test
  * hook: stall_step >= 0 announces that step's a_t copy on its mbarrier but
  * never issues it, so that every CTA's wait for it runs out with no MMA in

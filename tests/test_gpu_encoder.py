@@ -44,6 +44,42 @@ def test_encoder_gradients_match_fp64_autograd():
         o += n
 
 
+def test_weight_gradients_long_batch_match_fp64_autograd():
+    """The GRU weight gradients are reductions over every valid step of the
+    batch, formed on the tensor cores from BF16 hi/lo operand parts (about
+    2^-16 relative per product, FP32 accumulation).  24 trajectories of 20 to
+    160 points: about 2,000 valid steps in a padded 24 x 160 block, so the K
+    range spans several CTAs and stage boundaries fall inside trajectories."""
+    from oracle import encoder_ref as R
+    from trajsimimeasures_b200 import datagen as D
+    from trajsimimeasures_b200.surrogate import Encoder
+    rng = np.random.default_rng(8)
+    L = rng.integers(20, 161, 24)
+    pts, off, lens = D._walks(rng, L, D.STEP_SIGMA)
+    trajs = D.unpack(pts, off, lens)
+    s = _set(trajs)
+    enc = Encoder.init(s, seed=9)
+    enc.params.mul_(2.0)
+    ia, ib = np.arange(12), np.arange(12, 24)
+    y = rng.uniform(0.05, 0.5, 12)
+    loss, grad, _ = enc.loss_grad(s, np.arange(24), ia, ib, y)
+    enc.check_training()
+    _, g_ref, _ = R.loss_grad(enc.params.cpu().numpy(), trajs, enc.nrm, ia, ib, y)
+    g = grad.cpu().numpy().astype(np.float64)
+    o, blocks = 0, {}
+    for name, shape in R.SIZES:
+        n = int(np.prod(shape))
+        blocks[name] = (o, o + n)
+        o += n
+    for name in ("w_ih", "w_hh"):  # the tensor-core reductions, each against its own largest gradient
+        a, b = blocks[name]
+        scale = np.abs(g_ref[a:b]).max()
+        assert scale > 0
+        assert np.abs(g[a:b] - g_ref[a:b]).max() <= 1e-4 * scale, (name, np.abs(g[a:b] - g_ref[a:b]).max() / scale)
+    scale = np.abs(g_ref).max()
+    assert np.abs(g - g_ref).max() <= 1e-4 * scale
+
+
 def test_encoder_forward_long_batch():
     from oracle import encoder_ref as R
     from trajsimimeasures_b200 import datagen as D

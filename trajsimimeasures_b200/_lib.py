@@ -24,7 +24,8 @@ EXPORTS = ("tsm_version", "tsm_last_error", "tsm_max_supported_len", "tsm_matrix
            "tsm_sched_workspace_bytes", "tsm_pairs_sched", "tsm_topk_rows", "tsm_pairs_sched_noalloc",
            "tsm_enc_param_count", "tsm_enc_workspace_bytes", "tsm_enc_forward", "tsm_enc_loss_grad", "tsm_enc_adam",
            "tsm_select_rows", "tsm_allpairs_sym", "tsm_matrix_gather", "tsm_enc_embed_workspace_bytes",
-           "tsm_enc_embed", "tsm_enc_embed_status", "tsm_enc_embed_opts", "tsm_enc_loss_grad_w", "tsm_scan_dim",
+           "tsm_enc_embed", "tsm_enc_embed_status", "tsm_enc_train_status", "tsm_enc_embed_opts",
+           "tsm_enc_loss_grad_w", "tsm_scan_dim",
            "tsm_scan_image_bytes", "tsm_scan_prepare", "tsm_scan", "tsm_scan_opts")
 
 
@@ -93,6 +94,8 @@ def load():
         lib.tsm_enc_embed.argtypes = [_vp, _vp, _vp, _vp, _i32, _i32, _fp, _vp, _vp, _vp]
         lib.tsm_enc_embed_opts.restype = ctypes.c_int
         lib.tsm_enc_embed_opts.argtypes = [_vp, _vp, _vp, _vp, _i32, _i32, _fp, _vp, _vp, _i64, _i32, _vp]
+        lib.tsm_enc_train_status.restype = ctypes.c_int
+        lib.tsm_enc_train_status.argtypes = [_vp, _vp, _vp]
         lib.tsm_enc_embed_status.restype = ctypes.c_int
         lib.tsm_enc_embed_status.argtypes = [_vp, ctypes.POINTER(_i32), _vp]
         lib.tsm_enc_loss_grad.restype = ctypes.c_int

@@ -17,9 +17,11 @@
 // The reference trains its learned measures the same way (MSE on
 // distance / max distance, nn/MLP_trajsimi_train.py:74-84,197-200).
 //
-// Training kernels (hand-written, SIMT FP32 FMA): 16 trajectories per CTA,
+// Training recurrences (hand-written, SIMT FP32 FMA): 16 trajectories per CTA,
 // the BF16 weights resident in shared memory for all time steps, time stepped
-// inside the kernel, FP32 activations, and the caches BPTT needs.  Inference
+// inside the kernel, FP32 activations, and the caches BPTT needs.  The weight
+// gradients of the GRU (reductions over every valid step of the batch) run on
+// the tensor cores (tsm_wgrad.cu, BF16 hi/lo split products).  Inference
 // (embedding a database or a query batch) runs on the tensor cores instead:
 // enc_gru_embed_tc takes 128 trajectories per CTA, so each step's products
 // (128 x 384 x 192) are tcgen05 MMA tiles with the accumulators in tensor
@@ -32,7 +34,8 @@
 //   enc_pair_loss     distances, MSE loss, dL/de (atomic)
 //   enc_head_bwd      dWo, dbo, dh_last; enc_skip_bwd: d sc_k
 //   enc_gru_bwd       BPTT: gate gradients G [B][T][384] (input side), dA [B][T][64]
-//   enc_gemm_tn       split-K reduction dW[m][n] += sum_k A[k][m] B[k][n]  (weight gradients)
+//   tsm_wgrad_tc      weight gradients dW_ih, dW_hh on the tensor cores (tsm_wgrad.cu)
+//   enc_colsum        bias gradients (column sums of the gate gradients)
 //   enc_conv_bwd      dW1, db1
 //   enc_adam          Adam step on the FP32 master weights
 //   enc_conv_fwd_tc   conv + relu -> BF16 a_t operand images for the tensor-core GRU
@@ -44,6 +47,7 @@
 
 #include "tsm.h"
 #include "tsm_umma.cuh"
+#include "tsm_wgrad.h"
 
 int tsm_internal_fail(int code, const char* msg);
 
@@ -451,61 +455,6 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_bwd(
     }
 }
 
-// C[m][n] += sum_k A[k*lda + m] * Bm[k*ldb + n] over k in this CTA's K slice.
-// Tile 64 x 64 outputs per CTA (256 threads, a 4 x 4 register block each:
-// two 16-byte shared loads feed 16 FMAs), K split across blockIdx.z; partial
-// sums are atomically added.  Weight gradients are reductions over
-// (trajectory, time) with K up to a few 10^5.
-// bgroup > 0: B has one extra row after every bgroup rows (H holds T+1 rows
-// per trajectory, the gate gradients T), i.e. B row = k + k / bgroup.
-constexpr int GT = 64;  // output tile edge
-constexpr int GK = 32;  // k per shared-memory stage
-__global__ void __launch_bounds__(256) enc_gemm_tn(const float* __restrict__ Am, int64_t lda,
-                                                   const float* __restrict__ Bm, int64_t ldb, int64_t K, int M,
-                                                   int Nn, int64_t kchunk, int bgroup, float* __restrict__ C,
-                                                   int ldc) {
-    __shared__ __align__(16) float as[GK][GT];
-    __shared__ __align__(16) float bs[GK][GT];
-    const int m0 = blockIdx.x * GT, n0 = blockIdx.y * GT;
-    const int64_t k_begin = (int64_t)blockIdx.z * kchunk;
-    const int64_t k_end = min(K, k_begin + kchunk);
-    const int tid = threadIdx.x;
-    const int tn = tid & 15, tm = tid >> 4;  // outputs n0 + 4 tn .. +3, m0 + 4 tm .. +3
-    float acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
-    for (int64_t k0 = k_begin; k0 < k_end; k0 += GK) {
-        for (int e = tid; e < GK * GT; e += 256) {  // coalesced rows of A and B
-            const int r = e / GT, c = e % GT;
-            const int64_t k = k0 + r;
-            as[r][c] = (k < k_end && m0 + c < M) ? Am[k * lda + m0 + c] : 0.f;
-            const int64_t kb = bgroup > 0 ? k + k / bgroup : k;
-            bs[r][c] = (k < k_end && n0 + c < Nn) ? Bm[kb * ldb + n0 + c] : 0.f;
-        }
-        __syncthreads();
-#pragma unroll 8
-        for (int kk = 0; kk < GK; ++kk) {
-            const float4 a = *reinterpret_cast<const float4*>(&as[kk][4 * tm]);
-            const float4 b = *reinterpret_cast<const float4*>(&bs[kk][4 * tn]);
-            const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int m = m0 + 4 * tm + i, n = n0 + 4 * tn + j;
-            if (m < M && n < Nn) atomicAdd(C + (int64_t)m * ldc + n, acc[i][j]);
-        }
-}
-
 // Column sums: out[n] += sum_k A[k*lda + n] (bias gradients).
 __global__ void enc_colsum(const float* __restrict__ Am, int64_t lda, int64_t K, int Nn, int64_t kchunk,
                            float* __restrict__ out) {
@@ -875,8 +824,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) enc_gru_embed_tc(const __nv_bfl
 namespace {
 
 struct EncWs {  // views into the caller's workspace
+    int* status;  // first word: bits OR-ed in by the tensor-core weight-gradient kernel (zeroed by the caller)
     float *A, *H, *R, *Z, *N, *GHN, *G, *GH, *dA, *hl, *E, *dE, *dhl, *pred, *loss, *X;
     __nv_bfloat16* wq;
+    void* wg;  // scratch of tsm_wgrad_tc
 };
 
 int64_t align64(int64_t n) { return (n + 63) & ~int64_t(63); }
@@ -891,6 +842,9 @@ int64_t ws_layout(int B, int T, int P, float* base, EncWs* w) {
     EncWs tmp;
     EncWs* x = w ? w : &tmp;
     const int64_t BT = (int64_t)B * T;
+    float* st = nullptr;
+    take(&st, 1);
+    if (base) x->status = reinterpret_cast<int*>(st);
     take(&x->A, BT * enc::C1);
     take(&x->H, (int64_t)B * (T + 1) * enc::HD);
     take(&x->R, BT * enc::HD);
@@ -910,6 +864,9 @@ int64_t ws_layout(int B, int T, int P, float* base, EncWs* w) {
     float* wqf = nullptr;
     take(&wqf, (enc::N_PARAMS + 1) / 2);  // BF16 copy of the weights
     if (base) x->wq = reinterpret_cast<__nv_bfloat16*>(wqf);
+    float* wg = nullptr;
+    take(&wg, (tsm_wgrad_scratch_bytes(B, T) + 3) / 4);
+    if (base) x->wg = wg;
     return o;
 }
 
@@ -965,14 +922,13 @@ int enc_backward(const float* params, const float* pts, const int64_t* off, cons
     if (rc) return rc;
     enc_gru_bwd<<<(B + S - 1) / S, GRU_THREADS, kGruBwdSmem, s>>>(w.dhl, len, B, T, w.wq, w.H, w.R, w.Z, w.N,
                                                                    w.GHN, w.G, w.GH, w.dA);
-    // weight gradients: reductions over k = b*T + t
+    // weight gradients dWih[j][c] += G . A, dWhh[j][k] += GH . H[t]: reductions over the valid (b, t) on the
+    // tensor cores (tsm_wgrad.cu); the bias gradients are column sums over k = b*T + t
+    if ((rc = tsm_wgrad_tc(w.G, w.GH, w.A, w.H, len, B, T, w.wg, w.status, grad + OFF_WIH, grad + OFF_WHH, s)))
+        return rc;
     const int64_t K = (int64_t)B * T;
     const int64_t kchunk = 2048;
     const unsigned kz = (unsigned)((K + kchunk - 1) / kchunk);
-    enc_gemm_tn<<<dim3(G3 / GT, C1 / GT, kz), 256, 0, s>>>(w.G, G3, w.A, C1, K, G3, C1, kchunk, 0,
-                                                           grad + OFF_WIH, C1);  // dWih[j][c] += G . A
-    enc_gemm_tn<<<dim3(G3 / GT, HD / GT, kz), 256, 0, s>>>(w.GH, G3, w.H, HD, K, G3, HD, kchunk, T,
-                                                           grad + OFF_WHH, HD);  // dWhh[j][k] += GH . H[t]
     enc_colsum<<<dim3((G3 + 127) / 128, kz), 128, 0, s>>>(w.G, G3, K, G3, kchunk, grad + OFF_BIH);
     enc_colsum<<<dim3((G3 + 127) / 128, kz), 128, 0, s>>>(w.GH, G3, K, G3, kchunk, grad + OFF_BHH);
     const int tchunk = 64;
@@ -1114,6 +1070,21 @@ int tsm_enc_embed_opts(const float* params, const float* pts, const int64_t* off
 int tsm_enc_embed(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,
                   int32_t T, const float* nrm, void* workspace, float* emb, void* stream) {
     return tsm_enc_embed_opts(params, pts, off, len, B, T, nrm, workspace, emb, enc::TC_WAIT_CYCLES, -1, stream);
+}
+
+int tsm_enc_train_status(void* workspace, int32_t* status, void* stream) {
+    if (!workspace || !status) return tsm_internal_fail(TSM_EINVAL, "tsm_enc_train_status: null argument");
+    int rc = enc_check(cudaStreamSynchronize((cudaStream_t)stream), "tsm_enc_train_status: synchronise");
+    if (rc) return rc;
+    if ((rc = enc_check(cudaMemcpy(status, workspace, 4, cudaMemcpyDeviceToHost), "tsm_enc_train_status: read")))
+        return rc;
+    if (*status == 0) return TSM_OK;
+    if ((rc = enc_check(cudaMemset(workspace, 0, 4), "tsm_enc_train_status: clear"))) return rc;
+    char b[256];
+    snprintf(b, sizeof(b), "tsm_enc_loss_grad: a tensor-core wait ran out in the weight gradients (status %d%s); "
+             "the gradients of the calls since the last check are incomplete", *status,
+             (*status & 128) ? ": tensor memory not freed, reset the device" : "");
+    return tsm_internal_fail(TSM_ETIMEOUT, b);
 }
 
 int tsm_enc_embed_status(const void* workspace, int32_t* status, void* stream) {

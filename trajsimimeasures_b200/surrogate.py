@@ -112,9 +112,23 @@ class Encoder:
             nb = _lib.load().tsm_enc_workspace_bytes(*[max(k, h) for k, h in zip(key, self._ws_key)])
             if nb < 0:
                 raise ValueError("bad encoder batch shape")
+            if self._ws is not None:
+                self.check_training()  # the old workspace's status word goes with it
             self._ws = torch.empty(nb // 4 + 64, dtype=torch.float32, device=self.params.device)
+            self._ws[:1].zero_()  # the training status word (tsm_enc_train_status)
             self._ws_key = tuple(max(k, h) for k, h in zip(key, self._ws_key))
         return self._ws
+
+    def check_training(self, stream=None):
+        """Raises TsmError if a bounded wait of the tensor-core weight-gradient
+        kernel ran out in a loss_grad call since the last check (the gradients
+        of those calls are incomplete).  Synchronises the stream; fit() calls
+        it once per epoch."""
+        if self._ws is None:
+            return
+        st = ctypes.c_int32(0)
+        rc = _lib.load().tsm_enc_train_status(_ptr(self._ws), ctypes.byref(st), _stream_ptr(stream))
+        _lib.check(rc, "tsm_enc_train_status")
 
     def _nrm_ptr(self):
         return (ctypes.c_float * 4)(*[float(x) for x in self.nrm])
@@ -236,6 +250,7 @@ class Encoder:
                 self.adam(grad, lr=lr * 0.5 * (1 + math.cos(math.pi * (ep + b0 / n) / epochs)))
                 tot += loss.double() * P
             hist.append(float(tot.item()) / n)
+            self.check_training()
             if log:
                 log(f"epoch {ep}: mse {hist[-1]:.3e}")
         return hist
