@@ -299,7 +299,9 @@ int tsm_scan_opts(const void* q_img, int64_t nq, const void* db_img, int64_t nd,
  *   pts/off/len  a packed batch of B trajectories, T = max length in it
  *   nrm     HOST float[4] = (mean_x, mean_y, 1/s_x, 1/s_y) input scaling (the
  *           Python encoder uses one scale for both axes, s_x = s_y)
- *   workspace  device memory of tsm_enc_workspace_bytes(B, T, P) bytes
+ *   workspace  device memory of tsm_enc_workspace_bytes(B, T, P) bytes, 256-byte
+ *           aligned; its first 4 bytes are the training status word
+ *           (tsm_enc_train_status): zero them once after allocating it
  */
 int tsm_enc_param_count(void);
 int64_t tsm_enc_workspace_bytes(int32_t B, int32_t T, int32_t P);
@@ -312,7 +314,7 @@ int tsm_enc_forward(const float* params, const float* pts, const int64_t* off, c
  * keeps them FP32), and no training caches.  Used to embed the kNN database
  * and the queries: the test-time embedding of the reference's learned
  * measures (nn/MLP_trajsimi_train.py).  emb float32 [B][160] (device);
- * workspace of tsm_enc_embed_workspace_bytes(B, T) bytes.  Batches of similar
+ * workspace of tsm_enc_embed_workspace_bytes(B, T) bytes, 256-byte aligned.  Batches of similar
  * lengths waste fewer steps (a CTA runs its longest trajectory's length). */
 int64_t tsm_enc_embed_workspace_bytes(int32_t B, int32_t T);
 int tsm_enc_embed(const float* params, const float* pts, const int64_t* off, const int32_t* len, int32_t B,

@@ -78,9 +78,13 @@ def test_invalid_arguments_fail_before_cuda(lib):
     assert rc == -3 and b"max_len 40000 > 32768" in lib.tsm_last_error()
     st = ctypes.c_int32(0)
     assert lib.tsm_enc_embed_status(nul, ctypes.byref(st), nul) == -1
-    rc = lib.tsm_enc_embed_opts(dummy, dummy, dummy, dummy, 4, 8, (ctypes.c_float * 4)(0, 0, 1, 1), dummy, dummy, 0,
-                                -1, nul)
+    rc = lib.tsm_enc_embed_opts(dummy, dummy, dummy, dummy, 4, 8, (ctypes.c_float * 4)(0, 0, 1, 1),
+                                ctypes.c_void_p(256), dummy, 0, -1, nul)
     assert rc == -1 and b"wait limit" in lib.tsm_last_error()
+    assert lib.tsm_enc_train_status(nul, ctypes.byref(st), nul) == -1
+    rc = lib.tsm_enc_embed(dummy, dummy, dummy, dummy, 4, 8, (ctypes.c_float * 4)(0, 0, 1, 1), ctypes.c_void_p(272),
+                           dummy, nul)
+    assert rc == -1 and b"256-byte aligned" in lib.tsm_last_error()
     with pytest.raises(_lib.TsmError):
         _lib.check(-1, "x")
 

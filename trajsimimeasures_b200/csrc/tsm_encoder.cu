@@ -886,6 +886,8 @@ int enc_args(const void* params, const void* pts, const void* off, const void* l
              const void* ws) {
     if (!params || !pts || !off || !len || !nrm || !ws) return tsm_internal_fail(TSM_EINVAL, "encoder: null pointer");
     if (B < 1 || T < 1) return tsm_internal_fail(TSM_EINVAL, "encoder: batch and time must be positive");
+    if (reinterpret_cast<uintptr_t>(ws) % 256)
+        return tsm_internal_fail(TSM_EINVAL, "encoder: workspace must be 256-byte aligned");
     if ((int64_t)B * T * enc::G3 > (int64_t)1 << 40) return tsm_internal_fail(TSM_EINVAL, "encoder: batch too large");
     return TSM_OK;
 }
