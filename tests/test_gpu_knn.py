@@ -182,6 +182,12 @@ def test_scan_dense_matches_fp64_and_lists_match_dense():
     assert int(st.item()) == 0
     d = dense[:, :n].double()
     assert bool((dense[:, n:] == -7.0).all())  # nothing written past nd
+    # a row stride that is a multiple of 4 floats takes the 16-byte stores: the same values
+    dense4 = torch.full((nq, n + 4), -7.0, device="cuda")
+    assert lib.tsm_scan(_ptr(qimg), nq, _ptr(dimg), n, scale, None, 0, None, None, None, _ptr(dense4), n + 4,
+                        _ptr(st), None) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(dense4[:, :n], dense[:, :n]) and bool((dense4[:, n:] == -7.0).all())
     E64, Q64 = E.double(), Qe.double()
     assert ((norms.double() - (E64 * E64).sum(1)).abs() <= 1e-5 * (E64 * E64).sum(1)).all()
     ref = (E64 * E64).sum(1)[None, :] - 2.0 * Q64 @ E64.T

@@ -310,6 +310,8 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
         const int64_t q = (int64_t)qt * QM + 32 * quarter + lane;
         const bool qv = q < nq;
         const float to_d = -2.f * inv_s2;  // d = to_d * acc
+        // dense rows start on 16-byte boundaries when the output and its row stride allow
+        const bool vec_ok = DENSE && (reinterpret_cast<uintptr_t>(dense) % 16 == 0) && (ld % 4 == 0);
         // d <= thr  <=>  acc >= -(s^2 / 2) thr; padding queries get +inf (never)
         const float at = DENSE ? 0.f : (qv ? -0.5f * thr[q] / inv_s2 : __int_as_float(0x7f800000));
         int staged = 0;
@@ -345,9 +347,20 @@ __global__ void __launch_bounds__(THREADS, 1) scan_kernel(
                 const int64_t jb = jh + cb;
                 if (DENSE) {
                     if (qv) {
+                        float* row = dense + q * ld + jb;
+                        if (vec_ok && jb + EPI_COLS <= nd) {  // 16-byte stores: a quarter of the L2 transactions
 #pragma unroll
-                        for (int i = 0; i < EPI_COLS; ++i)
-                            if (jb + i < nd) dense[q * ld + jb + i] = to_d * __uint_as_float(r[i >> 4][i & 15]);
+                            for (int i = 0; i < EPI_COLS; i += 4)
+                                *reinterpret_cast<float4*>(row + i) =
+                                    make_float4(to_d * __uint_as_float(r[i >> 4][i & 15]),
+                                                to_d * __uint_as_float(r[(i + 1) >> 4][(i + 1) & 15]),
+                                                to_d * __uint_as_float(r[(i + 2) >> 4][(i + 2) & 15]),
+                                                to_d * __uint_as_float(r[(i + 3) >> 4][(i + 3) & 15]));
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < EPI_COLS; ++i)
+                                if (jb + i < nd) row[i] = to_d * __uint_as_float(r[i >> 4][i & 15]);
+                        }
                     }
                 } else {
                     // tree maximum (depth 6, not a chain of 64); the level of 8 is kept: group g holds
