@@ -97,6 +97,17 @@ def parse():
     return a
 
 
+def _measured_peaks():
+    """The driver-measured peaks of this pool's B200s (MEASURED_PEAKS.json at
+    the repository root), {} when absent."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -816,8 +827,9 @@ def run_knn(args, enc=None, emit=True):
         from trajsimimeasures_b200.knn import knn_rerank
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         torch.cuda.nvtx.range_push("knn_query")  # the launches of one query call (ncu --nvtx-include knn_query/)
+        scan_ev = []
         ev[0].record()
-        cand = index.candidates(Q, min(c, Dset.n)) if c else None
+        cand = index.candidates(Q, min(c, Dset.n), scan_events=scan_ev) if c else None
         ev[1].record()
         if cand is not None:
             knn_rerank(Q, Dset, cand, 10)
@@ -826,6 +838,16 @@ def run_knn(args, enc=None, emit=True):
         torch.cuda.synchronize()
         out["filtered_phase_s"] = {"candidates": ev[0].elapsed_time(ev[1]) / 1e3,
                                    "rerank": ev[1].elapsed_time(ev[2]) / 1e3}
+        if scan_ev:  # the main candidate scan, timed with events on its stream
+            ms = sum(a.elapsed_time(b) for a, b, _, _ in scan_ev)
+            flop = sum(2.0 * q * r * 483 for _, _, q, r in scan_ev)  # K = 3 x 160 split products + 3 norm columns
+            peak = _measured_peaks().get("bf16_tflops")
+            out["scan_roofline"] = {
+                "kernel": "scan::scan_kernel<false>", "bound": "tensor", "ms": ms, "unit": "TFLOP/s",
+                "achieved": flop / ms / 1e9, "peak": peak, "frac": (flop / ms / 1e9 / peak) if peak else None,
+                "flop_per_launch": flop, "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst), of measured",
+                "note": "algorithmic FLOPs: 2 x queries x rows x 483 (FP16 split products, K padded to 512 "
+                        "in the kernel)"}
         out["filtered_reps_s"] = reps
         out.update({"filtered_queries_per_s": args.n_queries / f_s, "filtered_s": f_s, "candidates": c,
                     "calibration_recall": {str(k): v for k, v in rec.items()},

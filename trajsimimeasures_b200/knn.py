@@ -236,12 +236,18 @@ class SurrogateIndex:
             self.status.zero_()
             raise _lib.TsmError(f"tsm_scan: a tensor-core wait ran out (status {st})")
 
-    def candidates(self, Q: TrajSet, c: int, chunk=4096) -> torch.Tensor:
-        """Candidate indices [nq, c] (int64, any order)."""
+    def candidates(self, Q: TrajSet, c: int, chunk=4096, scan_events=None) -> torch.Tensor:
+        """Candidate indices [nq, c] (int64, any order).  scan_events: a list
+        to which (start, end, queries, rows) CUDA events are appended around
+        each main scan launch (for timing it on its stream).  The host waits
+        on the device once per chunk, for the status words and the overflow
+        count together."""
         lib = _lib.load()
         n = self.E.shape[0]
         c = min(int(c), n)
-        eq = self.enc.embed(Q)
+        enc_status = torch.zeros(1, dtype=torch.int32, device=Q.device)
+        eq = self.enc.embed(Q, status_out=enc_status)
+        dense_only = False
         out = torch.empty((Q.n, c), dtype=torch.int64, device=Q.device)
         S = int(self.sample.shape[0])
         exp = c * S / n
@@ -254,23 +260,40 @@ class SurrogateIndex:
             qimg = self._query_image(e)
             if ks >= S or cap >= n:  # the list would hold most of the database: dense
                 out[q0:q0 + b] = select_rows(self._dense(qimg, b, self.img, n), c).long()
+                dense_only = True
                 continue
             ds = self._dense(qimg, b, self.s_img, S)
             thr = torch.topk(ds, ks, dim=1, largest=False, sorted=True).values[:, -1].contiguous()
             idx = torch.empty((b, cap), dtype=torch.int32, device=Q.device)
             dd = torch.full((b, cap), float("inf"), dtype=torch.float32, device=Q.device)
             cnt = torch.zeros(b, dtype=torch.int32, device=Q.device)
+            if scan_events is not None:
+                ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                ev[0].record()
             rc = lib.tsm_scan(_ptr(qimg), b, _ptr(self.img), n, self.scale, _ptr(thr), cap, _ptr(idx), _ptr(dd),
                               _ptr(cnt), None, 0, _ptr(self.status), _stream_ptr(None))
             _lib.check(rc, "tsm_scan")
+            if scan_events is not None:
+                ev[1].record()
+                scan_events.append((ev[0], ev[1], b, n))
             pos = select_rows(dd, c).long()
             res = torch.gather(idx, 1, pos).long()
-            bad = torch.nonzero((cnt < c) | (cnt > cap)).flatten()
-            if bad.numel():  # threshold too tight or list overflowed: those queries densely
+            badm = (cnt < c) | (cnt > cap)
+            # one host wait: embedding status, scan status and the number of lists to redo
+            flags = torch.stack([enc_status[0], self.status[0], badm.sum().to(torch.int32)]).cpu()
+            if int(flags[0]):
+                raise _lib.TsmError(f"tsm_enc_embed: a tensor-core wait ran out (status {int(flags[0])})")
+            if int(flags[1]):
+                self._check_status()
+            if int(flags[2]):  # threshold too tight or list overflowed: those queries densely
+                bad = torch.nonzero(badm).flatten()
                 eb = e[bad]
                 res[bad] = select_rows(self._dense(self._query_image(eb), eb.shape[0], self.img, n), c).long()
             out[q0:q0 + b] = res
-        self._check_status()
+        if dense_only:  # chunks without the combined wait above
+            if int(enc_status.item()):
+                raise _lib.TsmError(f"tsm_enc_embed: a tensor-core wait ran out (status {int(enc_status.item())})")
+            self._check_status()
         return out
 
     def query(self, Q: TrajSet, k=10, c=None, measure="dtw", **kw):

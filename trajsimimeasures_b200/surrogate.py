@@ -152,14 +152,19 @@ class Encoder:
     # trajectories per tensor-core embedding launch: 296 CTAs of 128, two waves over a B200's 148 SMs
     TC_BATCH = 296 * 128
 
-    def embed(self, s: TrajSet, idx=None, batch=None, stream=None, tensor_cores=True) -> torch.Tensor:
+    def embed(self, s: TrajSet, idx=None, batch=None, stream=None, tensor_cores=True,
+              status_out=None) -> torch.Tensor:
         """Embeddings [n, 160] of trajectories idx (default all) of s.
 
         tensor_cores=True: the tcgen05 inference kernel (tsm_enc_embed; a_t
         and h_t enter the gate products as BF16), over batches of similar
-        lengths.  False: the training forward (tsm_enc_forward, FP32 a_t and h_t)."""
+        lengths.  False: the training forward (tsm_enc_forward, FP32 a_t and h_t).
+        status_out: a device int32 [1] into which the kernels' status bits are
+        OR-ed, for a caller that checks it later (no host synchronisation
+        here); None: checked here, TsmError on a wait that ran out."""
         lib = _lib.load()
         batch = batch or (self.TC_BATCH if tensor_cores else 4096)
+        idx_given = idx is not None
         idx = torch.arange(s.n, device=s.device) if idx is None else torch.as_tensor(idx, device=s.device).long()
         n = int(idx.shape[0])
         out = torch.empty((n, EMB), dtype=torch.float32, device=s.device)
@@ -172,7 +177,9 @@ class Encoder:
         off_all, ln_all = s.off[sel_all].contiguous(), s.lens[sel_all].contiguous()
         starts = list(range(0, n, batch))
         ends = [min(b0 + batch, n) for b0 in starts]
-        if tensor_cores:  # sorted: a batch's longest trajectory is its last
+        if tensor_cores and len(starts) == 1 and idx_given is False:  # the whole set: its max length is known
+            tmax = np.array([s.max_len])
+        elif tensor_cores:  # sorted: a batch's longest trajectory is its last
             tmax = ln_all[torch.tensor([e - 1 for e in ends], device=s.device)].cpu().numpy()
         else:
             tmax = torch.stack([ln_all[b0:e].max() for b0, e in zip(starts, ends)]).cpu().numpy()
@@ -182,7 +189,9 @@ class Encoder:
                        for b0, e, t in zip(starts, ends, tmax))
             if self._ews is None or self._ews.numel() * 4 < need:
                 self._ews = torch.empty(need // 4 + 64, dtype=torch.float32, device=self.params.device)
-        status = torch.zeros(1, dtype=torch.int32, device=s.device) if tensor_cores else None
+        status = None
+        if tensor_cores:
+            status = status_out if status_out is not None else torch.zeros(1, dtype=torch.int32, device=s.device)
         for b0, e, t in zip(starts, ends, tmax):
             B, T = e - b0, max(int(t), 1)
             off, ln, r = off_all[b0:e], ln_all[b0:e], res[b0:e]
@@ -203,7 +212,7 @@ class Encoder:
                                          self._nrm_ptr(), _ptr(ws), _ptr(r), _stream_ptr(stream))
                 _lib.check(rc, "tsm_enc_forward")
         out[perm] = res
-        if status is not None and int(status.item()):
+        if status is not None and status_out is None and int(status.item()):
             raise _lib.TsmError(f"tsm_enc_embed: a tensor-core wait ran out (status {int(status.item())}); "
                                 "the affected embeddings are NaN")
         return out
