@@ -124,12 +124,15 @@ int tsm_pairs(int measure, const float* pts, const int64_t* off_a, const int32_t
  *   cand int32 [nq][ncand]: database indices; a query's row is best sorted by
  *        database length (neighbouring threads then get equal loop shapes);
  *        an index outside 0..nd-1 gives NaN (count -1) for that entry
+ *   q_order int32 [nq] or NULL: the order in which the queries are processed
+ *        (a permutation of 0..nq-1; longest first shortens the tail of the
+ *        launch); rows of cand and out stay indexed by query
  *   ld_out >= ncand; the other arguments as in tsm_matrix
  */
 int tsm_matrix_gather(int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len, int64_t nq,
                       int32_t q_max_len, const float* d_pts, const int64_t* d_off, const int32_t* d_len, int64_t nd,
-                      int32_t d_max_len, const int32_t* cand, int64_t ncand, const tsm_params* params, float* out,
-                      int64_t ld_out, int32_t* out_counts, void* stream);
+                      int32_t d_max_len, const int32_t* cand, int64_t ncand, const int32_t* q_order,
+                      const tsm_params* params, float* out, int64_t ld_out, int32_t* out_counts, void* stream);
 
 /*
  * All pairs of a query set Q and a database set D:

@@ -135,6 +135,13 @@ def test_matrix_gather_equals_matrix_entries(measure):
     if measure_id(measure) in (1, 2):
         np.testing.assert_array_equal(k[:, :301][ok], fc[qi[ok], cand[ok]])
         assert k[3, 5] == -1 and k[4, 7] == -1
+    # a processing order of the queries (longest first) changes nothing in the result
+    qo = torch.argsort(Q.lens, descending=True, stable=True).to(torch.int32)
+    out2 = torch.full((37, 320), -5.0, device=dev)
+    cnt2 = torch.full((37, 320), -5, dtype=torch.int32, device=dev)
+    matrix_gather_raw(measure, Q, Dset, c, out=out2, counts=cnt2, q_order=qo, **kw)
+    np.testing.assert_array_equal(out2.cpu().numpy(), o)
+    np.testing.assert_array_equal(cnt2.cpu().numpy(), k)
 
 
 def _scan_case(n=20000, nq=300, seed=21):

@@ -71,7 +71,7 @@ def load():
                                         ctypes.POINTER(TsmParams), _vp, _i64, _vp, _vp]
         lib.tsm_matrix_gather.restype = ctypes.c_int
         lib.tsm_matrix_gather.argtypes = [ctypes.c_int, _vp, _vp, _vp, _i64, _i32, _vp, _vp, _vp, _i64, _i32, _vp, _i64,
-                                          ctypes.POINTER(TsmParams), _vp, _i64, _vp, _vp]
+                                          _vp, ctypes.POINTER(TsmParams), _vp, _i64, _vp, _vp]
         lib.tsm_allpairs_sym.restype = ctypes.c_int
         lib.tsm_allpairs_sym.argtypes = [ctypes.c_int, _vp, _vp, _vp, _vp, _i64, _i32, ctypes.POINTER(TsmParams), _vp,
                                          _i64, _vp, _vp]

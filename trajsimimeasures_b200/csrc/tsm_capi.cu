@@ -362,8 +362,8 @@ int tsm_matrix_rows(int measure, const float* q_pts, const int64_t* q_off, const
 
 int tsm_matrix_gather(int measure, const float* q_pts, const int64_t* q_off, const int32_t* q_len, int64_t nq,
                       int32_t q_max_len, const float* d_pts, const int64_t* d_off, const int32_t* d_len, int64_t nd,
-                      int32_t d_max_len, const int32_t* cand, int64_t ncand, const tsm_params* params, float* out,
-                      int64_t ld_out, int32_t* out_counts, void* stream) {
+                      int32_t d_max_len, const int32_t* cand, int64_t ncand, const int32_t* q_order,
+                      const tsm_params* params, float* out, int64_t ld_out, int32_t* out_counts, void* stream) {
     g_err.clear();
     if (measure < TSM_DTW || measure > TSM_HAUSDORFF)
         return fail(TSM_EINVAL, "tsm_matrix_gather: unknown measure %d", measure);
@@ -373,7 +373,7 @@ int tsm_matrix_gather(int measure, const float* q_pts, const int64_t* q_off, con
         return fail(TSM_EINVAL, "tsm_matrix_gather: null pointer");
     if (ld_out < ncand) return fail(TSM_EINVAL, "tsm_matrix_gather: ld_out < ncand");
     if (q_max_len < 0 || d_max_len < 0) return fail(TSM_EINVAL, "tsm_matrix_gather: max_len < 0");
-    return matrix_launch("tsm_matrix_gather", measure, q_pts, q_off, q_len, nullptr, nq, q_max_len, d_pts, d_off,
+    return matrix_launch("tsm_matrix_gather", measure, q_pts, q_off, q_len, q_order, nq, q_max_len, d_pts, d_off,
                          d_len, cand, ncand, nd, d_max_len, 2, params, out, ld_out, out_counts, stream);
 }
 

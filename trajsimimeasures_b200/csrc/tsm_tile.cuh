@@ -404,7 +404,8 @@ __global__ void __launch_bounds__(128) dp_pairs_kernel(
 // computed (the upper triangle in sorted order), and each value is written to
 // out[i, j] and out[j, i]; CTAs wholly below the diagonal exit at once.
 // Gather mode (sym == 2): d_order holds one row of nd database indices per
-// query, and slot t of query i goes to out[i, t].  A database index outside
+// query i (row i, whatever the processing order q_order), and slot t of query i
+// goes to out[i, t].  A database index outside
 // 0..d_total-1 gives NaN (count -1).
 // Dynamic shared memory = cap float4 columns + W*32*cap floats.
 
@@ -442,7 +443,7 @@ __global__ void __launch_bounds__(128) dp_matrix_kernel(
     }
     const int64_t slot = (int64_t)chunk * blockDim.x + threadIdx.x;
     if (slot >= nd || (sym == 1 && slot < qs)) return;
-    const int64_t dj = d_order ? (int64_t)d_order[(sym == 2 ? qs * nd : 0) + slot] : slot;
+    const int64_t dj = d_order ? (int64_t)d_order[(sym == 2 ? qi * nd : 0) + slot] : slot;
     const bool dbad = dj < 0 || dj >= d_total;
     const int ndl = dbad ? -1 : d_len[dj];
     const bool count = (M == EDR || M == LCSS) && counts != nullptr;
@@ -674,7 +675,7 @@ __global__ void __launch_bounds__(128) hausdorff_matrix_kernel(
     __syncthreads();
     const int64_t slot = (int64_t)chunk * blockDim.x + threadIdx.x;
     if (slot >= nd || (sym == 1 && slot < qs)) return;
-    const int64_t dj = d_order ? (int64_t)d_order[(sym == 2 ? qs * nd : 0) + slot] : slot;
+    const int64_t dj = d_order ? (int64_t)d_order[(sym == 2 ? qi * nd : 0) + slot] : slot;
     const bool dbad = dj < 0 || dj >= d_total;
     const int ndl = dbad ? -1 : d_len[dj];
     const int64_t o_idx = qi * ld + (sym == 2 ? slot : dj);

@@ -349,16 +349,18 @@ def pair_order_dev(len_a: torch.Tensor, len_b: torch.Tensor, rows=DEFAULT_ROWS) 
 
 
 def matrix_gather_raw(measure, q: TrajSet, d: TrajSet, cand: torch.Tensor, *, out, counts=None, eps=0.0,
-                      gpoint=(0.0, 0.0), exact=False, rows=0, stream=None):
+                      gpoint=(0.0, 0.0), exact=False, rows=0, stream=None, q_order=None):
     """tsm_matrix_gather: out[i, s] = measure(Q_i, D_cand[i, s]) for an int32
-    candidate matrix cand [nq, c] on the device (no copies, no sync)."""
+    candidate matrix cand [nq, c] on the device (no copies, no sync).
+    q_order: int32 [nq] device processing order of the queries (None: 0..nq-1)."""
     m = measure_id(measure)
     lib = _lib.load()
     p = _lib.params(eps, shift_gpoint(gpoint, same_origin(q, d)), exact, rows)
     if cand.dtype != torch.int32 or cand.dim() != 2 or not cand.is_contiguous():
         raise ValueError("cand must be a contiguous int32 [nq, c] tensor")
     rc = lib.tsm_matrix_gather(m, _ptr(q.pts), _ptr(q.off), _ptr(q.lens), q.n, q.max_len, _ptr(d.pts), _ptr(d.off),
-                               _ptr(d.lens), d.n, d.max_len, _ptr(cand), int(cand.shape[1]), ctypes.byref(p),
+                               _ptr(d.lens), d.n, d.max_len, _ptr(cand), int(cand.shape[1]), _ptr(q_order),
+                               ctypes.byref(p),
                                _ptr(out), int(out.stride(0)), _ptr(counts), _stream_ptr(stream))
     _lib.check(rc, "tsm_matrix_gather")
     return out

@@ -80,7 +80,7 @@ def knn_exhaustive(Q: TrajSet, D: TrajSet, k=10, measure="dtw", *, chunk=1 << 18
 
 
 def knn_rerank(Q: TrajSet, D: TrajSet, cand: torch.Tensor, k=10, measure="dtw", *, eps=0.0, gpoint=(0.0, 0.0),
-               exact=False, stream=None):
+               exact=False, stream=None, gather_lpt=True):
     """Exact top-k among candidate database indices cand [nq, c] (int64):
     (dist [nq, k], index [nq, k])."""
     m = measure_id(measure)
@@ -91,7 +91,9 @@ def knn_rerank(Q: TrajSet, D: TrajSet, cand: torch.Tensor, k=10, measure="dtw", 
         o = torch.argsort(D.lens[cand], dim=1, stable=True)
         cs = torch.gather(cand, 1, o).to(torch.int32).contiguous()
         dd = torch.empty((nq, c), dtype=torch.float32, device=Q.device)
-        matrix_gather_raw(m, Q, D, cs, out=dd, eps=eps, gpoint=gpoint, exact=exact, stream=stream)
+        # longest queries first: their CTAs run longest, so the launch ends with short ones
+        qo = torch.argsort(Q.lens, descending=True, stable=True).to(torch.int32) if gather_lpt else None
+        matrix_gather_raw(m, Q, D, cs, out=dd, eps=eps, gpoint=gpoint, exact=exact, stream=stream, q_order=qo)
         cand = cs.long()
     else:  # queries too long for the matrix form: the paired kernel, in loop-shape order
         shift = D.pts.shape[0]
