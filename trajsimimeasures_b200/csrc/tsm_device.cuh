@@ -135,6 +135,11 @@ struct DtwCell {
                                                  float /*grow*/, float /*gcol*/, float /*eps2*/) {
         return __fadd_rn(tsqrt<EXACT>(d2), min3f(dg, up, left));
     }
+    // split form (cell == comb(term(d2))): the local term alone, then the recurrence
+    __device__ __forceinline__ static float term(float d2, float) { return tsqrt<EXACT>(d2); }
+    __device__ __forceinline__ static float comb(float dg, float up, float left, float t, float, float) {
+        return __fadd_rn(t, min3f(dg, up, left));
+    }
 };
 
 // Discrete Frechet on squared distances: F = max(d2, min(dg, up, left))
@@ -150,6 +155,10 @@ struct FrechetCell {
                                                  float, float, float) {
         return fmaxf(d2, min3f(dg, up, left));
     }
+    __device__ __forceinline__ static float term(float d2, float) { return d2; }
+    __device__ __forceinline__ static float comb(float dg, float up, float left, float t, float, float) {
+        return fmaxf(t, min3f(dg, up, left));
+    }
 };
 
 // ERP: D = min(left + g(col), up + g(row), dg + d)  (core/erp.py:80-85);
@@ -164,6 +173,10 @@ struct ErpCell {
     __device__ __forceinline__ static float cell(float dg, float up, float left, float d2,
                                                  float grow, float gcol, float) {
         return min3f(__fadd_rn(left, gcol), __fadd_rn(up, grow), __fadd_rn(dg, tsqrt<EXACT>(d2)));
+    }
+    __device__ __forceinline__ static float term(float d2, float) { return tsqrt<EXACT>(d2); }
+    __device__ __forceinline__ static float comb(float dg, float up, float left, float t, float grow, float gcol) {
+        return min3f(__fadd_rn(left, gcol), __fadd_rn(up, grow), __fadd_rn(dg, t));
     }
 };
 
@@ -185,6 +198,10 @@ struct EdrCell {
         const float s = (d2 < eps2) ? -2.f : -1.f;
         return min3f(__fadd_rn(dg, s), up, left);
     }
+    __device__ __forceinline__ static float term(float d2, float eps2) { return (d2 < eps2) ? -2.f : -1.f; }
+    __device__ __forceinline__ static float comb(float dg, float up, float left, float t, float, float) {
+        return min3f(__fadd_rn(dg, t), up, left);
+    }
 };
 
 // LCSS count: if d2 < eps2: C = dg + 1 else max(up, left), borders 0
@@ -201,6 +218,10 @@ struct LcssCell {
                                                  float, float, float eps2) {
         float m = (d2 < eps2) ? 1.f : 0.f;
         return max3f(__fadd_rn(dg, m), up, left);
+    }
+    __device__ __forceinline__ static float term(float d2, float eps2) { return (d2 < eps2) ? 1.f : 0.f; }
+    __device__ __forceinline__ static float comb(float dg, float up, float left, float t, float, float) {
+        return max3f(__fadd_rn(dg, t), up, left);
     }
 };
 

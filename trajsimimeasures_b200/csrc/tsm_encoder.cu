@@ -64,6 +64,7 @@ constexpr int ED = EO + SK; // embedding: [head outputs | skip weights * resampl
 static_assert(SK == 32, "enc_skip_bwd maps one skip value per lane");
 constexpr int S = 16;     // trajectories per GRU CTA
 constexpr int GRU_THREADS = 384;
+constexpr int SP = S + 2;  // row stride of the backward's trajectory-minor gate gradients (8-byte pairs, 2-way banks)
 
 // parameter offsets in the flat FP32 master buffer
 constexpr int OFF_W1 = 0;                    // [64][2][5]
@@ -160,12 +161,25 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
         for (int e = j; e < HD; e += GRU_THREADS) hb[e] = 0.f;
         for (int64_t e = (int64_t)(lens[s] + 1) * HD + j; e < (int64_t)(T + 1) * HD; e += GRU_THREADS) hb[e] = 0.f;
     }
-    for (int t = 0; t < tmax; ++t) {
-        for (int e = j; e < S * C1; e += GRU_THREADS) {
+    // this thread's elements e = j + 384 i of a_t, loaded a step ahead (the
+    // loads of step t + 1 are in flight during step t's products)
+    constexpr int AN = (S * C1 + GRU_THREADS - 1) / GRU_THREADS;
+    float an[AN];
+    auto load_a = [&](int t) {
+#pragma unroll
+        for (int i = 0; i < AN; ++i) {
+            const int e = j + GRU_THREADS * i;
             const int s = e / C1;
-            as[e] = (b0 + s < B && t < lens[s]) ? A[((int64_t)(b0 + s) * T + t) * C1 + e % C1] : 0.f;
+            an[i] = (e < S * C1 && b0 + s < B && t < lens[s]) ? A[((int64_t)(b0 + s) * T + t) * C1 + e % C1] : 0.f;
         }
+    };
+    if (tmax > 0) load_a(0);
+    for (int t = 0; t < tmax; ++t) {
+#pragma unroll
+        for (int i = 0; i < AN; ++i)
+            if (j + GRU_THREADS * i < S * C1) as[j + GRU_THREADS * i] = an[i];
         __syncthreads();
+        if (t + 1 < tmax) load_a(t + 1);
         float ai[S], ah[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -368,8 +382,8 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_bwd(
     __nv_bfloat16* wih = whh + G3 * HD;                             // [384][64]
     float* dh = reinterpret_cast<float*>(wih + G3 * C1);            // [S][128]
     float* dhd = dh + S * HD;                                       // [S][128] direct part (dh * z)
-    float* dgi = dhd + S * HD;                                      // [S][384]
-    float* dgh = dgi + S * G3;                                      // [S][384]
+    float* dgi = dhd + S * HD;                                      // [384][SP] gate gradients, trajectory-minor
+    float* dgh = dgi + G3 * SP;                                     // [384][SP]
     __shared__ int lens[S];
     const int tid = threadIdx.x;
     const int b0 = blockIdx.x * S;
@@ -394,14 +408,45 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_bwd(
     }
     int tmax = 0;
     for (int s = 0; s < S; ++s) tmax = max(tmax, lens[s]);
+    // The output products: threads 0..255 take 4 consecutive hidden units
+    // (dh) of two trajectories, threads 256..383 4 consecutive channels (dA)
+    // of two trajectories; per gate row jj one 8-byte load of 4 BF16 weights
+    // and one of the two trajectories' gate gradients feed 8 FMAs.  Each sum
+    // runs over jj in order from the same start as a dot product per output
+    // would, so the values are those of one thread per output.
+    const bool dh_part = tid < 256;
+    const int og = dh_part ? (tid & 31) : ((tid - 256) & 15);  // output group: units / channels 4 og .. +3
+    const int s0 = 2 * (dh_part ? (tid >> 5) : ((tid - 256) >> 4));  // trajectories s0, s0 + 1
+    // this thread's cache values (elements e = tid + 384 i of step t), loaded
+    // a step ahead: the loads of step t - 1 are in flight during step t's products
+    constexpr int EN = (S * HD + GRU_THREADS - 1) / GRU_THREADS;
+    float cr[EN], cz[EN], cn[EN], cg[EN], ch[EN];
+    auto load_c = [&](int t) {
+#pragma unroll
+        for (int i = 0; i < EN; ++i) {
+            const int e = tid + GRU_THREADS * i;
+            const int s = e / HD, k = e % HD;
+            if (e < S * HD && b0 + s < B && t < lens[s]) {
+                const int64_t o = ((int64_t)(b0 + s) * T + t) * HD + k;
+                cr[i] = R[o];
+                cz[i] = Z[o];
+                cn[i] = N[o];
+                cg[i] = GHN[o];
+                ch[i] = H[((int64_t)(b0 + s) * (T + 1) + t) * HD + k];
+            }
+        }
+    };
+    if (tmax > 0) load_c(tmax - 1);
     for (int t = tmax - 1; t >= 0; --t) {
-        for (int e = tid; e < S * HD; e += GRU_THREADS) {
+#pragma unroll
+        for (int i = 0; i < EN; ++i) {
+            const int e = tid + GRU_THREADS * i;
+            if (e >= S * HD) break;
             const int s = e / HD, k = e % HD;
             float gr = 0.f, gz = 0.f, gn = 0.f, gnh = 0.f, d = 0.f;
             if (b0 + s < B && t < lens[s]) {
-                const int64_t o = ((int64_t)(b0 + s) * T + t) * HD + k;
-                const float r = R[o], z = Z[o], n = N[o], ghn = GHN[o];
-                const float hp = H[((int64_t)(b0 + s) * (T + 1) + t) * HD + k];
+                const float r = cr[i], z = cz[i], n = cn[i], ghn = cg[i];
+                const float hp = ch[i];
                 const float g = dh[e];
                 const float dn = g * (1.f - z);
                 const float dz = g * (hp - n);
@@ -413,40 +458,62 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_bwd(
             } else {
                 d = dh[e];  // frozen step: dh passes through unchanged
             }
-            dgi[s * G3 + k] = gr;
-            dgi[s * G3 + HD + k] = gz;
-            dgi[s * G3 + 2 * HD + k] = gn;
-            dgh[s * G3 + k] = gr;
-            dgh[s * G3 + HD + k] = gz;
-            dgh[s * G3 + 2 * HD + k] = gnh;
+            dgi[k * SP + s] = gr;
+            dgi[(HD + k) * SP + s] = gz;
+            dgi[(2 * HD + k) * SP + s] = gn;
+            dgh[k * SP + s] = gr;
+            dgh[(HD + k) * SP + s] = gz;
+            dgh[(2 * HD + k) * SP + s] = gnh;
             dhd[e] = d;
         }
         __syncthreads();
+        if (t > 0) load_c(t - 1);
         for (int e = tid; e < S * G3; e += GRU_THREADS) {
-            const int s = e / G3;
+            const int s = e / G3, jj = e % G3;
             if (b0 + s < B && t < lens[s]) {
-                const int64_t o = ((int64_t)(b0 + s) * T + t) * G3 + e % G3;
-                G[o] = dgi[e];
-                GH[o] = dgh[e];
+                const int64_t o = ((int64_t)(b0 + s) * T + t) * G3 + jj;
+                G[o] = dgi[jj * SP + s];
+                GH[o] = dgh[jj * SP + s];
             }
         }
         // outputs: 128 dh values and 64 dA values per trajectory, each a dot
         // product over the 384 gate gradients
-        for (int e = tid; e < S * (HD + C1); e += GRU_THREADS) {
-            const int s = e / (HD + C1), q = e % (HD + C1);
-            const bool active = b0 + s < B && t < lens[s];
-            if (q < HD) {
-                float acc = dhd[s * HD + q];
-                if (active)
-                    for (int jj = 0; jj < G3; ++jj) acc = fmaf(__bfloat162float(whh[jj * HD + q]), dgh[s * G3 + jj], acc);
-                dhd[s * HD + q] = acc;
-            } else {
-                const int c = q - HD;
-                if (active) {
-                    float acc = 0.f;
-                    for (int jj = 0; jj < G3; ++jj) acc = fmaf(__bfloat162float(wih[jj * C1 + c]), dgi[s * G3 + jj], acc);
-                    dA[((int64_t)(b0 + s) * T + t) * C1 + c] = acc;
+        const bool act0 = b0 + s0 < B && t < lens[s0], act1 = b0 + s0 + 1 < B && t < lens[s0 + 1];
+        if (act0 || act1) {
+            const __nv_bfloat16* w = dh_part ? whh + 4 * og : wih + 4 * og;
+            const int wstride = dh_part ? HD : C1;
+            const float* dg = (dh_part ? dgh : dgi) + s0;
+            float a0[4], a1[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                a0[i] = dh_part ? dhd[s0 * HD + 4 * og + i] : 0.f;
+                a1[i] = dh_part ? dhd[(s0 + 1) * HD + 4 * og + i] : 0.f;
+            }
+#pragma unroll 4
+            for (int jj = 0; jj < G3; ++jj) {
+                const uint2 wv = *reinterpret_cast<const uint2*>(w + jj * wstride);
+                const float2 g2 = *reinterpret_cast<const float2*>(dg + jj * SP);
+                const float wf[4] = {__uint_as_float(wv.x << 16), __uint_as_float(wv.x & 0xffff0000u),
+                                     __uint_as_float(wv.y << 16), __uint_as_float(wv.y & 0xffff0000u)};
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    a0[i] = fmaf(wf[i], g2.x, a0[i]);
+                    a1[i] = fmaf(wf[i], g2.y, a1[i]);
                 }
+            }
+            if (dh_part) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if (act0) dhd[s0 * HD + 4 * og + i] = a0[i];
+                    if (act1) dhd[(s0 + 1) * HD + 4 * og + i] = a1[i];
+                }
+            } else {
+                if (act0)
+                    *reinterpret_cast<float4*>(dA + ((int64_t)(b0 + s0) * T + t) * C1 + 4 * og) =
+                        make_float4(a0[0], a0[1], a0[2], a0[3]);
+                if (act1)
+                    *reinterpret_cast<float4*>(dA + ((int64_t)(b0 + s0 + 1) * T + t) * C1 + 4 * og) =
+                        make_float4(a1[0], a1[1], a1[2], a1[3]);
             }
         }
         __syncthreads();
@@ -873,7 +940,7 @@ int64_t ws_layout(int B, int T, int P, float* base, EncWs* w) {
 constexpr int kGruFwdSmem = (enc::C1 * enc::G3 + enc::HD * enc::G3) * 2 +
                             (enc::S * enc::HD + enc::S * enc::C1 + 2 * enc::S * enc::G3) * 4;
 constexpr int kGruBwdSmem = (enc::G3 * enc::HD + enc::G3 * enc::C1) * 2 +
-                            (2 * enc::S * enc::HD + 2 * enc::S * enc::G3) * 4;
+                            (2 * enc::S * enc::HD + 2 * enc::G3 * enc::SP) * 4;
 
 int enc_check(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return TSM_OK;

@@ -109,6 +109,29 @@ struct RowBlock {
         return up;
     }
 
+    // The local terms of the R cells at column point c (C::term: the square
+    // root of the squared distance, or the match value), for step2t.
+    __device__ __forceinline__ void terms(const float4& c, float (&T)[R], float eps2) const {
+#pragma unroll
+        for (int r = 0; r < R; ++r) T[r] = C::term(d2nr<PACKED>(n[r], make_float2(c.x, c.y)), eps2);
+    }
+
+    // step2 with the local terms computed beforehand (by terms(), a step
+    // ahead): the same cells in the same order, so the same values.
+    __device__ __forceinline__ float step2t(const float (&Din)[R], float (&Dout)[R], const float (&T)[R], float gcol,
+                                            float top, float diag) const {
+        float up = top, dg = diag;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float left = Din[r];
+            const float nv = C::comb(dg, up, left, T[r], g[r], gcol);
+            Dout[r] = nv;
+            dg = left;
+            up = nv;
+        }
+        return up;
+    }
+
     __device__ __forceinline__ float pick(int rr) const {
         float v = 0.f;
 #pragma unroll
@@ -344,6 +367,130 @@ __device__ __forceinline__ float dp_pair_prefetch(const float2* __restrict__ row
     return dlast;
 }
 
+// The prefetching two-block pass with each cell's local term (C::term: for
+// DTW and ERP the MUFU square root of the squared distance) computed one
+// column step before the recurrence needs it.  At step j the upper block
+// computes column j and the lower block column j - 1 from terms made at step
+// j - 1; then the terms of step j + 1 are made: the lower block's at column j
+// (point already in registers), the upper block's at column j + 1 (point
+// loaded at the start of step j).  A cell's recurrence then no longer waits
+// on its own square root.  Term arrays alternate between two per block like
+// the value arrays.  The cells and their order along each dependency chain
+// are those of dp_pair_prefetch, so the values are identical.
+template <int M, int R, bool EXACT, class Cols>
+__device__ __forceinline__ float dp_pair_ahead(const float2* __restrict__ rowp, int nr, const Cols& cols, int nc,
+                                               float* buf, const KParams& p, float srow, float scol) {
+    using C = typename CellOf<M, EXACT>::type;
+    constexpr bool PK = kPacked<C, Cols>();
+    const float e2 = p.eps2;
+    for (int j = 0; j < nc; ++j) buf[32 * j] = C::topb(scol, j);
+    float dlast = 0.f;
+    int rb = 0;
+    for (; nr - rb > R; rb += 2 * R) {
+        RowBlock<C, R, EXACT, PK> hi, lo;
+        hi.load(rowp, rb, nr, srow, p);
+        lo.load(rowp, rb + R, nr, srow, p);
+        float HA[R], HB[R], LA[R], LB[R], THA[R], THB[R], TLA[R], TLB[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            HA[r] = hi.D[r];
+            LA[r] = lo.D[r];
+        }
+        float4 c = col4<EXACT>(cols, 0, p, C::kGap);
+        float top = buf[0];
+        const int j1 = min(1, nc - 1);
+        float4 cn = col4<EXACT>(cols, j1, p, C::kGap);
+        float tn = buf[32 * j1];
+        // step 0: the upper block's column 0; then the terms of step 1
+        hi.terms(c, THA, e2);
+        float ub1 = hi.step2t(HA, HB, THA, c.z, top, (rb == 0) ? C::corner() : C::rowb(srow, rb - 1));
+        lo.terms(c, TLA, e2);
+        hi.terms(cn, THA, e2);
+        float ub2 = C::rowb(srow, rb + R - 1), udiag = top, gprev = c.z;
+        // steps 1 .. nc-1: upper column j, lower column j-1, then the next step's terms
+        auto pair_step = [&](const float (&Hi)[R], float (&Ho)[R], const float (&Li)[R], float (&Lo)[R],
+                             const float (&THi)[R], float (&THo)[R], const float (&TLi)[R], float (&TLo)[R],
+                             int j) {
+            c = cn;
+            top = tn;
+            const int jn = min(j + 1, nc - 1);
+            cn = col4<EXACT>(cols, jn, p, C::kGap);
+            tn = buf[32 * jn];
+            const float nb = hi.step2t(Hi, Ho, THi, c.z, top, udiag);
+            const float lb = lo.step2t(Li, Lo, TLi, gprev, ub1, ub2);
+            buf[32 * (j - 1)] = lb;
+            lo.terms(c, TLo, e2);
+            hi.terms(cn, THo, e2);
+            udiag = top;
+            ub2 = ub1;
+            ub1 = nb;
+            gprev = c.z;
+        };
+        int j = 1;
+        for (; j + 1 < nc; j += 2) {
+            pair_step(HB, HA, LA, LB, THA, THB, TLA, TLB, j);
+            pair_step(HA, HB, LB, LA, THB, THA, TLB, TLA, j + 1);
+        }
+        float lb;
+        const int rr = nr - 1 - (rb + R);
+        if (j < nc) {
+            pair_step(HB, HA, LA, LB, THA, THB, TLA, TLB, j);
+            lb = lo.step2t(LB, LA, TLB, gprev, ub1, ub2);
+            if (rb + 2 * R >= nr) {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r == rr) dlast = LA[r];
+            }
+        } else {
+            lb = lo.step2t(LA, LB, TLA, gprev, ub1, ub2);
+            if (rb + 2 * R >= nr) {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r == rr) dlast = LB[r];
+            }
+        }
+        buf[32 * (nc - 1)] = lb;
+    }
+    if (rb < nr) {  // last rows (at most R): one block, its terms a step ahead too
+        RowBlock<C, R, EXACT, PK> blk;
+        blk.load(rowp, rb, nr, srow, p);
+        float DA[R], DB[R], TA[R], TB[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) DA[r] = blk.D[r];
+        float diag = (rb == 0) ? C::corner() : C::rowb(srow, rb - 1);
+        float4 c = col4<EXACT>(cols, 0, p, C::kGap);
+        float top = buf[0];
+        blk.terms(c, TA, e2);
+        auto st = [&](const float (&Di)[R], float (&Do)[R], const float (&Ti)[R], float (&To)[R], int j) {
+            const int jn = min(j + 1, nc - 1);
+            const float4 cn = col4<EXACT>(cols, jn, p, C::kGap);
+            const float tn = buf[32 * jn];
+            blk.step2t(Di, Do, Ti, c.z, top, diag);
+            blk.terms(cn, To, e2);
+            diag = top;
+            top = tn;
+            c = cn;
+        };
+        int j = 0;
+        for (; j + 1 < nc; j += 2) {
+            st(DA, DB, TA, TB, j);
+            st(DB, DA, TB, TA, j + 1);
+        }
+        const int rr = nr - 1 - rb;
+        if (j < nc) {
+            st(DA, DB, TA, TB, j);
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (r == rr) dlast = DB[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (r == rr) dlast = DA[r];
+        }
+    }
+    return dlast;
+}
+
 // Four-block pass (used for ERP, whose cells wait on a MUFU square root and a
 // three-way min of sums): rows rb .. rb + 4R - 1 as four blocks of R rows, block k
 // computing column s - k at step s, so a thread carries four independent
@@ -487,22 +634,39 @@ __device__ __forceinline__ float dp_pair_quad(const float2* __restrict__ rowp, i
     return dp_pair_prefetch<M, R, EXACT>(rowp, nr, cols, nc, buf, p, srow, scol, rb);
 }
 
-// The DP of one pair: the lower-block-first pass where it was measured
-// faster (EDR and LCSS with shared-memory columns), the four-block pass for
-// ERP (kQuadPass), else the prefetching one.  Measured on B200, all-pairs
-// 2000 x 2000: ERP 18.84 -> 18.05 ms with four blocks of 8 rows; DTW 15.29 ->
-// 15.69 ms (four blocks of 8) and 16.17 ms (of 4), so DTW keeps two blocks.
+// The DP of one pair, with shared-memory columns (the matrix kernels): the
+// terms-ahead pass for EDR (kAheadMask), the lower-block-first pass for LCSS,
+// the four-block pass for ERP (kQuadPass), else the prefetching one; with
+// per-lane global columns (paired and scheduled kernels) the prefetching one.
+// Measured on B200, all-pairs 2000 x 2000: ERP 18.84 -> 18.05 ms with four
+// blocks of 8 rows; DTW 15.29 -> 15.69 ms (four blocks of 8) and 16.17 ms (of
+// 4), so DTW keeps two blocks.  The four-block pass stays out of the scheduled
+// kernel: compiled into its ERP tile tasks it raised the whole kernel from 127
+// to 190 registers, and the 500k-pair uneven batch from 5.1 to 6.5 ms.
 #ifndef TSM_QUAD_PASS
 #define TSM_QUAD_PASS 1
 #endif
 constexpr bool kQuadPass = TSM_QUAD_PASS != 0;
+// Measures (bit M) whose matrix kernels run dp_pair_ahead.  Measured on B200,
+// all-pairs 2000 x 2000, every measure bit-identical to its default pass:
+// EDR 14.79 -> 13.91 ms (its match terms a step ahead beat the lower-first
+// pass); slower for the others: DTW 15.17 -> 16.02, LCSS 12.49 -> 12.87, ERP
+// 18.05 -> 19.84 (against the four-block pass), Frechet 12.33 -> 12.94 ms,
+// and slower still with blocks of 16 rows.
+#ifndef TSM_AHEAD_MASK
+#define TSM_AHEAD_MASK (1 << EDR)
+#endif
+constexpr int kAheadMask = TSM_AHEAD_MASK;
 template <int M, int R, bool EXACT, class Cols>
 __device__ __forceinline__ float dp_pair(const float2* __restrict__ rowp, int nr, const Cols& cols,
                                          int nc, float* buf, const KParams& p, float srow, float scol) {
     if (nr <= 0 || nc <= 0) return 0.f;
-    if constexpr (LowerFirst<M, Cols>::value) {
+    if constexpr (kAheadMask & (1 << M) && std::is_same<Cols, SmemCols>::value) {
+        return dp_pair_ahead<M, R, EXACT>(rowp, nr, cols, nc, buf, p, srow, scol);
+    } else if constexpr (LowerFirst<M, Cols>::value) {
         return dp_pair_lower_first<M, R, EXACT>(rowp, nr, cols, nc, buf, p, srow, scol);
-    } else if constexpr (kQuadPass && M == ERP && R <= 8) {  // 16 rows: four blocks spill
+    } else if constexpr (kQuadPass && M == ERP && R <= 8 && std::is_same<Cols, SmemCols>::value) {
+        // (16 rows: four blocks spill)
         return dp_pair_quad<M, R, EXACT>(rowp, nr, cols, nc, buf, p, srow, scol);
     } else {
         return dp_pair_prefetch<M, R, EXACT>(rowp, nr, cols, nc, buf, p, srow, scol);
