@@ -33,9 +33,8 @@
 //   enc_head_fwd      e = [Wo h_last + bo | sc_k r_k]
 //   enc_pair_loss     distances, MSE loss, dL/de (atomic)
 //   enc_head_bwd      dWo, dbo, dh_last; enc_skip_bwd: d sc_k
-//   enc_gru_bwd       BPTT: gate gradients G [B][T][384] (input side), dA [B][T][64]
+//   enc_gru_bwd       BPTT: gate gradients G [B][T][384] (input side), dA [B][T][64], bias gradients
 //   tsm_wgrad_tc      weight gradients dW_ih, dW_hh on the tensor cores (tsm_wgrad.cu)
-//   enc_colsum        bias gradients (column sums of the gate gradients)
 //   enc_conv_bwd      dW1, db1
 //   enc_adam          Adam step on the FP32 master weights
 //   enc_conv_fwd_tc   conv + relu -> BF16 a_t operand images for the tensor-core GRU
@@ -64,7 +63,7 @@ constexpr int ED = EO + SK; // embedding: [head outputs | skip weights * resampl
 static_assert(SK == 32, "enc_skip_bwd maps one skip value per lane");
 constexpr int S = 16;     // trajectories per GRU CTA
 constexpr int GRU_THREADS = 384;
-constexpr int SP = S + 2;  // row stride of the backward's trajectory-minor gate gradients (8-byte pairs, 2-way banks)
+constexpr int SP = S + 4;  // row stride of the backward's trajectory-minor gate gradients (16-byte groups of 4)
 
 // parameter offsets in the flat FP32 master buffer
 constexpr int OFF_W1 = 0;                    // [64][2][5]
@@ -117,10 +116,12 @@ __global__ void enc_conv_fwd(const float2* __restrict__ pts, const int64_t* __re
     A[gid] = a;
 }
 
-// Persistent GRU forward.  CTA = S trajectories, 384 threads (one per gate
-// row).  Shared memory: Wih^T [64][384] and Whh^T [128][384] BF16 (thread j
-// reads column j: consecutive threads, consecutive addresses), h [S][128],
-// a [S][64], gate pre-activations gi, gh [S][384].
+// Persistent GRU forward.  CTA = S trajectories, 384 threads (thread j: gate
+// rows j % 192 and j % 192 + 192 of trajectories 8 (j / 192) .. +7).  Shared
+// memory: Wih and Whh BF16, transposed into (k, k+1) pairs per gate row
+// ([k/2][384][2]: a thread reads one 4-byte pair per row, consecutive threads
+// consecutive words), h [S][128], a [S][64], gate pre-activations gi, gh
+// [S][384].
 // Caches for the backward pass (only steps t < len are written):
 //   H [B][T+1][128] (H[b][0] = 0), R, Z, N, GHN [B][T][128] with
 //   GHN = Whn h + bhn.  hl [B][128] = h after the last valid step.
@@ -129,8 +130,8 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
     const float* __restrict__ p, float* __restrict__ H, float* __restrict__ R, float* __restrict__ Z,
     float* __restrict__ N, float* __restrict__ GHN, float* __restrict__ hl) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    __nv_bfloat16* wih = reinterpret_cast<__nv_bfloat16*>(smraw);        // [64][384]
-    __nv_bfloat16* whh = wih + C1 * G3;                                   // [128][384]
+    __nv_bfloat16* wih = reinterpret_cast<__nv_bfloat16*>(smraw);        // [32][384][2]: (k, k+1) pairs per gate row
+    __nv_bfloat16* whh = wih + C1 * G3;                                   // [64][384][2]
     float* hs = reinterpret_cast<float*>(whh + HD * G3);                  // [S][128]
     float* as = hs + S * HD;                                              // [S][64]
     float* gi = as + S * C1;                                              // [S][384]
@@ -138,17 +139,25 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
     __shared__ int lens[S];
     const int j = threadIdx.x;
     const int b0 = blockIdx.x * S;
-    for (int e = j; e < G3 * C1; e += GRU_THREADS) {  // transpose into [k][j]
+    for (int e = j; e < G3 * C1; e += GRU_THREADS) {  // transpose into k-pair-major [k/2][row][k%2]
         const int row = e / C1, col = e % C1;
-        wih[col * G3 + row] = wq[OFF_WIH + e];
+        wih[((col >> 1) * G3 + row) * 2 + (col & 1)] = wq[OFF_WIH + e];
     }
     for (int e = j; e < G3 * HD; e += GRU_THREADS) {
         const int row = e / HD, col = e % HD;
-        whh[col * G3 + row] = wq[OFF_WHH + e];
+        whh[((col >> 1) * G3 + row) * 2 + (col & 1)] = wq[OFF_WHH + e];
     }
     for (int e = j; e < S * HD; e += GRU_THREADS) hs[e] = 0.f;
     if (j < S) lens[j] = (b0 + j < B) ? len[b0 + j] : 0;
-    const float bih = p[OFF_BIH + j], bhh = p[OFF_BHH + j];
+    // the products: thread j takes gate rows jr and jr + 192 for trajectories
+    // 8 sh .. 8 sh + 7, so a 4-byte load of two weights feeds 16 FMAs and a
+    // broadcast 16-byte load of four activations feeds 8
+    constexpr int SH = S / 2;
+    const int jr = j % (G3 / 2), sh = j / (G3 / 2);
+    const float bih0 = p[OFF_BIH + jr], bhh0 = p[OFF_BHH + jr];
+    const float bih1 = p[OFF_BIH + jr + G3 / 2], bhh1 = p[OFF_BHH + jr + G3 / 2];
+    const uint32_t* wih2 = reinterpret_cast<const uint32_t*>(wih);
+    const uint32_t* whh2 = reinterpret_cast<const uint32_t*>(whh);
     __syncthreads();
     int tmax = 0;
     for (int s = 0; s < S; ++s) tmax = max(tmax, lens[s]);
@@ -173,6 +182,9 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
             an[i] = (e < S * C1 && b0 + s < B && t < lens[s]) ? A[((int64_t)(b0 + s) * T + t) * C1 + e % C1] : 0.f;
         }
     };
+    // the two BF16 weights of a pair as floats (low half: even k)
+    auto lo = [](uint32_t u) { return __uint_as_float(u << 16); };
+    auto hi = [](uint32_t u) { return __uint_as_float(u & 0xffff0000u); };
     if (tmax > 0) load_a(0);
     for (int t = 0; t < tmax; ++t) {
 #pragma unroll
@@ -180,34 +192,44 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
             if (j + GRU_THREADS * i < S * C1) as[j + GRU_THREADS * i] = an[i];
         __syncthreads();
         if (t + 1 < tmax) load_a(t + 1);
-        float ai[S], ah[S];
+        float ai0[SH], ai1[SH], ah0[SH], ah1[SH];
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-            ai[s] = bih;
-            ah[s] = bhh;
+        for (int s = 0; s < SH; ++s) {
+            ai0[s] = bih0;
+            ai1[s] = bih1;
+            ah0[s] = bhh0;
+            ah1[s] = bhh1;
         }
         for (int k = 0; k < C1; k += 4) {
-            const float w0 = __bfloat162float(wih[(k + 0) * G3 + j]), w1 = __bfloat162float(wih[(k + 1) * G3 + j]);
-            const float w2 = __bfloat162float(wih[(k + 2) * G3 + j]), w3 = __bfloat162float(wih[(k + 3) * G3 + j]);
+            const uint32_t p01 = wih2[(k / 2) * G3 + jr], p23 = wih2[(k / 2 + 1) * G3 + jr];
+            const uint32_t q01 = wih2[(k / 2) * G3 + jr + G3 / 2], q23 = wih2[(k / 2 + 1) * G3 + jr + G3 / 2];
+            const float w0 = lo(p01), w1 = hi(p01), w2 = lo(p23), w3 = hi(p23);
+            const float x0 = lo(q01), x1 = hi(q01), x2 = lo(q23), x3 = hi(q23);
 #pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const float4 v = *reinterpret_cast<const float4*>(as + s * C1 + k);
-                ai[s] = fmaf(w0, v.x, fmaf(w1, v.y, fmaf(w2, v.z, fmaf(w3, v.w, ai[s]))));
+            for (int s = 0; s < SH; ++s) {
+                const float4 v = *reinterpret_cast<const float4*>(as + (SH * sh + s) * C1 + k);
+                ai0[s] = fmaf(w0, v.x, fmaf(w1, v.y, fmaf(w2, v.z, fmaf(w3, v.w, ai0[s]))));
+                ai1[s] = fmaf(x0, v.x, fmaf(x1, v.y, fmaf(x2, v.z, fmaf(x3, v.w, ai1[s]))));
             }
         }
         for (int k = 0; k < HD; k += 4) {
-            const float w0 = __bfloat162float(whh[(k + 0) * G3 + j]), w1 = __bfloat162float(whh[(k + 1) * G3 + j]);
-            const float w2 = __bfloat162float(whh[(k + 2) * G3 + j]), w3 = __bfloat162float(whh[(k + 3) * G3 + j]);
+            const uint32_t p01 = whh2[(k / 2) * G3 + jr], p23 = whh2[(k / 2 + 1) * G3 + jr];
+            const uint32_t q01 = whh2[(k / 2) * G3 + jr + G3 / 2], q23 = whh2[(k / 2 + 1) * G3 + jr + G3 / 2];
+            const float w0 = lo(p01), w1 = hi(p01), w2 = lo(p23), w3 = hi(p23);
+            const float x0 = lo(q01), x1 = hi(q01), x2 = lo(q23), x3 = hi(q23);
 #pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const float4 v = *reinterpret_cast<const float4*>(hs + s * HD + k);
-                ah[s] = fmaf(w0, v.x, fmaf(w1, v.y, fmaf(w2, v.z, fmaf(w3, v.w, ah[s]))));
+            for (int s = 0; s < SH; ++s) {
+                const float4 v = *reinterpret_cast<const float4*>(hs + (SH * sh + s) * HD + k);
+                ah0[s] = fmaf(w0, v.x, fmaf(w1, v.y, fmaf(w2, v.z, fmaf(w3, v.w, ah0[s]))));
+                ah1[s] = fmaf(x0, v.x, fmaf(x1, v.y, fmaf(x2, v.z, fmaf(x3, v.w, ah1[s]))));
             }
         }
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-            gi[s * G3 + j] = ai[s];
-            gh[s * G3 + j] = ah[s];
+        for (int s = 0; s < SH; ++s) {
+            gi[(SH * sh + s) * G3 + jr] = ai0[s];
+            gi[(SH * sh + s) * G3 + jr + G3 / 2] = ai1[s];
+            gh[(SH * sh + s) * G3 + jr] = ah0[s];
+            gh[(SH * sh + s) * G3 + jr + G3 / 2] = ah1[s];
         }
         __syncthreads();
         for (int e = j; e < S * HD; e += GRU_THREADS) {
@@ -376,7 +398,8 @@ __global__ void enc_skip_bwd(const float* __restrict__ dE, const float* __restri
 __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_bwd(
     const float* __restrict__ dhl, const int32_t* __restrict__ len, int B, int T, const __nv_bfloat16* __restrict__ wq,
     const float* __restrict__ H, const float* __restrict__ R, const float* __restrict__ Z, const float* __restrict__ N,
-    const float* __restrict__ GHN, float* __restrict__ G, float* __restrict__ GH, float* __restrict__ dA) {
+    const float* __restrict__ GHN, float* __restrict__ G, float* __restrict__ GH, float* __restrict__ dA,
+    float* __restrict__ gbih, float* __restrict__ gbhh) {
     extern __shared__ __align__(16) unsigned char smraw[];
     __nv_bfloat16* whh = reinterpret_cast<__nv_bfloat16*>(smraw);  // [384][128]
     __nv_bfloat16* wih = whh + G3 * HD;                             // [384][64]
@@ -408,15 +431,16 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_bwd(
     }
     int tmax = 0;
     for (int s = 0; s < S; ++s) tmax = max(tmax, lens[s]);
-    // The output products: threads 0..255 take 4 consecutive hidden units
-    // (dh) of two trajectories, threads 256..383 4 consecutive channels (dA)
-    // of two trajectories; per gate row jj one 8-byte load of 4 BF16 weights
-    // and one of the two trajectories' gate gradients feed 8 FMAs.  Each sum
-    // runs over jj in order from the same start as a dot product per output
-    // would, so the values are those of one thread per output.
+    // The output products: threads 0..255 take 2 consecutive hidden units
+    // (dh) of four trajectories, threads 256..383 2 consecutive channels (dA)
+    // of four trajectories; per gate row jj one 4-byte load of 2 BF16 weights
+    // and one 16-byte load of the four trajectories' gate gradients feed 8
+    // FMAs.  Each sum runs over jj in order from the same start as a dot
+    // product per output would, so the values are those of one thread per output.
+    float sbi = 0.f, sbh = 0.f;  // this CTA's bias gradients of gate row tid (phase 2 maps e % 384 = tid)
     const bool dh_part = tid < 256;
-    const int og = dh_part ? (tid & 31) : ((tid - 256) & 15);  // output group: units / channels 4 og .. +3
-    const int s0 = 2 * (dh_part ? (tid >> 5) : ((tid - 256) >> 4));  // trajectories s0, s0 + 1
+    const int og = dh_part ? (tid & 63) : ((tid - 256) & 31);  // output pair: units / channels 2 og, 2 og + 1
+    const int s0 = 4 * (dh_part ? (tid >> 6) : ((tid - 256) >> 5));  // trajectories s0 .. s0 + 3
     // this thread's cache values (elements e = tid + 384 i of step t), loaded
     // a step ahead: the loads of step t - 1 are in flight during step t's products
     constexpr int EN = (S * HD + GRU_THREADS - 1) / GRU_THREADS;
@@ -468,99 +492,99 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_bwd(
         }
         __syncthreads();
         if (t > 0) load_c(t - 1);
+        // gate gradients to global memory; thread tid always holds gate row
+        // jj = tid here, so it also sums that row's bias gradients
         for (int e = tid; e < S * G3; e += GRU_THREADS) {
             const int s = e / G3, jj = e % G3;
             if (b0 + s < B && t < lens[s]) {
                 const int64_t o = ((int64_t)(b0 + s) * T + t) * G3 + jj;
-                G[o] = dgi[jj * SP + s];
-                GH[o] = dgh[jj * SP + s];
+                const float vi = dgi[jj * SP + s], vh = dgh[jj * SP + s];
+                G[o] = vi;
+                GH[o] = vh;
+                sbi += vi;
+                sbh += vh;
             }
         }
         // outputs: 128 dh values and 64 dA values per trajectory, each a dot
         // product over the 384 gate gradients
-        const bool act0 = b0 + s0 < B && t < lens[s0], act1 = b0 + s0 + 1 < B && t < lens[s0 + 1];
-        if (act0 || act1) {
-            const __nv_bfloat16* w = dh_part ? whh + 4 * og : wih + 4 * og;
+        bool act[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) act[q] = b0 + s0 + q < B && t < lens[s0 + q];
+        if (act[0] || act[1] || act[2] || act[3]) {
+            const __nv_bfloat16* w = dh_part ? whh + 2 * og : wih + 2 * og;
             const int wstride = dh_part ? HD : C1;
             const float* dg = (dh_part ? dgh : dgi) + s0;
-            float a0[4], a1[4];
+            float a[4][2];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                a0[i] = dh_part ? dhd[s0 * HD + 4 * og + i] : 0.f;
-                a1[i] = dh_part ? dhd[(s0 + 1) * HD + 4 * og + i] : 0.f;
-            }
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int i = 0; i < 2; ++i) a[q][i] = dh_part ? dhd[(s0 + q) * HD + 2 * og + i] : 0.f;
 #pragma unroll 4
             for (int jj = 0; jj < G3; ++jj) {
-                const uint2 wv = *reinterpret_cast<const uint2*>(w + jj * wstride);
-                const float2 g2 = *reinterpret_cast<const float2*>(dg + jj * SP);
-                const float wf[4] = {__uint_as_float(wv.x << 16), __uint_as_float(wv.x & 0xffff0000u),
-                                     __uint_as_float(wv.y << 16), __uint_as_float(wv.y & 0xffff0000u)};
+                const uint32_t wv = *reinterpret_cast<const uint32_t*>(w + jj * wstride);
+                const float4 g4 = *reinterpret_cast<const float4*>(dg + jj * SP);
+                const float w0 = __uint_as_float(wv << 16), w1 = __uint_as_float(wv & 0xffff0000u);
+                const float gq[4] = {g4.x, g4.y, g4.z, g4.w};
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    a0[i] = fmaf(wf[i], g2.x, a0[i]);
-                    a1[i] = fmaf(wf[i], g2.y, a1[i]);
+                for (int q = 0; q < 4; ++q) {
+                    a[q][0] = fmaf(w0, gq[q], a[q][0]);
+                    a[q][1] = fmaf(w1, gq[q], a[q][1]);
                 }
             }
-            if (dh_part) {
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    if (act0) dhd[s0 * HD + 4 * og + i] = a0[i];
-                    if (act1) dhd[(s0 + 1) * HD + 4 * og + i] = a1[i];
+            for (int q = 0; q < 4; ++q) {
+                if (!act[q]) continue;
+                if (dh_part) {
+                    dhd[(s0 + q) * HD + 2 * og] = a[q][0];
+                    dhd[(s0 + q) * HD + 2 * og + 1] = a[q][1];
+                } else {
+                    *reinterpret_cast<float2*>(dA + ((int64_t)(b0 + s0 + q) * T + t) * C1 + 2 * og) =
+                        make_float2(a[q][0], a[q][1]);
                 }
-            } else {
-                if (act0)
-                    *reinterpret_cast<float4*>(dA + ((int64_t)(b0 + s0) * T + t) * C1 + 4 * og) =
-                        make_float4(a0[0], a0[1], a0[2], a0[3]);
-                if (act1)
-                    *reinterpret_cast<float4*>(dA + ((int64_t)(b0 + s0 + 1) * T + t) * C1 + 4 * og) =
-                        make_float4(a1[0], a1[1], a1[2], a1[3]);
             }
         }
         __syncthreads();
         for (int e = tid; e < S * HD; e += GRU_THREADS) dh[e] = dhd[e];
         __syncthreads();
     }
+    atomicAdd(gbih + tid, sbi);
+    atomicAdd(gbhh + tid, sbh);
 }
 
-// Column sums: out[n] += sum_k A[k*lda + n] (bias gradients).
-__global__ void enc_colsum(const float* __restrict__ Am, int64_t lda, int64_t K, int Nn, int64_t kchunk,
-                           float* __restrict__ out) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= Nn) return;
-    const int64_t k_begin = (int64_t)blockIdx.y * kchunk, k_end = min(K, k_begin + kchunk);
-    float acc = 0.f;
-    for (int64_t k = k_begin; k < k_end; ++k) acc += Am[k * lda + n];
-    atomicAdd(out + n, acc);
-}
-
-// Conv weight gradients.  One CTA per (b, t-chunk); thread per (c, i, k) of
-// the 640 weights + 64 biases accumulates over the chunk's steps.
-__global__ void enc_conv_bwd(const float2* __restrict__ pts, const int64_t* __restrict__ off,
-                             const int32_t* __restrict__ len, int B, int T, float4 nrm, const float* __restrict__ A,
-                             const float* __restrict__ dA, int tchunk, float* __restrict__ grad) {
+// Conv weight gradients.  One CTA per trajectory, 704 threads: thread q
+// takes weight (c, i, k) = (q / 10, (q / 5) % 2, q % 5) of the 640, or the
+// bias of channel q - 640, summed over the trajectory's steps (one atomic per
+// thread and trajectory).  The normalised input points are staged in shared
+// memory, CBW_T steps (plus the window's two on either side) at a time.
+constexpr int CBW_THREADS = C1 * 2 * KW + C1;  // 704
+constexpr int CBW_T = 256;
+__global__ void __launch_bounds__(CBW_THREADS) enc_conv_bwd(const float2* __restrict__ pts,
+                                                           const int64_t* __restrict__ off,
+                                                           const int32_t* __restrict__ len, int T, float4 nrm,
+                                                           const float* __restrict__ A, const float* __restrict__ dA,
+                                                           float* __restrict__ grad) {
+    __shared__ float xs[CBW_T + KW - 1][2];  // xs[u][i] = input i at step t0 + u - 2
     const int b = blockIdx.x;
-    const int t0 = blockIdx.y * tchunk;
     const int n = len[b];
-    const int t1 = min(n, t0 + tchunk);
-    const int q = threadIdx.x;  // 0..703
-    if (q >= C1 * 2 * KW + C1) return;
+    if (n <= 0) return;  // uniform per CTA
+    const int q = threadIdx.x;
+    const bool wt = q < C1 * 2 * KW;
+    const int c = wt ? q / (2 * KW) : q - C1 * 2 * KW, i = (q / KW) % 2, k = q % KW;
+    const int64_t o0 = off[b];
     float acc = 0.f;
-    if (q < C1 * 2 * KW) {
-        const int c = q / (2 * KW), i = (q / KW) % 2, k = q % KW;
+    for (int t0 = 0; t0 < n; t0 += CBW_T) {
+        const int t1 = min(n, t0 + CBW_T);
+        __syncthreads();  // the previous chunk's readers are done
+        for (int e = q; e < (t1 - t0 + KW - 1) * 2; e += CBW_THREADS)
+            xs[e / 2][e % 2] = xin(pts, o0, n, t0 + e / 2 - 2, e % 2, nrm);
+        __syncthreads();
         for (int t = t0; t < t1; ++t) {
             const int64_t o = ((int64_t)b * T + t) * C1 + c;
             const float g = A[o] > 0.f ? dA[o] : 0.f;
-            acc = fmaf(g, xin(pts, off[b], n, t + k - 2, i, nrm), acc);
+            acc = wt ? fmaf(g, xs[t - t0 + k][i], acc) : acc + g;
         }
-        atomicAdd(grad + OFF_W1 + q, acc);
-    } else {
-        const int c = q - C1 * 2 * KW;
-        for (int t = t0; t < t1; ++t) {
-            const int64_t o = ((int64_t)b * T + t) * C1 + c;
-            acc += A[o] > 0.f ? dA[o] : 0.f;
-        }
-        atomicAdd(grad + OFF_B1 + c, acc);
     }
+    atomicAdd(grad + (wt ? OFF_W1 + q : OFF_B1 + c), acc);
 }
 
 __global__ void enc_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
@@ -989,20 +1013,15 @@ int enc_backward(const float* params, const float* pts, const int64_t* off, cons
     int rc = enc_check(cudaFuncSetAttribute(enc_gru_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, kGruBwdSmem),
                        "cudaFuncSetAttribute(enc_gru_bwd)");
     if (rc) return rc;
+    // the bias gradients (sums of the gate gradients over the valid (b, t)) come out of the BPTT kernel
     enc_gru_bwd<<<(B + S - 1) / S, GRU_THREADS, kGruBwdSmem, s>>>(w.dhl, len, B, T, w.wq, w.H, w.R, w.Z, w.N,
-                                                                   w.GHN, w.G, w.GH, w.dA);
+                                                                   w.GHN, w.G, w.GH, w.dA, grad + OFF_BIH,
+                                                                   grad + OFF_BHH);
     // weight gradients dWih[j][c] += G . A, dWhh[j][k] += GH . H[t]: reductions over the valid (b, t) on the
-    // tensor cores (tsm_wgrad.cu); the bias gradients are column sums over k = b*T + t
+    // tensor cores (tsm_wgrad.cu)
     if ((rc = tsm_wgrad_tc(w.G, w.GH, w.A, w.H, len, B, T, w.wg, w.status, grad + OFF_WIH, grad + OFF_WHH, s)))
         return rc;
-    const int64_t K = (int64_t)B * T;
-    const int64_t kchunk = 2048;
-    const unsigned kz = (unsigned)((K + kchunk - 1) / kchunk);
-    enc_colsum<<<dim3((G3 + 127) / 128, kz), 128, 0, s>>>(w.G, G3, K, G3, kchunk, grad + OFF_BIH);
-    enc_colsum<<<dim3((G3 + 127) / 128, kz), 128, 0, s>>>(w.GH, G3, K, G3, kchunk, grad + OFF_BHH);
-    const int tchunk = 64;
-    enc_conv_bwd<<<dim3(B, (T + tchunk - 1) / tchunk), 704, 0, s>>>(reinterpret_cast<const float2*>(pts), off, len,
-                                                                    B, T, n4, w.A, w.dA, tchunk, grad);
+    enc_conv_bwd<<<B, CBW_THREADS, 0, s>>>(reinterpret_cast<const float2*>(pts), off, len, T, n4, w.A, w.dA, grad);
     return enc_check(cudaGetLastError(), "encoder backward launch");
 }
 
