@@ -64,6 +64,7 @@ static_assert(SK == 32, "enc_skip_bwd maps one skip value per lane");
 constexpr int S = 16;     // trajectories per GRU CTA
 constexpr int GRU_THREADS = 384;
 constexpr int SP = S + 4;  // row stride of the backward's trajectory-minor gate gradients (16-byte groups of 4)
+constexpr int SPA = S + 4; // row stride of the forward's trajectory-minor h and a_t
 
 // parameter offsets in the flat FP32 master buffer
 constexpr int OFF_W1 = 0;                    // [64][2][5]
@@ -132,9 +133,9 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
     extern __shared__ __align__(16) unsigned char smraw[];
     __nv_bfloat16* wih = reinterpret_cast<__nv_bfloat16*>(smraw);        // [32][384][2]: (k, k+1) pairs per gate row
     __nv_bfloat16* whh = wih + C1 * G3;                                   // [64][384][2]
-    float* hs = reinterpret_cast<float*>(whh + HD * G3);                  // [S][128]
-    float* as = hs + S * HD;                                              // [S][64]
-    float* gi = as + S * C1;                                              // [S][384]
+    float* hs = reinterpret_cast<float*>(whh + HD * G3);                  // [128][SPA]: h, trajectory-minor
+    float* as = hs + HD * SPA;                                            // [64][SPA]: a_t, trajectory-minor
+    float* gi = as + C1 * SPA;                                            // [S][384]
     float* gh = gi + S * G3;                                              // [S][384]
     __shared__ int lens[S];
     const int j = threadIdx.x;
@@ -147,11 +148,12 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
         const int row = e / HD, col = e % HD;
         whh[((col >> 1) * G3 + row) * 2 + (col & 1)] = wq[OFF_WHH + e];
     }
-    for (int e = j; e < S * HD; e += GRU_THREADS) hs[e] = 0.f;
+    for (int e = j; e < HD * SPA; e += GRU_THREADS) hs[e] = 0.f;
     if (j < S) lens[j] = (b0 + j < B) ? len[b0 + j] : 0;
     // the products: thread j takes gate rows jr and jr + 192 for trajectories
-    // 8 sh .. 8 sh + 7, so a 4-byte load of two weights feeds 16 FMAs and a
-    // broadcast 16-byte load of four activations feeds 8
+    // 8 sh .. 8 sh + 7 as four (s, s + 1) pairs, FP32x2 FMAs of one weight
+    // against two trajectories' activations: a 4-byte load of two weights
+    // feeds 16 FMAs, a broadcast 16-byte load of four activations 8
     constexpr int SH = S / 2;
     const int jr = j % (G3 / 2), sh = j / (G3 / 2);
     const float bih0 = p[OFF_BIH + jr], bhh0 = p[OFF_BHH + jr];
@@ -188,48 +190,57 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
     if (tmax > 0) load_a(0);
     for (int t = 0; t < tmax; ++t) {
 #pragma unroll
-        for (int i = 0; i < AN; ++i)
-            if (j + GRU_THREADS * i < S * C1) as[j + GRU_THREADS * i] = an[i];
+        for (int i = 0; i < AN; ++i) {
+            const int e = j + GRU_THREADS * i;  // element (s, c) = (e / 64, e % 64)
+            if (e < S * C1) as[(e % C1) * SPA + e / C1] = an[i];
+        }
         __syncthreads();
         if (t + 1 < tmax) load_a(t + 1);
-        float ai0[SH], ai1[SH], ah0[SH], ah1[SH];
+        // accumulator pairs (trajectories 8 sh + 2 q, 8 sh + 2 q + 1) of rows jr and jr + 192
+        float2 ai0[SH / 2], ai1[SH / 2], ah0[SH / 2], ah1[SH / 2];
 #pragma unroll
-        for (int s = 0; s < SH; ++s) {
-            ai0[s] = bih0;
-            ai1[s] = bih1;
-            ah0[s] = bhh0;
-            ah1[s] = bhh1;
+        for (int q = 0; q < SH / 2; ++q) {
+            ai0[q] = make_float2(bih0, bih0);
+            ai1[q] = make_float2(bih1, bih1);
+            ah0[q] = make_float2(bhh0, bhh0);
+            ah1[q] = make_float2(bhh1, bhh1);
         }
-        for (int k = 0; k < C1; k += 4) {
-            const uint32_t p01 = wih2[(k / 2) * G3 + jr], p23 = wih2[(k / 2 + 1) * G3 + jr];
-            const uint32_t q01 = wih2[(k / 2) * G3 + jr + G3 / 2], q23 = wih2[(k / 2 + 1) * G3 + jr + G3 / 2];
-            const float w0 = lo(p01), w1 = hi(p01), w2 = lo(p23), w3 = hi(p23);
-            const float x0 = lo(q01), x1 = hi(q01), x2 = lo(q23), x3 = hi(q23);
+        // k + 3, k + 2, k + 1, k within each group of four: the order of a
+        // nested fmaf(w_k, v_k, fmaf(w_k+1, v_k+1, ...)) dot product
+        auto prods = [&](const uint32_t* w2, const float* v, int K, float2 (&acc0)[SH / 2], float2 (&acc1)[SH / 2]) {
+            for (int k = 0; k < K; k += 4) {
+                const uint32_t p01 = w2[(k / 2) * G3 + jr], p23 = w2[(k / 2 + 1) * G3 + jr];
+                const uint32_t q01 = w2[(k / 2) * G3 + jr + G3 / 2], q23 = w2[(k / 2 + 1) * G3 + jr + G3 / 2];
+                const float wr0[4] = {lo(p01), hi(p01), lo(p23), hi(p23)};
+                const float wr1[4] = {lo(q01), hi(q01), lo(q23), hi(q23)};
 #pragma unroll
-            for (int s = 0; s < SH; ++s) {
-                const float4 v = *reinterpret_cast<const float4*>(as + (SH * sh + s) * C1 + k);
-                ai0[s] = fmaf(w0, v.x, fmaf(w1, v.y, fmaf(w2, v.z, fmaf(w3, v.w, ai0[s]))));
-                ai1[s] = fmaf(x0, v.x, fmaf(x1, v.y, fmaf(x2, v.z, fmaf(x3, v.w, ai1[s]))));
+                for (int kk = 3; kk >= 0; --kk) {
+                    const float4 va = *reinterpret_cast<const float4*>(v + (k + kk) * SPA + SH * sh);
+                    const float4 vb = *reinterpret_cast<const float4*>(v + (k + kk) * SPA + SH * sh + 4);
+                    const float2 vv[4] = {make_float2(va.x, va.y), make_float2(va.z, va.w),
+                                          make_float2(vb.x, vb.y), make_float2(vb.z, vb.w)};
+                    const float2 w0 = make_float2(wr0[kk], wr0[kk]), w1 = make_float2(wr1[kk], wr1[kk]);
+#pragma unroll
+                    for (int q = 0; q < SH / 2; ++q) {
+                        acc0[q] = __ffma2_rn(w0, vv[q], acc0[q]);
+                        acc1[q] = __ffma2_rn(w1, vv[q], acc1[q]);
+                    }
+                }
             }
-        }
-        for (int k = 0; k < HD; k += 4) {
-            const uint32_t p01 = whh2[(k / 2) * G3 + jr], p23 = whh2[(k / 2 + 1) * G3 + jr];
-            const uint32_t q01 = whh2[(k / 2) * G3 + jr + G3 / 2], q23 = whh2[(k / 2 + 1) * G3 + jr + G3 / 2];
-            const float w0 = lo(p01), w1 = hi(p01), w2 = lo(p23), w3 = hi(p23);
-            const float x0 = lo(q01), x1 = hi(q01), x2 = lo(q23), x3 = hi(q23);
+        };
+        prods(wih2, as, C1, ai0, ai1);
+        prods(whh2, hs, HD, ah0, ah1);
 #pragma unroll
-            for (int s = 0; s < SH; ++s) {
-                const float4 v = *reinterpret_cast<const float4*>(hs + (SH * sh + s) * HD + k);
-                ah0[s] = fmaf(w0, v.x, fmaf(w1, v.y, fmaf(w2, v.z, fmaf(w3, v.w, ah0[s]))));
-                ah1[s] = fmaf(x0, v.x, fmaf(x1, v.y, fmaf(x2, v.z, fmaf(x3, v.w, ah1[s]))));
-            }
-        }
-#pragma unroll
-        for (int s = 0; s < SH; ++s) {
-            gi[(SH * sh + s) * G3 + jr] = ai0[s];
-            gi[(SH * sh + s) * G3 + jr + G3 / 2] = ai1[s];
-            gh[(SH * sh + s) * G3 + jr] = ah0[s];
-            gh[(SH * sh + s) * G3 + jr + G3 / 2] = ah1[s];
+        for (int q = 0; q < SH / 2; ++q) {
+            const int s = SH * sh + 2 * q;
+            gi[s * G3 + jr] = ai0[q].x;
+            gi[(s + 1) * G3 + jr] = ai0[q].y;
+            gi[s * G3 + jr + G3 / 2] = ai1[q].x;
+            gi[(s + 1) * G3 + jr + G3 / 2] = ai1[q].y;
+            gh[s * G3 + jr] = ah0[q].x;
+            gh[(s + 1) * G3 + jr] = ah0[q].y;
+            gh[s * G3 + jr + G3 / 2] = ah1[q].x;
+            gh[(s + 1) * G3 + jr + G3 / 2] = ah1[q].y;
         }
         __syncthreads();
         for (int e = j; e < S * HD; e += GRU_THREADS) {
@@ -239,7 +250,7 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
                 const float z = sigm(gi[s * G3 + HD + k] + gh[s * G3 + HD + k]);
                 const float ghn = gh[s * G3 + 2 * HD + k];
                 const float n = tanhf(gi[s * G3 + 2 * HD + k] + r * ghn);
-                const float hp = hs[e];
+                const float hp = hs[k * SPA + s];
                 const float hn = (1.f - z) * n + z * hp;
                 const int64_t o = ((int64_t)(b0 + s) * T + t) * HD + k;
                 R[o] = r;
@@ -247,14 +258,14 @@ __global__ void __launch_bounds__(GRU_THREADS, 1) enc_gru_fwd(
                 N[o] = n;
                 GHN[o] = ghn;
                 H[((int64_t)(b0 + s) * (T + 1) + t + 1) * HD + k] = hn;
-                hs[e] = hn;
+                hs[k * SPA + s] = hn;
             }
         }
         __syncthreads();
     }
     for (int e = j; e < S * HD; e += GRU_THREADS) {
         const int s = e / HD;
-        if (b0 + s < B) hl[(int64_t)(b0 + s) * HD + e % HD] = hs[e];
+        if (b0 + s < B) hl[(int64_t)(b0 + s) * HD + e % HD] = hs[(e % HD) * SPA + s];
     }
 }
 
@@ -962,7 +973,7 @@ int64_t ws_layout(int B, int T, int P, float* base, EncWs* w) {
 }
 
 constexpr int kGruFwdSmem = (enc::C1 * enc::G3 + enc::HD * enc::G3) * 2 +
-                            (enc::S * enc::HD + enc::S * enc::C1 + 2 * enc::S * enc::G3) * 4;
+                            (enc::HD * enc::SPA + enc::C1 * enc::SPA + 2 * enc::S * enc::G3) * 4;
 constexpr int kGruBwdSmem = (enc::G3 * enc::HD + enc::G3 * enc::C1) * 2 +
                             (2 * enc::S * enc::HD + 2 * enc::G3 * enc::SP) * 4;
 
