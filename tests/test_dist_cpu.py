@@ -225,3 +225,85 @@ def test_two_rank_gloo_matrix_sharded_matches_single_process():
     so = np.concatenate([[0], np.cumsum(ls)[:-1]])
     d64, _ = O.matrix_idx(O.pairs_f64, 0, qp, qo, lq, sp, so, ls)
     assert np.all(np.abs(want["dtw"] - d64) <= 1e-5 * d64)
+
+
+# -- data-parallel encoder training -------------------------------------------------
+# Encoder.fit's data-parallel loop (shares of one global batch per rank, one
+# all-reduce of the pair-weighted gradients per step) around a CPU stand-in
+# for the kernels: a linear model of the pair's feature difference, plain
+# gradient steps.  Two gloo ranks with batch_pairs = B must end where one
+# process with batch_pairs = 2B ends.
+
+class _FakeSet:
+    def __init__(self, feat):
+        import torch
+        self.feat = feat
+        self.device = torch.device("cpu")
+
+
+def _linear_encoder():
+    import torch
+    from trajsimimeasures_b200.surrogate import Encoder
+
+    class _Linear(Encoder):
+        def loss_grad(self, s, tidx, ia, ib, y, w=None, stream=None):
+            t = torch.as_tensor(np.asarray(tidx))
+            d = s.feat[t[torch.as_tensor(ia)]] - s.feat[t[torch.as_tensor(ib)]]
+            err = d @ self.params - torch.as_tensor(np.asarray(y), dtype=torch.float64)
+            wp = torch.ones_like(err) if w is None else torch.as_tensor(np.asarray(w), dtype=torch.float64)
+            loss = (wp * err * err).mean().reshape(1)
+            grad = 2.0 * ((wp * err)[:, None] * d).mean(0)
+            return loss, grad, None
+
+        def adam(self, grad, lr=1e-3, **kw):
+            self.params -= lr * grad
+
+        def check_training(self, stream=None):
+            pass
+
+    return _Linear(params=torch.zeros(24, dtype=torch.float64), nrm=np.zeros(4))
+
+
+def _dp_case():
+    import torch
+    rng = np.random.default_rng(9)
+    feat = torch.as_tensor(rng.normal(size=(300, 24)))
+    pa, pb = rng.integers(0, 300, 257), rng.integers(0, 300, 257)  # 257: a last global batch of one pair
+    theta = rng.normal(size=24)
+    y = np.abs((feat.numpy()[pa] - feat.numpy()[pb]) @ theta) + 0.1
+    return _FakeSet(feat), pa, pb, y
+
+
+def _dp_worker(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        s, pa, pb, y = _dp_case()
+        enc = _linear_encoder()
+        hist = enc.fit(s, pa, pb, y, epochs=3, batch_pairs=64, lr=0.002, seed=4, relative=True,
+                       group=dist.group.WORLD)
+        q.put((rank, enc.params.numpy().copy(), hist))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_two_rank_gloo_data_parallel_fit_matches_one_process():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_dp_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict((r, (th, h)) for r, th, h in (q.get(timeout=240) for _ in range(2)))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    s, pa, pb, y = _dp_case()
+    one = _linear_encoder()
+    hist = one.fit(s, pa, pb, y, epochs=3, batch_pairs=128, lr=0.002, seed=4, relative=True)
+    np.testing.assert_array_equal(got[0][0], got[1][0])  # the replicas stay equal
+    np.testing.assert_allclose(got[0][0], one.params.numpy(), rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(got[0][1], hist, rtol=1e-10)
+    assert hist[-1] < hist[0]  # it trains

@@ -250,13 +250,26 @@ class Encoder:
         _lib.check(rc, "tsm_enc_adam")
 
     def fit(self, s: TrajSet, pa, pb, y, *, epochs=5, batch_pairs=1024, lr=1e-3, seed=0, log=None,
-            relative=False, floor=1e-3, train_skip=True):
+            relative=False, floor=1e-3, train_skip=True, group=None):
         """Trains on pairs (pa[i], pb[i]) of s with targets y (normalised
         distances).  relative=True weights each pair by 1 / max(y, floor)^2
         (relative squared error: near pairs count as much as far ones).
         Every step encodes the 2*batch_pairs endpoints.  The loss is summed
         on the device and read once per epoch (the host does not wait for
-        each step).  -> mean loss per epoch."""
+        each step).  -> mean loss per epoch.
+
+        Data-parallel with `group`, a torch.distributed process group
+        (torch.distributed.group.WORLD for all ranks), called on every rank
+        of it: every rank holds the same pool,
+        pairs, targets and initial parameters; a step takes one global batch
+        of batch_pairs * world pairs from the permutation that every rank
+        draws from `seed`, rank r computes the gradient of pairs r, r + world,
+        ... of it, and one all-reduce forms the pair-weighted mean gradient,
+        so every rank applies the same Adam step and the replicas stay equal.
+        One process trains exactly as before."""
+        import torch.distributed as dist
+        world = dist.get_world_size(group) if group is not None else 1
+        rank = dist.get_rank(group) if world > 1 else 0
         pa, pb, y = np.asarray(pa), np.asarray(pb), np.asarray(y, dtype=np.float32)
         wts = (1.0 / np.maximum(y, floor) ** 2).astype(np.float32) if relative else None
         rng = np.random.Generator(np.random.PCG64(seed))
@@ -265,16 +278,26 @@ class Encoder:
         for ep in range(epochs):
             perm = rng.permutation(n)
             tot = torch.zeros(1, dtype=torch.float64, device=s.device)
-            for b0 in range(0, n, batch_pairs):
-                sel = perm[b0:b0 + batch_pairs]
+            for b0 in range(0, n, batch_pairs * world):
+                sel_all = perm[b0:b0 + batch_pairs * world]
+                sel = sel_all[rank::world]
                 P = len(sel)
-                tidx = np.concatenate([pa[sel], pb[sel]])
-                loss, grad, _ = self.loss_grad(s, tidx, np.arange(P), P + np.arange(P), y[sel],
-                                               None if wts is None else wts[sel])
+                if P:
+                    tidx = np.concatenate([pa[sel], pb[sel]])
+                    loss, grad, _ = self.loss_grad(s, tidx, np.arange(P), P + np.arange(P), y[sel],
+                                                   None if wts is None else wts[sel])
+                else:  # a final global batch smaller than the world: this rank adds nothing
+                    loss, grad = torch.zeros(1, device=s.device), torch.zeros_like(self.params)
+                if world > 1:  # per-rank means -> the mean over the global batch
+                    grad.mul_(P)
+                    dist.all_reduce(grad, group=group)
+                    grad.div_(len(sel_all))
                 if not train_skip:
                     grad[-NSKIP:] = 0.0  # the skip weights keep their initial values
                 self.adam(grad, lr=lr * 0.5 * (1 + math.cos(math.pi * (ep + b0 / n) / epochs)))
                 tot += loss.double() * P
+            if world > 1:
+                dist.all_reduce(tot, group=group)
             hist.append(float(tot.item()) / n)
             self.check_training()
             if log:
