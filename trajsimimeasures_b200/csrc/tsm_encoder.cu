@@ -976,6 +976,10 @@ constexpr int kGruFwdSmem = (enc::C1 * enc::G3 + enc::HD * enc::G3) * 2 +
                             (enc::HD * enc::SPA + enc::C1 * enc::SPA + 2 * enc::S * enc::G3) * 4;
 constexpr int kGruBwdSmem = (enc::G3 * enc::HD + enc::G3 * enc::C1) * 2 +
                             (2 * enc::S * enc::HD + 2 * enc::G3 * enc::SP) * 4;
+// one CTA per SM: dynamic shared memory plus the kernels' 1 KB of static
+// shared memory must fit the 227 KB a CTA may use
+static_assert(kGruFwdSmem + 1024 <= 227 * 1024, "enc_gru_fwd shared memory");
+static_assert(kGruBwdSmem + 1024 <= 227 * 1024, "enc_gru_bwd shared memory");
 
 int enc_check(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return TSM_OK;
